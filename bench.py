@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Throughput of the per-Runge-Kutta-stage ideal-MHD path on B200.
+
+A step is one full RK3 cycle (3 stages: fluxes, corner EMF, update + CT, FOFC test and
+repair, boundaries, con2prim + dt) over the whole mesh, with dt computed on the device.
+Default workload: 3D MHD blast, 512^3, PPM + HLLD + RK3, FOFC and flattening on, seeded
+1e-3 density noise, in the FP64 form (headline `value`) and the mixed FP32/FP64 form.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl chasqui|reference] [--n 512]
+
+Multi-GPU: the path does not shard (single-block solver): N ranks run N independent
+replicas ("replicas only"); value = all ranks' zone updates / max-over-ranks device time.
+Every timing is CUDA-event device time on the mesh's stream. The state (~67 GB FP64 at
+512^3) is far larger than L2, so no flush is needed between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s & % HBM peak (FP64 vs mixed); served-jobs p50/p99 latency"
+UNIT = "zone-updates/s"
+# algorithmic bytes per cell per RK stage (3D, FOFC on); K1 face fluxes alone
+BYTES_STEP = {"fp64": 1132, "mixed": 748}
+BYTES_K1 = {"fp64": 408, "mixed": 216}
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------------------
+def dist_init():
+    world = env_int("WORLD_SIZE", 1)
+    if world <= 1:
+        return None
+    import torch.distributed as dist
+    import datetime
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def dist_max(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def blast_config(n: int, precision: int):
+    from chasqui_b200 import make_config
+    return make_config(nx1=n, nx2=n, nx3=n, x1min=-0.5, x1max=0.5, x2min=-0.5, x2max=0.5, x3min=-0.5, x3max=0.5,
+                       recon=2, rsolver=1, integrator=3, cfl=0.3, fofc=1, flatten=1, precision=precision, tlim=0.2)
+
+
+def run_form(n, precision, ics_state, steps, warmup, dist, device, sample_clocks=False, profile_cycles=2):
+    from chasqui_b200 import Mesh
+    u, b1, b2, b3 = ics_state
+    mesh = Mesh(blast_config(n, precision))
+    mesh.set_state(u, b1, b2, b3)
+    mesh.prime(0.0)
+    mesh.cycles(warmup)
+    mesh.clock()
+    l0 = mesh.kernel_launches()
+    barrier(dist)
+    sampler = ClockSampler(device) if sample_clocks else None
+    if sampler:
+        sampler.__enter__()
+    mesh.record(0)
+    mesh.cycles(steps)
+    mesh.record(1)
+    ms = mesh.elapsed_ms(0, 1)
+    if sampler:
+        sampler.__exit__()
+    launches = mesh.kernel_launches() - l0
+    ck = mesh.clock()
+    ms_max = dist_max(dist, ms)
+    # per-kernel device times (separate short run with per-kernel events)
+    mesh.profile(True)
+    mesh.cycles(profile_cycles)
+    prof = mesh.profile_read(reset=True)
+    mesh.profile(False)
+    fofc, _ = mesh.counters()
+    return mesh, {"ms": ms, "ms_max": ms_max, "launches": launches, "clock": ck, "prof": prof,
+                  "clocks": sampler.summary() if sampler else None, "fofc": fofc}
+
+
+def e2e_host(mesh, ics_state, steps, warmup, dist):
+    """zone-updates/s through the host-buffer C-ABI call: each step uploads the state from
+    pinned host memory, primes it, runs one cycle and downloads the new state."""
+    from chasqui_b200 import PinnedArray
+    pins = [PinnedArray(a.shape) for a in ics_state]
+    for p, a in zip(pins, ics_state):
+        p.array[...] = a
+    arrs = [p.array for p in pins]
+    for _ in range(max(1, warmup)):
+        mesh.run_host(*arrs, 1)
+    barrier(dist)
+    times = []
+    for _ in range(steps):
+        mesh.record(2)
+        mesh.run_host(*arrs, 1)
+        mesh.record(3)
+        times.append(mesh.elapsed_ms(2, 3))
+    nbytes = sum(a.nbytes for a in arrs)
+    # one job through the same call: one upload, `steps` cycles, one download
+    mesh.record(4)
+    mesh.run_host(*arrs, steps)
+    mesh.record(5)
+    job_ms = mesh.elapsed_ms(4, 5)
+    del arrs, pins
+    return times, nbytes, job_ms
+
+
+def cpu_reference(n: int, warmup: int, max_steps: int, budget_s: float, threads: int):
+    """The reference's own kernels (oracle/_ref, OpenMP) on the host cores: blast with
+    noise at n^3, timed per cycle."""
+    from chasqui_b200 import ics
+    from oracle.refsim import RefSim, available
+    if not available():
+        return None
+    g, u, b1, b2, b3 = ics.blast_noise(n)
+    text = f"""[mesh]
+nx1 = {n}
+nx2 = {n}
+nx3 = {n}
+x1min = -0.5
+x1max = 0.5
+x2min = -0.5
+x2max = 0.5
+x3min = -0.5
+x3max = 0.5
+[time]
+integrator = rk3
+cfl = 0.3
+tlim = 0.2
+[mhd]
+reconstruct = ppm
+rsolver = hlld
+[problem]
+name = blast
+"""
+    with tempfile.TemporaryDirectory() as d:
+        rst = os.path.join(d, "ic.rst")
+        ics.write_restart(rst, g, u, b1, b2, b3)
+        sim = RefSim(text, [], restart=rst, threads=threads)
+    for _ in range(warmup):
+        sim.cycles(1)
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max_steps:
+        t0 = time.perf_counter()
+        sim.cycles(1)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s and len(times) >= 1:
+            break
+    sim.close()
+    return times
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------------------
+def main_reference(args, rank):
+    if rank != 0:
+        return 0
+    threads = host_threads()
+    n = args.cpu_n
+    times = cpu_reference(n, args.warmup, args.steps, 1e9, threads)
+    if times is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (make -C oracle)"}))
+        return 0
+    per = statistics.mean(times)
+    v = n ** 3 / per
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"blast3d {n}^3 noise, ppm+hlld+rk3, fofc (bounded sample of the 512^3 workload)",
+                   "note": "reference kernels, shim OpenMP dispatch"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"blast3d {n}^3 with 1e-3 noise, {len(times)} RK3 cycles after {args.warmup} warm-up"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="chasqui", choices=["chasqui", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--cpu-n", type=int, default=128)
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+    rank, local = env_int("RANK", 0), env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return main_reference(args, rank)
+
+    from chasqui_b200 import ics, set_device
+    dist = dist_init()
+    world = env_int("WORLD_SIZE", 1)
+    set_device(local)
+    n = args.n
+    g, u, b1, b2, b3 = ics.blast_noise(n)
+    state = (u, b1, b2, b3)
+    hbm, peak_kind = peaks()
+
+    mesh, r64 = run_form(n, 0, state, args.steps, args.warmup, dist, local, sample_clocks=True)
+    zones = float(n) ** 3
+    value = world * zones * args.steps / (r64["ms_max"] / 1e3)
+    ms_step = r64["ms_max"] / args.steps
+    prof = r64["prof"]
+    k1_ms, k1_n = prof["fluxes"]
+    k1_avg_s = (k1_ms / max(k1_n, 1)) / 1e3
+    k1_gbs = BYTES_K1["fp64"] * zones / k1_avg_s / 1e9
+    step_gbs = (zones * args.steps / (r64["ms"] / 1e3)) * 3 * BYTES_STEP["fp64"] / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("fluxes_fp64_per_launch_bytes")
+    e2e = None
+    if not args.no_e2e:
+        times, nbytes, job_ms = e2e_host(mesh, state, args.steps, args.warmup, dist)
+        per = dist_max(dist, statistics.mean(times))
+        job = dist_max(dist, job_ms)
+        e2e = {"value": world * zones / (per / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "ms_per_step": per,
+               "call": "chq_run_host(pinned host state -> prime -> 1 cycle -> host state)",
+               "job": {"value": world * zones * args.steps / (job / 1e3), "cycles_per_call": args.steps,
+                       "h2d_bytes": nbytes, "d2h_bytes": nbytes}}
+    mesh.close()
+    del mesh
+
+    mixed = None
+    if not args.no_mixed:
+        meshm, rm = run_form(n, 1, state, args.steps, args.warmup, dist, local)
+        vm = world * zones * args.steps / (rm["ms_max"] / 1e3)
+        pm = rm["prof"]
+        km, kn = pm["fluxes"]
+        mixed = {"value": vm, "ms_per_step": rm["ms_max"] / args.steps,
+                 "hbm_frac_step": (zones * args.steps / (rm["ms"] / 1e3)) * 3 * BYTES_STEP["mixed"] / 1e9 / hbm,
+                 "k1_gbs": BYTES_K1["mixed"] * zones / ((km / max(kn, 1)) / 1e3) / 1e9,
+                 "speedup_vs_fp64": vm / value,
+                 "kernel_ms_per_step": {k: v[0] / 2 for k, v in pm.items()}}
+        meshm.close()
+        del meshm
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = host_threads()
+        times = cpu_reference(args.cpu_n, 1, 20, 15.0, threads)
+        if times:
+            cpu = {"value": args.cpu_n ** 3 / statistics.mean(times), "unit": UNIT, "cores": threads,
+                   "kind": "reference",
+                   "sample": f"blast3d {args.cpu_n}^3 with 1e-3 noise, {len(times)} RK3 cycles, OpenMP on all host threads"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"blast3d {n}^3 ppm+hlld+rk3 fofc flatten, seeded 1e-3 density noise, FP64 form",
+                       "cells": int(zones), "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "state (~67 GB) >> L2; no flush needed"},
+            "hbm_frac_step": step_gbs / hbm,
+            "roofline": {"bound": "hbm", "achieved": k1_gbs, "peak": hbm, "unit": "GB/s", "frac": k1_gbs / hbm,
+                         "traffic": traffic, "kernel": "flux_kernel (K1, all 3 directions, one launch)",
+                         "peak_kind": peak_kind, "bytes_per_cell": BYTES_K1["fp64"]},
+            "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},
+            "gpu_launches": r64["launches"],
+            "clocks": r64["clocks"],
+            "fofc_corrections": r64["fofc"],
+            "e2e": e2e,
+            "mixed": mixed,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,35 @@
+// chasqui_b200 — device-resident time-step control.
+//
+// The reference returns dt and the FOFC count to the host at every stage (src/main.cpp:247,
+// src/fofc.hpp:17-43), which forces a host synchronisation per stage. Here both stay in
+// device memory: kernels read this cycle's beta*dt from StepCtl and accumulate the FOFC and
+// limiter counts into it, so whole cycles run back to back (and can be graph-captured)
+// without the host. The host reads StepCtl only when asked.
+#pragma once
+#include "chq_common.cuh"
+
+namespace chq {
+
+struct StepCtl {
+  double t, tlim, cfl, dt;
+  double min_dt;                 // last completed dt reduction (before cfl)
+  double beta_dt[4];             // beta_s * dt of each stage of the current cycle
+  double beta[4], g0[4], g1[4];  // integrator table, written once by the host
+  unsigned long long mdt_bits;   // running min of the c2p dt reduction (positive doubles order as integers)
+  long long fofc_count, limiter_count;
+  int nbad;                      // cells flagged by the FOFC test in the current stage
+  int cycle, done, nstage, dt_pending;
+  int err;                       // nonzero: a kernel detected an invalid launch configuration
+};
+
+// Start of a cycle: dt = cfl * min_dt, clamped to reach tlim exactly (src/main.cpp:246-248).
+__global__ void ctl_begin_kernel(StepCtl *c, int nlim_left);
+// End of a cycle: t += dt, ++cycle, min_dt from this cycle's reduction (src/main.cpp:291-292).
+__global__ void ctl_end_kernel(StepCtl *c);
+
+CHQ_D void atomic_min_pos(unsigned long long *bits, double v) {
+  // non-negative doubles (and +inf / NaN above them) order like their bit patterns
+  atomicMin(bits, (unsigned long long)__double_as_longlong(v));
+}
+
+}  // namespace chq

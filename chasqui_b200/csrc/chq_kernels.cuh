@@ -1,0 +1,583 @@
+// chasqui_b200 — the stage kernels other than the face fluxes:
+//   K2  corner_emf_kernel   upwind edge EMFs (Gardiner & Stone 2005)   src/physics.hpp:228-297
+//   K3  update_kernel       RK combination + flux divergence + CT     src/physics.hpp:299-348
+//       fofc_flag_kernel    FOFC test of the tentative state + count   src/fofc.hpp:17-43
+//       fofc_repair_kernel  DC + HLLE fluxes on faces of flagged cells  src/fofc.hpp:46-95
+//       limit_kernel        Hu-Adams-Shu positivity flux limiter        src/positivity.hpp:25-88
+//   K4  bc_kernel<dir>      periodic / outflow / reflect ghost fill     src/physics.hpp:354-432
+//   K5  c2p_kernel          con2prim + centred B + cell EMF + dt min    src/physics.hpp:437-494
+//       history kernels     the .hst sums and div B                     src/output.hpp:91-119
+// P is the storage/arithmetic type of primitives, fluxes and EMFs (double in the FP64 form,
+// float in the mixed form); conserved variables and face fields are always double.
+#pragma once
+#include "chq_common.cuh"
+#include "chq_riemann.cuh"
+#include "chq_ctl.cuh"
+
+namespace chq {
+
+// ---------------------------------------------------------------------------------------
+// K2
+template <class P> struct EmfArgs {
+  Geom g;
+  const P *f1, *f2, *f3;                           // mass flux = component 0 of each
+  const P *e2x1, *e3x1, *e1x2, *e3x2, *e1x3, *e2x3;
+  const P *ecc;
+  P *e1, *e2, *e3;
+  const int *done;   // skip when nonzero
+  const int *need;   // run only when *need != 0 (FOFC re-run); null = always
+};
+
+template <class P> CHQ_D P upwind(P flux, P left, P right) {
+  const P tol = P(1e-14);
+  return (flux > tol) ? left : (flux < -tol) ? right : P(0.5) * (left + right);
+}
+
+template <class P> __global__ void __launch_bounds__(256) corner_emf_kernel(const EmfArgs<P> A) {
+  if (A.done && *A.done) return;
+  if (A.need && *A.need == 0) return;
+  const Geom &g = A.g;
+  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = g.ks + blockIdx.z;
+  const long vs = g.vstride;
+  const long sj = g.sj, sk = g.sk;
+  if (i > g.ie + 1) return;
+  const long l = g.idx(k, j, i);
+  if (g.three_d) {
+    if (j > g.je + 1 || k > g.ke + 1) return;
+    const P *c0 = A.ecc, *c1 = A.ecc + vs, *c2 = A.ecc + 2 * vs;
+    if (i <= g.ie) {   // E1 on x1-edges (k-1/2, j-1/2, i)
+      const P l3 = upwind(ldg(A.f2 + l - sk), ldg(A.e1x3 + l - sj) - ldg(c0 + l - sk - sj), ldg(A.e1x3 + l) - ldg(c0 + l - sk));
+      const P r3 = upwind(ldg(A.f2 + l), ldg(A.e1x3 + l - sj) - ldg(c0 + l - sj), ldg(A.e1x3 + l) - ldg(c0 + l));
+      const P l2 = upwind(ldg(A.f3 + l - sj), ldg(A.e1x2 + l - sk) - ldg(c0 + l - sk - sj), ldg(A.e1x2 + l) - ldg(c0 + l - sj));
+      const P r2 = upwind(ldg(A.f3 + l), ldg(A.e1x2 + l - sk) - ldg(c0 + l - sk), ldg(A.e1x2 + l) - ldg(c0 + l));
+      A.e1[l] = P(0.25) * (((l3 + r3) + (l2 + r2)) + ((ldg(A.e1x2 + l - sk) + ldg(A.e1x2 + l)) + (ldg(A.e1x3 + l - sj) + ldg(A.e1x3 + l))));
+    }
+    if (j <= g.je) {   // E2 on x2-edges (k-1/2, j, i-1/2)
+      const P l3 = upwind(ldg(A.f1 + l - sk), ldg(A.e2x3 + l - 1) - ldg(c1 + l - sk - 1), ldg(A.e2x3 + l) - ldg(c1 + l - sk));
+      const P r3 = upwind(ldg(A.f1 + l), ldg(A.e2x3 + l - 1) - ldg(c1 + l - 1), ldg(A.e2x3 + l) - ldg(c1 + l));
+      const P l1 = upwind(ldg(A.f3 + l - 1), ldg(A.e2x1 + l - sk) - ldg(c1 + l - sk - 1), ldg(A.e2x1 + l) - ldg(c1 + l - 1));
+      const P r1 = upwind(ldg(A.f3 + l), ldg(A.e2x1 + l - sk) - ldg(c1 + l - sk), ldg(A.e2x1 + l) - ldg(c1 + l));
+      A.e2[l] = P(0.25) * (((l3 + r3) + (l1 + r1)) + ((ldg(A.e2x3 + l - 1) + ldg(A.e2x3 + l)) + (ldg(A.e2x1 + l - sk) + ldg(A.e2x1 + l))));
+    }
+    if (k <= g.ke) {   // E3 on x3-edges (k, j-1/2, i-1/2)
+      const P l2 = upwind(ldg(A.f1 + l - sj), ldg(A.e3x2 + l - 1) - ldg(c2 + l - sj - 1), ldg(A.e3x2 + l) - ldg(c2 + l - sj));
+      const P r2 = upwind(ldg(A.f1 + l), ldg(A.e3x2 + l - 1) - ldg(c2 + l - 1), ldg(A.e3x2 + l) - ldg(c2 + l));
+      const P l1 = upwind(ldg(A.f2 + l - 1), ldg(A.e3x1 + l - sj) - ldg(c2 + l - sj - 1), ldg(A.e3x1 + l) - ldg(c2 + l - 1));
+      const P r1 = upwind(ldg(A.f2 + l), ldg(A.e3x1 + l - sj) - ldg(c2 + l - sj), ldg(A.e3x1 + l) - ldg(c2 + l));
+      A.e3[l] = P(0.25) * (((l2 + r2) + (l1 + r1)) + ((ldg(A.e3x2 + l - 1) + ldg(A.e3x2 + l)) + (ldg(A.e3x1 + l - sj) + ldg(A.e3x1 + l))));
+    }
+  } else {
+    // 2D / 1D: E1 and E2 live on x3-edges that coincide with the x2- and x1-faces
+    if (j > g.je + 1) return;
+    const P a = ldg(A.e1x2 + l), b = ldg(A.e2x1 + l);
+    A.e1[l] = a; A.e1[l + sk] = a;
+    A.e2[l] = b; A.e2[l + sk] = b;
+    if (!g.two_d) {
+      if (j == g.js) {
+        const P c = ldg(A.e3x1 + l);
+        A.e3[l] = c;
+        A.e3[l + sj] = c;
+      }
+    } else {
+      const P *c2 = A.ecc + 2 * vs;
+      const P l2 = upwind(ldg(A.f1 + l - sj), ldg(A.e3x2 + l - 1) - ldg(c2 + l - sj - 1), ldg(A.e3x2 + l) - ldg(c2 + l - sj));
+      const P r2 = upwind(ldg(A.f1 + l), ldg(A.e3x2 + l - 1) - ldg(c2 + l - 1), ldg(A.e3x2 + l) - ldg(c2 + l));
+      const P l1 = upwind(ldg(A.f2 + l - 1), ldg(A.e3x1 + l - sj) - ldg(c2 + l - sj - 1), ldg(A.e3x1 + l) - ldg(c2 + l - 1));
+      const P r1 = upwind(ldg(A.f2 + l), ldg(A.e3x1 + l - sj) - ldg(c2 + l - sj), ldg(A.e3x1 + l) - ldg(c2 + l));
+      A.e3[l] = P(0.25) * (((l2 + r2) + (l1 + r1)) + ((ldg(A.e3x2 + l - 1) + ldg(A.e3x2 + l)) + (ldg(A.e3x1 + l - sj) + ldg(A.e3x1 + l))));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// K3. Each thread owns one (k, j, i) of the face/edge frame: the cell update when (k, j, i)
+// is an active cell and the x1/x2/x3 face updates when it is an active face. The reads of
+// ua/ub/b?a/b?b precede this thread's writes to the same elements and no other thread
+// touches them, so the RK aliasing of out with a or b is safe.
+template <class P> struct UpdateArgs {
+  Geom g;
+  EOSp eos;
+  const P *f1, *f2, *f3, *e1, *e2, *e3;
+  const double *ua, *ub;
+  double *uout;
+  const double *b1a, *b2a, *b3a, *b1b, *b2b, *b3b;
+  double *b1o, *b2o, *b3o;
+  double g0, g1, beta_dt;    // used when beta_dt_dev is null
+  const double *beta_dt_dev; // device beta*dt of this stage (StepCtl::beta_dt[s])
+  double idx1, idx2, idx3;
+  const int *done;
+  const int *need;           // run only when *need != 0 (FOFC re-run); null = always
+};
+
+// new face fields; curl of the edge EMFs (src/physics.hpp:327-347)
+template <class P> CHQ_D double new_b1(const UpdateArgs<P> &A, long l, double g0, double g1, double bdt) {
+  const Geom &g = A.g;
+  double curl = 0.0;
+  if (g.two_d) curl += ((double)ldg(A.e3 + l + g.sj) - (double)ldg(A.e3 + l)) * A.idx2;
+  if (g.three_d) curl -= ((double)ldg(A.e2 + l + g.sk) - (double)ldg(A.e2 + l)) * A.idx3;
+  return g0 * A.b1a[l] + g1 * A.b1b[l] - bdt * curl;
+}
+template <class P> CHQ_D double new_b2(const UpdateArgs<P> &A, long l, double g0, double g1, double bdt) {
+  const Geom &g = A.g;
+  double curl = -((double)ldg(A.e3 + l + 1) - (double)ldg(A.e3 + l)) * A.idx1;
+  if (g.three_d) curl += ((double)ldg(A.e1 + l + g.sk) - (double)ldg(A.e1 + l)) * A.idx3;
+  return g0 * A.b2a[l] + g1 * A.b2b[l] - bdt * curl;
+}
+template <class P> CHQ_D double new_b3(const UpdateArgs<P> &A, long l, double g0, double g1, double bdt) {
+  const Geom &g = A.g;
+  double curl = ((double)ldg(A.e2 + l + 1) - (double)ldg(A.e2 + l)) * A.idx1;
+  if (g.two_d) curl -= ((double)ldg(A.e1 + l + g.sj) - (double)ldg(A.e1 + l)) * A.idx2;
+  return g0 * A.b3a[l] + g1 * A.b3b[l] - bdt * curl;
+}
+
+template <class P> __global__ void __launch_bounds__(256) update_kernel(const UpdateArgs<P> A) {
+  if (A.done && *A.done) return;
+  if (A.need && *A.need == 0) return;
+  const Geom &g = A.g;
+  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = g.ks + blockIdx.z;
+  if (i > g.ie + 1 || j > g.je + 1 || k > g.ke + 1) return;
+  const double g0 = A.g0, g1 = A.g1;
+  const double bdt = A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt;
+  const long l = g.idx(k, j, i);
+  const long vs = g.vstride;
+  const bool cell = (i <= g.ie && j <= g.je && k <= g.ke);
+  double un[NVAR];
+  if (cell) {
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) {
+      const long ln = n * vs + l;
+      double divf = ((double)ldg(A.f1 + ln + 1) - (double)ldg(A.f1 + ln)) * A.idx1;
+      if (g.two_d) divf += ((double)ldg(A.f2 + ln + g.sj) - (double)ldg(A.f2 + ln)) * A.idx2;
+      if (g.three_d) divf += ((double)ldg(A.f3 + ln + g.sk) - (double)ldg(A.f3 + ln)) * A.idx3;
+      un[n] = g0 * A.ua[ln] + g1 * A.ub[ln] - bdt * divf;
+    }
+  }
+  double nb1 = 0, nb2 = 0, nb3 = 0;
+  if (j <= g.je && k <= g.ke) nb1 = new_b1(A, l, g0, g1, bdt);
+  if (i <= g.ie && k <= g.ke && (g.two_d || j == g.js)) nb2 = new_b2(A, l, g0, g1, bdt);
+  if (i <= g.ie && j <= g.je && (g.three_d || k == g.ks)) nb3 = new_b3(A, l, g0, g1, bdt);
+  if (cell) {
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) A.uout[n * vs + l] = un[n];
+  }
+  if (j <= g.je && k <= g.ke) A.b1o[l] = nb1;
+  if (i <= g.ie && k <= g.ke && (g.two_d || j == g.js)) {
+    A.b2o[l] = nb2;
+    if (!g.two_d) A.b2o[l + g.sj] = nb2;
+  }
+  if (i <= g.ie && j <= g.je && (g.three_d || k == g.ks)) {
+    A.b3o[l] = nb3;
+    if (!g.three_d) A.b3o[l + g.sk] = nb3;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// FOFC flag of the tentative state (src/fofc.hpp:17-43): rho <= dfloor or p <= pfloor,
+// written for every active cell, with a warp-aggregated count into *nbad.
+struct FlagArgs {
+  Geom g;
+  EOSp eos;
+  const double *u, *b1, *b2, *b3;
+  int *flag;
+  int *nbad;
+  const int *done;
+};
+
+__global__ void __launch_bounds__(256) fofc_flag_kernel(const FlagArgs A) {
+  if (A.done && *A.done) return;
+  const Geom &g = A.g;
+  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = g.ks + blockIdx.z;
+  int bad = 0;
+  if (i <= g.ie && j <= g.je) {
+    const long vs = g.vstride;
+    const long l = g.idx(k, j, i);
+    const double bx = 0.5 * (A.b1[l] + A.b1[l + 1]);
+    const double by = g.two_d ? 0.5 * (A.b2[l] + A.b2[l + g.sj]) : A.b2[l];
+    const double bz = g.three_d ? 0.5 * (A.b3[l] + A.b3[l + g.sk]) : A.b3[l];
+    const double d = A.u[IDN * vs + l];
+    bool b = (d <= A.eos.dfloor);
+    if (!b) {
+      const double ke = 0.5 * (sqr(A.u[IM1 * vs + l]) + sqr(A.u[IM2 * vs + l]) + sqr(A.u[IM3 * vs + l])) / d;
+      const double eint = A.u[IEN * vs + l] - ke - 0.5 * (bx * bx + by * by + bz * bz);
+      double p = A.eos.gm1 * eint;
+      if (A.eos.dual_energy && eint < A.eos.de_eta * fabs(A.u[IEN * vs + l]))
+        p = (A.u[IENT * vs + l] / d) * pow(d, A.eos.gamma);
+      b = (p <= A.eos.pfloor);
+    }
+    bad = b ? 1 : 0;
+    A.flag[l] = bad;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, bad != 0);
+  if (m && (threadIdx.x & 31) == 0) atomicAdd(A.nbad, __popc(m));
+}
+
+// ---------------------------------------------------------------------------------------
+// FOFC repair: first-order (donor cell) HLLE fluxes on faces touching a flagged cell,
+// from the stage-start primitives (src/fofc.hpp:46-95). One launch, all directions.
+template <class P> struct RepairArgs {
+  Geom g;
+  EOSp eos;
+  const P *w, *bcc;
+  const double *bn[3];
+  P *flx[3], *et2[3], *et1[3];
+  const int *flag;
+  int lo[3][3], hi[3][3];   // flux face ranges per direction (k, j, i)
+  long nface[3];
+  const int *done;
+  const int *need;
+};
+
+template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k, int j, int i) {
+  const Geom &g = A.g;
+  constexpr int IVU = IVX + DIR, IVV = IVX + (DIR + 1) % 3, IVW = IVX + (DIR + 2) % 3;
+  constexpr int IBT1 = (DIR + 1) % 3, IBT2 = (DIR + 2) % 3;
+  const int kL = k - (DIR == 2), jL = j - (DIR == 1), iL = i - (DIR == 0);
+  auto inside = [&](int kk, int jj, int ii) {
+    return (ii >= g.is && ii <= g.ie && jj >= g.js && jj <= g.je && kk >= g.ks && kk <= g.ke);
+  };
+  const long l = g.idx(k, j, i), lL = g.idx(kL, jL, iL);
+  const bool fr = inside(k, j, i) && A.flag[l];
+  const bool fl = inside(kL, jL, iL) && A.flag[lL];
+  if (!(fl || fr)) return;
+  const long vs = g.vstride;
+  MState<P> L{A.w[IDN * vs + lL], A.w[IVU * vs + lL], A.w[IVV * vs + lL], A.w[IVW * vs + lL], A.w[IPR * vs + lL],
+              A.bcc[IBT1 * vs + lL], A.bcc[IBT2 * vs + lL]};
+  MState<P> R{A.w[IDN * vs + l], A.w[IVU * vs + l], A.w[IVV * vs + l], A.w[IVW * vs + l], A.w[IPR * vs + l],
+              A.bcc[IBT1 * vs + l], A.bcc[IBT2 * vs + l]};
+  P f[NFLX];
+  hlle(L, R, P(A.bn[DIR][l]), P(A.eos.gamma), P(A.eos.gm1), f);
+  P *flx = A.flx[DIR];
+  flx[IDN * vs + l] = f[FD];
+  flx[IVU * vs + l] = f[FMU];
+  flx[IVV * vs + l] = f[FMV];
+  flx[IVW * vs + l] = f[FMW];
+  flx[IEN * vs + l] = f[FEN];
+  const P sL = A.w[IENT * vs + lL], sR = A.w[IENT * vs + l];
+  flx[IENT * vs + l] = (f[FD] > P(0)) ? f[FD] * sL : (f[FD] < P(0)) ? f[FD] * sR : P(0.5) * (f[FD] * (sL + sR));
+  A.et2[DIR][l] = -f[FBY];
+  A.et1[DIR][l] = f[FBZ];
+}
+
+template <class P> __global__ void __launch_bounds__(256) fofc_repair_kernel(const RepairArgs<P> A) {
+  if (A.done && *A.done) return;
+  if (A.need && *A.need == 0) return;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (t < A.nface[d]) {
+      const int ni = A.hi[d][2] - A.lo[d][2] + 1, nj = A.hi[d][1] - A.lo[d][1] + 1;
+      const int i = A.lo[d][2] + (int)(t % ni);
+      const long r = t / ni;
+      const int j = A.lo[d][1] + (int)(r % nj);
+      const int k = A.lo[d][0] + (int)(r / nj);
+      if (d == 0) repair_face<0, P>(A, k, j, i);
+      else if (d == 1) repair_face<1, P>(A, k, j, i);
+      else repair_face<2, P>(A, k, j, i);
+      return;
+    }
+    t -= A.nface[d];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Positivity flux limiter (Hu, Adams & Shu 2013) on the active faces of each direction.
+template <class P> struct LimitArgs {
+  Geom g;
+  EOSp eos;
+  const P *w, *bcc;
+  P *flx[3];
+  double two_ndim;              // 2 * ndim
+  double dx[3];
+  double beta_dt;
+  const double *beta_dt_dev;
+  int lo[3][3], hi[3][3];
+  long nface[3];
+  long long *count;
+  const int *done;
+};
+
+template <class P> CHQ_D void cell_flux6(const MState<P> &s, P bn, P sent, P gm1, P gamma, P fc[6], P uc[6], P &cf) {
+  P f[NFLX], e, pt;
+  phys_flux(s, bn, gm1, e, pt, f);
+  fc[0] = f[FD]; fc[1] = f[FMU]; fc[2] = f[FMV]; fc[3] = f[FMW]; fc[4] = f[FEN]; fc[5] = f[FD] * sent;
+  uc[0] = s.d; uc[1] = s.d * s.u; uc[2] = s.d * s.v; uc[3] = s.d * s.w; uc[4] = e; uc[5] = s.d * sent;
+  cf = fast_speed(s, bn, gamma);
+}
+
+template <int DIR, class P> CHQ_D int limit_face(const LimitArgs<P> &A, int k, int j, int i, double bdt) {
+  const Geom &g = A.g;
+  constexpr int IVU = IVX + DIR, IVV = IVX + (DIR + 1) % 3, IVW = IVX + (DIR + 2) % 3;
+  constexpr int IBT1 = (DIR + 1) % 3, IBT2 = (DIR + 2) % 3;
+  const long vs = g.vstride;
+  const int kL = k - (DIR == 2), jL = j - (DIR == 1), iL = i - (DIR == 0);
+  const long l = g.idx(k, j, i), lL = g.idx(kL, jL, iL);
+  const P gamma = P(A.eos.gamma), gm1 = P(A.eos.gm1);
+  // lam2 = 2 ndim beta_dt / dx, in the reference's order ((2*ndim)*beta_dt)/dx
+  const P lam2 = P((A.two_ndim * bdt) / A.dx[DIR]);
+  MState<P> L{A.w[IDN * vs + lL], A.w[IVU * vs + lL], A.w[IVV * vs + lL], A.w[IVW * vs + lL], A.w[IPR * vs + lL],
+              A.bcc[IBT1 * vs + lL], A.bcc[IBT2 * vs + lL]};
+  MState<P> R{A.w[IDN * vs + l], A.w[IVU * vs + l], A.w[IVV * vs + l], A.w[IVW * vs + l], A.w[IPR * vs + l],
+              A.bcc[IBT1 * vs + l], A.bcc[IBT2 * vs + l]};
+  const P bnL = A.bcc[DIR * vs + lL], bnR = A.bcc[DIR * vs + l];
+  P fL[6], fR[6], uL[6], uR[6], cfL, cfR;
+  cell_flux6(L, bnL, A.w[IENT * vs + lL], gm1, gamma, fL, uL, cfL);
+  cell_flux6(R, bnR, A.w[IENT * vs + l], gm1, gamma, fR, uR, cfR);
+  const P alpha = fmax_(fabs_(L.u) + cfL, fabs_(R.u) + cfR);
+  const int nv[6] = {IDN, IVU, IVV, IVW, IEN, IENT};
+  P fho[6], flf[6];
+  P *flx = A.flx[DIR];
+#pragma unroll
+  for (int n = 0; n < 6; ++n) {
+    fho[n] = flx[nv[n] * vs + l];
+    flf[n] = P(0.5) * (fL[n] + fR[n]) - P(0.5) * (alpha * (uR[n] - uL[n]));
+  }
+  const P emL = P(0.5) * (bnL * bnL + L.by * L.by + L.bz * L.bz);
+  const P emR = P(0.5) * (bnR * bnR + R.by * R.by + R.bz * R.bz);
+  const P dfl = P(A.eos.dfloor), pfl = P(A.eos.pfloor), deta = P(A.eos.de_eta);
+  auto ok = [&](P th) {
+    P f[6];
+#pragma unroll
+    for (int n = 0; n < 6; ++n) f[n] = flf[n] + th * (fho[n] - flf[n]);
+    P a[5], b[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      a[n] = uL[n] - lam2 * (f[n] - fL[n]);
+      b[n] = uR[n] + lam2 * (f[n] - fR[n]);
+    }
+    if (a[0] < dfl || b[0] < dfl) return false;
+    const P ea = a[4] - P(0.5) * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) / a[0] - emL;
+    const P eb = b[4] - P(0.5) * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]) / b[0] - emR;
+    P pa = gm1 * ea, pb = gm1 * eb;
+    if (A.eos.dual_energy) {
+      const P sa = (uL[5] - lam2 * (f[5] - fL[5])) / a[0], sb = (uR[5] + lam2 * (f[5] - fR[5])) / b[0];
+      if (ea < deta * fabs_(a[4])) pa = sa * P(pow((double)a[0], A.eos.gamma));
+      if (eb < deta * fabs_(b[4])) pb = sb * P(pow((double)b[0], A.eos.gamma));
+    }
+    return (pa >= pfl && pb >= pfl);
+  };
+  if (ok(P(1))) return 0;
+  P lo = P(0), hi = P(1);
+  for (int it = 0; it < 12; ++it) {
+    const P mid = P(0.5) * (lo + hi);
+    if (ok(mid)) lo = mid; else hi = mid;
+  }
+  const P th = lo;
+#pragma unroll
+  for (int n = 0; n < 6; ++n) flx[nv[n] * vs + l] = flf[n] + th * (fho[n] - flf[n]);
+  return 1;
+}
+
+template <class P> __global__ void __launch_bounds__(256) limit_kernel(const LimitArgs<P> A) {
+  if (A.done && *A.done) return;
+  const double bdt = A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int lim = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (t >= 0 && t < A.nface[d]) {
+      const int ni = A.hi[d][2] - A.lo[d][2] + 1, nj = A.hi[d][1] - A.lo[d][1] + 1;
+      const int i = A.lo[d][2] + (int)(t % ni);
+      const long r = t / ni;
+      const int j = A.lo[d][1] + (int)(r % nj);
+      const int k = A.lo[d][0] + (int)(r / nj);
+      if (d == 0) lim = limit_face<0, P>(A, k, j, i, bdt);
+      else if (d == 1) lim = limit_face<1, P>(A, k, j, i, bdt);
+      else lim = limit_face<2, P>(A, k, j, i, bdt);
+      t = -1;
+    } else if (t >= 0) {
+      t -= A.nface[d];
+    }
+  }
+  const unsigned m = __ballot_sync(__activemask(), lim != 0);
+  if (m && (threadIdx.x & 31) == (__ffs(__activemask()) - 1)) atomicAdd((unsigned long long *)A.count, (unsigned long long)__popc(m));
+}
+
+// ---------------------------------------------------------------------------------------
+// K4 ghost fill; DIR selects the x1, x2 or x3 slabs. Must run x1, x2, x3 in order.
+struct BcArgs {
+  Geom g;
+  double *u, *b1, *b2, *b3;
+  int bc;
+  const int *done;
+};
+
+template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs A) {
+  if (A.done && *A.done) return;
+  const Geom &g = A.g;
+  const long vs = g.vstride;
+  const double sgn = (A.bc == BC_REFLECT) ? -1.0 : 1.0;
+  if (DIR == 0) {
+    // threads over (k in [0,nk], j in [0,nj], gh in [0,ng))
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int gh = (int)(t % g.ng);
+    const long r = t / g.ng;
+    const int j = (int)(r % (g.nj + 1));
+    const int k = (int)(r / (g.nj + 1));
+    if (k > g.nk) return;
+    const int il = gh, ir = g.ie + 1 + gh;
+    const int srcl = (A.bc == 0) ? il + g.nx1 : (A.bc == 1) ? g.is : 2 * g.is - 1 - il;
+    const int srcr = (A.bc == 0) ? ir - g.nx1 : (A.bc == 1) ? g.ie : 2 * g.ie + 1 - ir;
+    const long row = g.idx(k, j, 0);
+    if (k < g.nk && j < g.nj) {
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) {
+        const double f = (n == IM1) ? sgn : 1.0;
+        A.u[n * vs + row + il] = f * A.u[n * vs + row + srcl];
+        A.u[n * vs + row + ir] = f * A.u[n * vs + row + srcr];
+      }
+      A.b2[row + il] = A.b2[row + srcl]; A.b2[row + ir] = A.b2[row + srcr];
+      A.b3[row + il] = A.b3[row + srcl]; A.b3[row + ir] = A.b3[row + srcr];
+    }
+    const int fl = gh, fr = g.ie + 2 + gh;
+    if (A.bc == 0) { A.b1[row + fl] = A.b1[row + fl + g.nx1]; A.b1[row + fr] = A.b1[row + fr - g.nx1]; }
+    else if (A.bc == 1) { A.b1[row + fl] = A.b1[row + g.is]; A.b1[row + fr] = A.b1[row + g.ie + 1]; }
+    else { A.b1[row + fl] = -A.b1[row + 2 * g.is - fl]; A.b1[row + fr] = -A.b1[row + 2 * (g.ie + 1) - fr]; }
+    if (A.bc == 0 && gh == 0) A.b1[row + g.ie + 1] = A.b1[row + g.is];
+  } else if (DIR == 1) {
+    // threads over (k in [0,nk], gh in [0,ng), i in [0,ni])
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t % (g.ni + 1));
+    const long r = t / (g.ni + 1);
+    const int gh = (int)(r % g.ng);
+    const int k = (int)(r / g.ng);
+    if (k > g.nk) return;
+    const int jl = gh, jr = g.je + 1 + gh;
+    const int srcl = (A.bc == 0) ? jl + g.nx2 : (A.bc == 1) ? g.js : 2 * g.js - 1 - jl;
+    const int srcr = (A.bc == 0) ? jr - g.nx2 : (A.bc == 1) ? g.je : 2 * g.je + 1 - jr;
+    const long ljl = g.idx(k, jl, i), ljr = g.idx(k, jr, i), lsl = g.idx(k, srcl, i), lsr = g.idx(k, srcr, i);
+    if (k < g.nk && i < g.ni) {
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) {
+        const double f = (n == IM2) ? sgn : 1.0;
+        A.u[n * vs + ljl] = f * A.u[n * vs + lsl];
+        A.u[n * vs + ljr] = f * A.u[n * vs + lsr];
+      }
+      A.b3[ljl] = A.b3[lsl]; A.b3[ljr] = A.b3[lsr];
+    }
+    if (k < g.nk) { A.b1[ljl] = A.b1[lsl]; A.b1[ljr] = A.b1[lsr]; }
+    const int fl = gh, fr = g.je + 2 + gh;
+    const long lfl = g.idx(k, fl, i), lfr = g.idx(k, fr, i);
+    if (A.bc == 0) { A.b2[lfl] = A.b2[g.idx(k, fl + g.nx2, i)]; A.b2[lfr] = A.b2[g.idx(k, fr - g.nx2, i)]; }
+    else if (A.bc == 1) { A.b2[lfl] = A.b2[g.idx(k, g.js, i)]; A.b2[lfr] = A.b2[g.idx(k, g.je + 1, i)]; }
+    else { A.b2[lfl] = -A.b2[g.idx(k, 2 * g.js - fl, i)]; A.b2[lfr] = -A.b2[g.idx(k, 2 * (g.je + 1) - fr, i)]; }
+    if (A.bc == 0 && gh == 0) A.b2[g.idx(k, g.je + 1, i)] = A.b2[g.idx(k, g.js, i)];
+  } else {
+    // threads over (gh in [0,ng), j in [0,nj], i in [0,ni])
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t % (g.ni + 1));
+    const long r = t / (g.ni + 1);
+    const int j = (int)(r % (g.nj + 1));
+    const int gh = (int)(r / (g.nj + 1));
+    if (gh >= g.ng) return;
+    const int kl = gh, kr = g.ke + 1 + gh;
+    const int srcl = (A.bc == 0) ? kl + g.nx3 : (A.bc == 1) ? g.ks : 2 * g.ks - 1 - kl;
+    const int srcr = (A.bc == 0) ? kr - g.nx3 : (A.bc == 1) ? g.ke : 2 * g.ke + 1 - kr;
+    const long lkl = g.idx(kl, j, i), lkr = g.idx(kr, j, i), lsl = g.idx(srcl, j, i), lsr = g.idx(srcr, j, i);
+    if (j < g.nj && i < g.ni) {
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) {
+        const double f = (n == IM3) ? sgn : 1.0;
+        A.u[n * vs + lkl] = f * A.u[n * vs + lsl];
+        A.u[n * vs + lkr] = f * A.u[n * vs + lsr];
+      }
+    }
+    A.b1[lkl] = A.b1[lsl]; A.b1[lkr] = A.b1[lsr];
+    A.b2[lkl] = A.b2[lsl]; A.b2[lkr] = A.b2[lsr];
+    const int fl = gh, fr = g.ke + 2 + gh;
+    const long lfl = g.idx(fl, j, i), lfr = g.idx(fr, j, i);
+    if (A.bc == 0) { A.b3[lfl] = A.b3[g.idx(fl + g.nx3, j, i)]; A.b3[lfr] = A.b3[g.idx(fr - g.nx3, j, i)]; }
+    else if (A.bc == 1) { A.b3[lfl] = A.b3[g.idx(g.ks, j, i)]; A.b3[lfr] = A.b3[g.idx(g.ke + 1, j, i)]; }
+    else { A.b3[lfl] = -A.b3[g.idx(2 * g.ks - fl, j, i)]; A.b3[lfr] = -A.b3[g.idx(2 * (g.ke + 1) - fr, j, i)]; }
+    if (A.bc == 0 && gh == 0) A.b3[g.idx(g.ke + 1, j, i)] = A.b3[g.idx(g.ks, j, i)];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// K5
+template <class P> struct C2pArgs {
+  Geom g;
+  EOSp eos;
+  double *u;
+  const double *b1, *b2, *b3;
+  P *w, *bcc, *ecc;
+  int compute_dt;
+  unsigned long long *mdt_bits;   // atomic min of dt over active cells
+  StepCtl *ctl;                   // when set: fold the FOFC count and reset it (block 0)
+  const int *done;
+};
+
+template <class P> __global__ void __launch_bounds__(256) c2p_kernel(const C2pArgs<P> A) {
+  if (A.done && *A.done) return;
+  const Geom &g = A.g;
+  if (A.ctl && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    A.ctl->fofc_count += A.ctl->nbad;
+    A.ctl->nbad = 0;
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double mdt = __longlong_as_double(0x7ff0000000000000LL);   // +inf
+  if (i < g.ni && j < g.nj && k < g.nk) {
+    const long vs = g.vstride;
+    const long l = g.idx(k, j, i);
+    const double bx = 0.5 * (A.b1[l] + A.b1[l + 1]);
+    const double by = g.two_d ? 0.5 * (A.b2[l] + A.b2[l + g.sj]) : A.b2[l];
+    const double bz = g.three_d ? 0.5 * (A.b3[l] + A.b3[l + g.sk]) : A.b3[l];
+    const EOSp &e = A.eos;
+    const double d = fmax(A.u[IDN * vs + l], e.dfloor);
+    const double id = 1.0 / d;
+    const double vx = A.u[IM1 * vs + l] * id, vy = A.u[IM2 * vs + l] * id, vz = A.u[IM3 * vs + l] * id;
+    const double bsq = bx * bx + by * by + bz * bz;
+    const double ke = 0.5 * d * (vx * vx + vy * vy + vz * vz);
+    const double etot = A.u[IEN * vs + l];
+    const double eint = etot - ke - 0.5 * bsq;
+    double p = e.gm1 * eint;
+    double sent = A.u[IENT * vs + l] * id;
+    if (e.dual_energy && eint < e.de_eta * fabs(etot)) {
+      p = sent * pow(d, e.gamma);
+      p = fmax(p, e.pfloor);
+      A.u[IEN * vs + l] = ke + 0.5 * bsq + p / e.gm1;
+    } else {
+      p = fmax(p, e.pfloor);
+      sent = p / pow(d, e.gamma);
+      A.u[IENT * vs + l] = d * sent;
+    }
+    A.w[IDN * vs + l] = P(d);
+    A.w[IVX * vs + l] = P(vx);
+    A.w[IVY * vs + l] = P(vy);
+    A.w[IVZ * vs + l] = P(vz);
+    A.w[IPR * vs + l] = P(p);
+    A.w[IENT * vs + l] = P(sent);
+    A.bcc[0 * vs + l] = P(bx);
+    A.bcc[1 * vs + l] = P(by);
+    A.bcc[2 * vs + l] = P(bz);
+    A.ecc[0 * vs + l] = P(vz * by - vy * bz);
+    A.ecc[1 * vs + l] = P(vx * bz - vz * bx);
+    A.ecc[2 * vs + l] = P(vy * bx - vx * by);
+    if (A.compute_dt && i >= g.is && i <= g.ie && j >= g.js && j <= g.je && k >= g.ks && k <= g.ke) {
+      const double gp = e.gamma * p;
+      const double a = (gp + bsq) * id;
+      auto cf = [&](double bn) {
+        const double disc = a * a - 4.0 * gp * bn * bn * id * id;
+        return sqrt(0.5 * (a + sqrt(fmax(disc, 0.0))));
+      };
+      double dt = g.dx1 / (fabs(vx) + cf(bx));
+      if (g.two_d) dt = fmin(dt, g.dx2 / (fabs(vy) + cf(by)));
+      if (g.three_d) dt = fmin(dt, g.dx3 / (fabs(vz) + cf(bz)));
+      mdt = dt;
+    }
+  }
+  if (A.compute_dt) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mdt = fmin(mdt, __shfl_xor_sync(0xffffffffu, mdt, o));
+    if ((threadIdx.x & 31) == 0) atomic_min_pos(A.mdt_bits, mdt);
+  }
+}
+
+}  // namespace chq

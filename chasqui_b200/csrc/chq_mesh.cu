@@ -1,0 +1,1034 @@
+// chasqui_b200 — device mesh, stage orchestration and the C ABI declared in include/chq.h.
+//
+// One chq_mesh owns every field of one simulation in a single device allocation, laid out
+// in the common padded frame described in chq_common.cuh. The stage sequence is the
+// reference's Stage() (src/main.cpp:46-93) with the host synchronisations removed: the
+// time step, the FOFC decision and all counters live in a device StepCtl.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "chq.h"
+#include "chq_common.cuh"
+#include "chq_ctl.cuh"
+#include "chq_kernels.cuh"
+#include "chq_launch.h"
+
+using namespace chq;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char *where) {
+  return fail(CHQ_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CHQ_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// device control kernels
+namespace chq {
+__global__ void ctl_begin_kernel(StepCtl *c, int) {
+  if (c->done) return;
+  if (!(c->t < c->tlim)) { c->done = 1; return; }
+  double dt = c->cfl * c->min_dt;
+  if (c->t + dt > c->tlim) dt = c->tlim - c->t;
+  c->dt = dt;
+  for (int s = 0; s < c->nstage; ++s) c->beta_dt[s] = c->beta[s] * dt;
+  c->mdt_bits = 0x7ff0000000000000ULL;
+}
+__global__ void ctl_end_kernel(StepCtl *c) {
+  if (c->done) return;
+  c->t += c->dt;
+  c->cycle += 1;
+  c->min_dt = __longlong_as_double((long long)c->mdt_bits);
+}
+__global__ void ctl_prime_kernel(StepCtl *c, double t) {
+  c->t = t;
+  c->done = 0;
+  c->cycle = 0;
+  c->nbad = 0;
+  c->fofc_count = 0;
+  c->limiter_count = 0;
+  c->mdt_bits = 0x7ff0000000000000ULL;
+}
+__global__ void ctl_take_dt_kernel(StepCtl *c) { c->min_dt = __longlong_as_double((long long)c->mdt_bits); }
+__global__ void reset_bits_kernel(unsigned long long *b) { *b = 0x7ff0000000000000ULL; }
+}  // namespace chq
+
+// ---------------------------------------------------------------------------------------
+// history: two-pass deterministic reduction (block partials in scratch, then one block)
+namespace chq {
+template <class P>
+__global__ void __launch_bounds__(256) hst_partial_kernel(Geom g, const double *u, const P *w, const P *bcc,
+                                                          const double *b1, const double *b2, const double *b3,
+                                                          double idx1, double idx2, double idx3, double *part) {
+  __shared__ double sm[10][8];
+  double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const long ncell = (long)g.nx1 * g.nx2 * g.nx3;
+  const long vs = g.vstride;
+  for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long)gridDim.x * blockDim.x) {
+    const int i = g.is + (int)(c % g.nx1);
+    const long r = c / g.nx1;
+    const int j = g.js + (int)(r % g.nx2);
+    const int k = g.ks + (int)(r / g.nx2);
+    const long l = g.idx(k, j, i);
+    const double d = (double)w[IDN * vs + l];
+    const double vx = (double)w[IVX * vs + l], vy = (double)w[IVY * vs + l], vz = (double)w[IVZ * vs + l];
+    const double bx = (double)bcc[l], by = (double)bcc[vs + l], bz = (double)bcc[2 * vs + l];
+    v[0] += u[IDN * vs + l];
+    v[1] += u[IM1 * vs + l];
+    v[2] += u[IM2 * vs + l];
+    v[3] += u[IM3 * vs + l];
+    v[4] += u[IEN * vs + l];
+    const double ek = 0.5 * d * (sqr(vx) + sqr(vy) + sqr(vz));
+    const double em = 0.5 * (sqr(bx) + sqr(by) + sqr(bz));
+    v[5] += ek;
+    v[6] += em;
+    v[7] += u[IEN * vs + l] - 0.5 * d * (sqr(vx) + sqr(vy) + sqr(vz)) - 0.5 * (sqr(bx) + sqr(by) + sqr(bz));
+    double db = (b1[l + 1] - b1[l]) * idx1;
+    if (g.two_d) db += (b2[l + g.sj] - b2[l]) * idx2;
+    if (g.three_d) db += (b3[l + g.sk] - b3[l]) * idx3;
+    v[8] = fmax(v[8], fabs(db));
+    v[9] += fabs(db);
+  }
+  // fixed-order tree: warp shuffles, then warps in order
+#pragma unroll
+  for (int q = 0; q < 10; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double x = __shfl_down_sync(0xffffffffu, v[q], o);
+      v[q] = (q == 8) ? fmax(v[q], x) : v[q] + x;
+    }
+  }
+  const int wid = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int q = 0; q < 10; ++q) sm[q][wid] = v[q];
+  __syncthreads();
+  if (threadIdx.x < 10) {
+    double s = sm[threadIdx.x][0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) s = (threadIdx.x == 8) ? fmax(s, sm[threadIdx.x][q]) : s + sm[threadIdx.x][q];
+    part[(long)blockIdx.x * 10 + threadIdx.x] = s;
+  }
+}
+__global__ void hst_final_kernel(const double *part, int nblk, double *out) {
+  const int q = threadIdx.x;
+  if (q >= 10) return;
+  double s = (q == 8) ? 0.0 : 0.0;
+  for (int b = 0; b < nblk; ++b) s = (q == 8) ? fmax(s, part[b * 10 + q]) : s + part[b * 10 + q];
+  out[q] = s;
+}
+}  // namespace chq
+
+// ---------------------------------------------------------------------------------------
+struct chq_mesh {
+  chq_config cfg;
+  Geom g;
+  EOSp eos;
+  int nstage;
+  int mixed;
+  size_t psize;            // bytes of one P element
+  cudaStream_t stream = nullptr;
+  char *slab = nullptr;
+  size_t slab_bytes = 0;
+  double *u[2];
+  double *bf[2][3];
+  void *w, *bcc, *ecc, *flx[3], *et2[3], *et1[3], *e[3];
+  int *flag;
+  StepCtl *ctl;            // device
+  double *hst_part, *hst_out;
+  int hst_blocks;
+  // flux launch geometry
+  int lo[3][3], hi[3][3], active[3];
+  int act_lo[3][3], act_hi[3][3];
+  int seglen;
+  // timing
+  cudaEvent_t slots[8] = {};
+  bool prof = false;
+  struct Pend { int kind; cudaEvent_t b, e; };
+  std::vector<Pend> pending;
+  std::vector<cudaEvent_t> pool;
+  long long nlaunch = 0;
+  double prof_ms[CHQ_NPROF] = {};
+  long long prof_n[CHQ_NPROF] = {};
+};
+
+namespace {
+
+const int kSeglen = 16;
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// reference stage table (src/main.cpp:250-268)
+void stage_table(int nstage, int s, double &g0, double &g1, double &beta, int &cur, int &out) {
+  if (nstage == 1) { g0 = 1; g1 = 0; beta = 1; cur = 0; out = 0; }
+  else if (nstage == 2) {
+    if (s == 1) { g0 = 1; g1 = 0; beta = 1; cur = 0; out = 1; }
+    else { g0 = 0.5; g1 = 0.5; beta = 0.5; cur = 1; out = 0; }
+  } else if (nstage == 3) {
+    if (s == 1) { g0 = 1; g1 = 0; beta = 1; cur = 0; out = 1; }
+    else if (s == 2) { g0 = 0.75; g1 = 0.25; beta = 0.25; cur = 1; out = 1; }
+    else { g0 = 1.0 / 3.0; g1 = 2.0 / 3.0; beta = 2.0 / 3.0; cur = 1; out = 0; }
+  } else {
+    if (s == 1) { g0 = 1; g1 = 0; beta = 0.5; cur = 0; out = 1; }
+    else if (s == 2) { g0 = 0; g1 = 1; beta = 0.5; cur = 1; out = 1; }
+    else if (s == 3) { g0 = 2.0 / 3.0; g1 = 1.0 / 3.0; beta = 1.0 / 6.0; cur = 1; out = 1; }
+    else { g0 = 0; g1 = 1; beta = 0.5; cur = 1; out = 0; }
+  }
+}
+
+cudaStream_t S(chq_mesh *m, void *s) { return s ? static_cast<cudaStream_t>(s) : m->stream; }
+
+template <class P> P *as(void *p) { return static_cast<P *>(p); }
+
+cudaEvent_t pool_event(chq_mesh *m) {
+  if (!m->pool.empty()) {
+    cudaEvent_t e = m->pool.back();
+    m->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// CUDA-event timing of one kernel kind around a launch sequence (when profiling is on)
+struct Prof {
+  chq_mesh *m;
+  int kind;
+  cudaStream_t s;
+  cudaEvent_t b = nullptr;
+  Prof(chq_mesh *m_, int k, cudaStream_t s_) : m(m_), kind(k), s(s_) {
+    if (m->prof) {
+      b = pool_event(m);
+      cudaEventRecord(b, s);
+    }
+  }
+  ~Prof() {
+    if (m->prof && b) {
+      cudaEvent_t e = pool_event(m);
+      cudaEventRecord(e, s);
+      m->pending.push_back({kind, b, e});
+    }
+  }
+};
+enum { PK_FLUX = 0, PK_CORNER = 1, PK_UPDATE = 2, PK_FLAG = 3, PK_REPAIR = 4, PK_BC = 5, PK_C2P = 6, PK_LIMIT = 7,
+       PK_CTL = 8 };
+
+// ---- fluxes --------------------------------------------------------------------------
+template <class P>
+FluxArgs<P> flux_args(chq_mesh *m, int cur, unsigned dirmask) {
+  FluxArgs<P> a{};
+  a.g = m->g;
+  a.eos = m->eos;
+  a.w = as<P>(m->w);
+  a.bcc = as<P>(m->bcc);
+  for (int d = 0; d < 3; ++d) {
+    a.bn[d] = m->bf[cur][d];
+    a.flx[d] = as<P>(m->flx[d]);
+    a.et2[d] = as<P>(m->et2[d]);
+    a.et1[d] = as<P>(m->et1[d]);
+    for (int q = 0; q < 3; ++q) { a.lo[d][q] = m->lo[d][q]; a.hi[d][q] = m->hi[d][q]; }
+    a.active[d] = m->active[d] && ((dirmask >> d) & 1);
+  }
+  a.flatten = m->cfg.flatten;
+  a.low_mach = m->cfg.low_mach;
+  a.lhlld_phi = m->cfg.lhlld_phi;
+  a.seglen = m->seglen;
+  a.nchunk = (m->g.ni + 1 + 31) / 32;
+  // x: rows x 31-face segments; y/z: i chunks x outer x segments
+  a.nseg[0] = (m->hi[0][2] - m->lo[0][2] + 1 + 30) / 31;
+  a.nwarp[0] = a.active[0] ? (long)(m->hi[0][0] - m->lo[0][0] + 1) * (m->hi[0][1] - m->lo[0][1] + 1) * a.nseg[0] : 0;
+  a.nseg[1] = (m->hi[1][1] - m->lo[1][1] + 1 + a.seglen - 1) / a.seglen;
+  a.nwarp[1] = a.active[1] ? (long)a.nchunk * (m->hi[1][0] - m->lo[1][0] + 1) * a.nseg[1] : 0;
+  a.nseg[2] = (m->hi[2][0] - m->lo[2][0] + 1 + a.seglen - 1) / a.seglen;
+  a.nwarp[2] = a.active[2] ? (long)a.nchunk * (m->hi[2][1] - m->lo[2][1] + 1) * a.nseg[2] : 0;
+  a.skip = nullptr;
+  return a;
+}
+
+template <class P>
+cudaError_t launch_flux_any(const FluxArgs<P> &a, int recon, int rsolver, int charac, cudaStream_t s) {
+  const long warps = a.nwarp[0] + a.nwarp[1] + a.nwarp[2];
+  const unsigned nblocks = (unsigned)((warps + 3) / 4);
+  switch (recon) {
+    case R_DC: return launch_flux<P, R_DC>(a, rsolver, charac, nblocks, s);
+    case R_PLM: return launch_flux<P, R_PLM>(a, rsolver, charac, nblocks, s);
+    case R_PPM: return launch_flux<P, R_PPM>(a, rsolver, charac, nblocks, s);
+    case R_PPMX: return launch_flux<P, R_PPMX>(a, rsolver, charac, nblocks, s);
+    case R_WENOZ: return launch_flux<P, R_WENOZ>(a, rsolver, charac, nblocks, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int do_fluxes(chq_mesh *m, int cur, unsigned dirmask, const int *done, cudaStream_t s) {
+  cudaError_t e;
+  m->nlaunch += 1;
+  if (m->mixed) {
+    FluxArgs<float> a = flux_args<float>(m, cur, dirmask);
+    a.skip = done;
+    e = launch_flux_any(a, m->cfg.recon, m->cfg.rsolver, m->cfg.characteristic, s);
+  } else {
+    FluxArgs<double> a = flux_args<double>(m, cur, dirmask);
+    a.skip = done;
+    e = launch_flux_any(a, m->cfg.recon, m->cfg.rsolver, m->cfg.characteristic, s);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "flux_kernel launch");
+  return CHQ_OK;
+}
+
+// ---- corner EMF ----------------------------------------------------------------------
+template <class P>
+int do_corner(chq_mesh *m, const int *done, const int *need, cudaStream_t s) {
+  const Geom &g = m->g;
+  EmfArgs<P> a{};
+  a.g = g;
+  a.f1 = as<P>(m->flx[0]); a.f2 = as<P>(m->flx[1]); a.f3 = as<P>(m->flx[2]);
+  a.e2x1 = as<P>(m->et1[0]); a.e3x1 = as<P>(m->et2[0]);
+  a.e1x2 = as<P>(m->et2[1]); a.e3x2 = as<P>(m->et1[1]);
+  a.e1x3 = as<P>(m->et1[2]); a.e2x3 = as<P>(m->et2[2]);
+  a.ecc = as<P>(m->ecc);
+  a.e1 = as<P>(m->e[0]); a.e2 = as<P>(m->e[1]); a.e3 = as<P>(m->e[2]);
+  a.done = done;
+  a.need = need;
+  const int nxi = g.ie + 2 - g.is, nyj = g.je + 2 - g.js;
+  const int nzk = g.three_d ? g.ke + 2 - g.ks : 1;
+  dim3 blk(32, 8), grd((nxi + 31) / 32, (nyj + 7) / 8, nzk);
+  m->nlaunch += 1;
+  corner_emf_kernel<P><<<grd, blk, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+// ---- update --------------------------------------------------------------------------
+template <class P>
+int do_update(chq_mesh *m, int out, double g0, double g1, double bdt, const double *bdt_dev, const int *done,
+              const int *need, cudaStream_t s) {
+  const Geom &g = m->g;
+  UpdateArgs<P> a{};
+  a.g = g;
+  a.eos = m->eos;
+  a.f1 = as<P>(m->flx[0]); a.f2 = as<P>(m->flx[1]); a.f3 = as<P>(m->flx[2]);
+  a.e1 = as<P>(m->e[0]); a.e2 = as<P>(m->e[1]); a.e3 = as<P>(m->e[2]);
+  a.ua = m->u[0]; a.ub = m->u[1]; a.uout = m->u[out];
+  a.b1a = m->bf[0][0]; a.b2a = m->bf[0][1]; a.b3a = m->bf[0][2];
+  a.b1b = m->bf[1][0]; a.b2b = m->bf[1][1]; a.b3b = m->bf[1][2];
+  a.b1o = m->bf[out][0]; a.b2o = m->bf[out][1]; a.b3o = m->bf[out][2];
+  a.g0 = g0; a.g1 = g1; a.beta_dt = bdt; a.beta_dt_dev = bdt_dev;
+  a.idx1 = 1.0 / g.dx1; a.idx2 = 1.0 / g.dx2; a.idx3 = 1.0 / g.dx3;
+  a.done = done;
+  a.need = need;
+  const int nxi = g.ie + 2 - g.is, nyj = g.je + 2 - g.js, nzk = g.ke + 2 - g.ks;
+  dim3 blk(32, 8), grd((nxi + 31) / 32, (nyj + 7) / 8, nzk);
+  m->nlaunch += 1;
+  update_kernel<P><<<grd, blk, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+int do_flag(chq_mesh *m, int buf, int *nbad_dev, const int *done, cudaStream_t s) {
+  const Geom &g = m->g;
+  FlagArgs a{};
+  a.g = g;
+  a.eos = m->eos;
+  a.u = m->u[buf];
+  a.b1 = m->bf[buf][0]; a.b2 = m->bf[buf][1]; a.b3 = m->bf[buf][2];
+  a.flag = m->flag;
+  a.nbad = nbad_dev;
+  a.done = done;
+  dim3 blk(32, 8), grd((g.nx1 + 31) / 32, (g.je - g.js + 1 + 7) / 8, g.ke - g.ks + 1);
+  m->nlaunch += 1;
+  fofc_flag_kernel<<<grd, blk, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+template <class P>
+int do_repair(chq_mesh *m, int cur, unsigned dirmask, const int *done, const int *need, cudaStream_t s) {
+  RepairArgs<P> a{};
+  a.g = m->g;
+  a.eos = m->eos;
+  a.w = as<P>(m->w);
+  a.bcc = as<P>(m->bcc);
+  long tot = 0;
+  for (int d = 0; d < 3; ++d) {
+    a.bn[d] = m->bf[cur][d];
+    a.flx[d] = as<P>(m->flx[d]);
+    a.et2[d] = as<P>(m->et2[d]);
+    a.et1[d] = as<P>(m->et1[d]);
+    for (int q = 0; q < 3; ++q) { a.lo[d][q] = m->lo[d][q]; a.hi[d][q] = m->hi[d][q]; }
+    const bool on = m->active[d] && ((dirmask >> d) & 1);
+    a.nface[d] = on ? (long)(m->hi[d][0] - m->lo[d][0] + 1) * (m->hi[d][1] - m->lo[d][1] + 1) * (m->hi[d][2] - m->lo[d][2] + 1) : 0;
+    tot += a.nface[d];
+  }
+  a.flag = m->flag;
+  a.done = done;
+  a.need = need;
+  if (tot == 0) return CHQ_OK;
+  m->nlaunch += 1;
+  fofc_repair_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+template <class P>
+int do_limit(chq_mesh *m, unsigned dirmask, double bdt, const double *bdt_dev, long long *count_dev, const int *done,
+             cudaStream_t s) {
+  const Geom &g = m->g;
+  LimitArgs<P> a{};
+  a.g = g;
+  a.eos = m->eos;
+  a.w = as<P>(m->w);
+  a.bcc = as<P>(m->bcc);
+  const int ndim = 1 + g.two_d + g.three_d;
+  a.two_ndim = 2.0 * ndim;
+  a.dx[0] = g.dx1; a.dx[1] = g.dx2; a.dx[2] = g.dx3;
+  a.beta_dt = bdt;
+  a.beta_dt_dev = bdt_dev;
+  long tot = 0;
+  for (int d = 0; d < 3; ++d) {
+    a.flx[d] = as<P>(m->flx[d]);
+    for (int q = 0; q < 3; ++q) { a.lo[d][q] = m->act_lo[d][q]; a.hi[d][q] = m->act_hi[d][q]; }
+    const bool on = m->active[d] && ((dirmask >> d) & 1);
+    a.nface[d] = on ? (long)(a.hi[d][0] - a.lo[d][0] + 1) * (a.hi[d][1] - a.lo[d][1] + 1) * (a.hi[d][2] - a.lo[d][2] + 1) : 0;
+    tot += a.nface[d];
+  }
+  a.count = count_dev;
+  a.done = done;
+  if (tot == 0) return CHQ_OK;
+  m->nlaunch += 1;
+  limit_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+int do_bc(chq_mesh *m, int buf, const int *done, cudaStream_t s) {
+  const Geom &g = m->g;
+  BcArgs a{};
+  a.g = g;
+  a.u = m->u[buf];
+  a.b1 = m->bf[buf][0]; a.b2 = m->bf[buf][1]; a.b3 = m->bf[buf][2];
+  a.done = done;
+  a.bc = m->cfg.bc1;
+  long n = (long)(g.nk + 1) * (g.nj + 1) * g.ng;
+  m->nlaunch += 1;
+  bc_kernel<0><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  if (g.two_d) {
+    a.bc = m->cfg.bc2;
+    n = (long)(g.nk + 1) * g.ng * (g.ni + 1);
+    m->nlaunch += 1;
+    bc_kernel<1><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+    CHQ_CUDA(cudaGetLastError());
+  }
+  if (g.three_d) {
+    a.bc = m->cfg.bc3;
+    n = (long)g.ng * (g.nj + 1) * (g.ni + 1);
+    m->nlaunch += 1;
+    bc_kernel<2><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+    CHQ_CUDA(cudaGetLastError());
+  }
+  return CHQ_OK;
+}
+
+template <class P>
+int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done,
+           cudaStream_t s) {
+  const Geom &g = m->g;
+  C2pArgs<P> a{};
+  a.g = g;
+  a.eos = m->eos;
+  a.u = m->u[buf];
+  a.b1 = m->bf[buf][0]; a.b2 = m->bf[buf][1]; a.b3 = m->bf[buf][2];
+  a.w = as<P>(m->w); a.bcc = as<P>(m->bcc); a.ecc = as<P>(m->ecc);
+  a.compute_dt = compute_dt;
+  a.mdt_bits = bits;
+  a.ctl = fold;
+  a.done = done;
+  dim3 blk(32, 8), grd((g.ni + 31) / 32, (g.nj + 7) / 8, g.nk);
+  m->nlaunch += 1;
+  c2p_kernel<P><<<grd, blk, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+#define DISPATCH_P(m, call) ((m)->mixed ? call<float> : call<double>)
+
+// One RK stage (src/main.cpp:46-93) with all decisions on the device.
+int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, const double *bdt_dev,
+              const int *done, cudaStream_t s) {
+  int rc;
+  {
+    Prof p(m, PK_FLUX, s);
+    if ((rc = do_fluxes(m, cur, 7u, done, s))) return rc;
+  }
+  if (m->cfg.flux_limiter) {
+    Prof p(m, PK_LIMIT, s);
+    if ((rc = DISPATCH_P(m, do_limit)(m, 7u, bdt, bdt_dev, &m->ctl->limiter_count, done, s))) return rc;
+  }
+  {
+    Prof p(m, PK_CORNER, s);
+    if ((rc = DISPATCH_P(m, do_corner)(m, done, nullptr, s))) return rc;
+  }
+  {
+    Prof p(m, PK_UPDATE, s);
+    if ((rc = DISPATCH_P(m, do_update)(m, out, g0, g1, bdt, bdt_dev, done, nullptr, s))) return rc;
+  }
+  if (m->cfg.fofc) {
+    int *nbad = &m->ctl->nbad;
+    {
+      Prof p(m, PK_FLAG, s);
+      if ((rc = do_flag(m, out, nbad, done, s))) return rc;
+    }
+    Prof p(m, PK_REPAIR, s);
+    if ((rc = DISPATCH_P(m, do_repair)(m, cur, 7u, done, nbad, s))) return rc;
+    if ((rc = DISPATCH_P(m, do_corner)(m, done, nbad, s))) return rc;
+    if ((rc = DISPATCH_P(m, do_update)(m, out, g0, g1, bdt, bdt_dev, done, nbad, s))) return rc;
+  }
+  Prof p(m, PK_BC, s);
+  return do_bc(m, out, done, s);
+}
+
+// ---- layout conversion ---------------------------------------------------------------
+struct FieldRef {
+  void *base;
+  int ncomp;
+  int face;      // 1: (nk+1, nj+1, ni+1) shape; 0: cell shape
+  int isp;       // 1: element type is P (float in the mixed form); 0: double
+  int isint;     // the int flag array
+};
+
+bool field_by_name(chq_mesh *m, const char *n, FieldRef &f) {
+  struct E { const char *name; void *base; int ncomp, face, isp, isint; };
+  const E tab[] = {
+      {"u0", m->u[0], 6, 0, 0, 0},      {"u1", m->u[1], 6, 0, 0, 0},      {"w", m->w, 6, 0, 1, 0},
+      {"bcc", m->bcc, 3, 0, 1, 0},      {"ecc", m->ecc, 3, 0, 1, 0},      {"b1f0", m->bf[0][0], 1, 1, 0, 0},
+      {"b2f0", m->bf[0][1], 1, 1, 0, 0}, {"b3f0", m->bf[0][2], 1, 1, 0, 0}, {"b1f1", m->bf[1][0], 1, 1, 0, 0},
+      {"b2f1", m->bf[1][1], 1, 1, 0, 0}, {"b3f1", m->bf[1][2], 1, 1, 0, 0}, {"f1", m->flx[0], 6, 1, 1, 0},
+      {"f2", m->flx[1], 6, 1, 1, 0},     {"f3", m->flx[2], 6, 1, 1, 0},     {"e2x1", m->et1[0], 1, 1, 1, 0},
+      {"e3x1", m->et2[0], 1, 1, 1, 0},   {"e1x2", m->et2[1], 1, 1, 1, 0},   {"e3x2", m->et1[1], 1, 1, 1, 0},
+      {"e1x3", m->et1[2], 1, 1, 1, 0},   {"e2x3", m->et2[2], 1, 1, 1, 0},   {"e1", m->e[0], 1, 1, 1, 0},
+      {"e2", m->e[1], 1, 1, 1, 0},       {"e3", m->e[2], 1, 1, 1, 0},       {"flag", m->flag, 1, 0, 0, 1},
+  };
+  for (const E &e : tab)
+    if (!std::strcmp(e.name, n)) { f = FieldRef{e.base, e.ncomp, e.face, e.isp, e.isint}; return true; }
+  return false;
+}
+
+long field_size(const chq_mesh *m, const FieldRef &f) {
+  const Geom &g = m->g;
+  return f.face ? (long)f.ncomp * (g.nk + 1) * (g.nj + 1) * (g.ni + 1) : (long)f.ncomp * g.nk * g.nj * g.ni;
+}
+
+// element size on the device
+size_t field_esize(const chq_mesh *m, const FieldRef &f) {
+  if (f.isint) return sizeof(int);
+  if (f.isp && m->mixed) return sizeof(float);
+  return sizeof(double);
+}
+
+int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaStream_t s) {
+  FieldRef f;
+  if (!field_by_name(m, name, f)) return fail(CHQ_ERR_ARG, std::string("unknown field: ") + name);
+  if (field_size(m, f) != n) return fail(CHQ_ERR_ARG, std::string("size mismatch for field ") + name);
+  const Geom &g = m->g;
+  const int nx = f.face ? g.ni + 1 : g.ni, ny = f.face ? g.nj + 1 : g.nj, nz = f.face ? g.nk + 1 : g.nk;
+  const size_t es = field_esize(m, f);
+  // stage through a host buffer of the device element type when it is not double
+  std::vector<unsigned char> tmp;
+  void *hptr = host;
+  if (es != sizeof(double) || f.isint) {
+    tmp.resize((size_t)n * es);
+    hptr = tmp.data();
+    if (up) {
+      for (long q = 0; q < n; ++q) {
+        if (f.isint) reinterpret_cast<int *>(hptr)[q] = (int)host[q];
+        else reinterpret_cast<float *>(hptr)[q] = (float)host[q];
+      }
+    }
+  }
+  for (int c = 0; c < f.ncomp; ++c) {
+    cudaMemcpy3DParms p{};
+    char *dev = static_cast<char *>(f.base) + (size_t)c * g.vstride * es;
+    char *hst = static_cast<char *>(hptr) + (size_t)c * nx * ny * nz * es;
+    cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)g.sj * es, (size_t)nx * es, (size_t)(g.nj + 1));
+    cudaPitchedPtr hp = make_cudaPitchedPtr(hst, (size_t)nx * es, (size_t)nx * es, (size_t)ny);
+    p.extent = make_cudaExtent((size_t)nx * es, (size_t)ny, (size_t)nz);
+    if (up) { p.srcPtr = hp; p.dstPtr = dp; p.kind = cudaMemcpyHostToDevice; }
+    else { p.srcPtr = dp; p.dstPtr = hp; p.kind = cudaMemcpyDeviceToHost; }
+    CHQ_CUDA(cudaMemcpy3DAsync(&p, s));
+  }
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  if (!up && hptr != host) {
+    for (long q = 0; q < n; ++q) {
+      if (f.isint) host[q] = (double)reinterpret_cast<int *>(hptr)[q];
+      else host[q] = (double)reinterpret_cast<float *>(hptr)[q];
+    }
+  }
+  return CHQ_OK;
+}
+
+}  // namespace
+
+// =======================================================================================
+extern "C" {
+
+const char *chq_last_error(void) { return g_err.c_str(); }
+
+void chq_config_defaults(chq_config *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->nx1 = 64; c->nx2 = 1; c->nx3 = 1;
+  c->nghost = 0;
+  c->x1min = 0; c->x1max = 1; c->x2min = 0; c->x2max = 1; c->x3min = 0; c->x3max = 1;
+  c->recon = CHQ_RECON_PPM;
+  c->rsolver = CHQ_RS_HLLD;
+  c->integrator = 3;
+  c->bc1 = c->bc2 = c->bc3 = CHQ_BC_PERIODIC;
+  c->gamma = 5.0 / 3.0;
+  c->dfloor = 1.0e-10;
+  c->pfloor = 1.0e-12;
+  c->cfl = 0.3;
+  c->de_eta = 1.0e-3;
+  c->lhlld_phi = -1.0;
+  c->flatten = 1;
+  c->fofc = 1;
+  c->precision = CHQ_FP64;
+  c->tlim = 1.0;
+}
+
+int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
+  if (!cfg || !out) return fail(CHQ_ERR_ARG, "null argument");
+  *out = nullptr;
+  const chq_config &c = *cfg;
+  if (c.nx1 < 1 || c.nx2 < 1 || c.nx3 < 1) return fail(CHQ_ERR_ARG, "nx must be >= 1");
+  if (c.nx2 == 1 && c.nx3 > 1) return fail(CHQ_ERR_ARG, "nx3 > 1 requires nx2 > 1");
+  if (c.recon < 0 || c.recon > 4) return fail(CHQ_ERR_ARG, "unknown reconstruction");
+  if (c.rsolver < 0 || c.rsolver > 2) return fail(CHQ_ERR_ARG, "unknown Riemann solver");
+  if (c.integrator < 1 || c.integrator > 4) return fail(CHQ_ERR_ARG, "unknown integrator");
+  if (c.precision != CHQ_FP64 && c.precision != CHQ_MIXED) return fail(CHQ_ERR_ARG, "unknown precision");
+  const int bcs[3] = {c.bc1, c.bc2, c.bc3};
+  for (int q = 0; q < 3; ++q)
+    if (bcs[q] < 0 || bcs[q] > 2) return fail(CHQ_ERR_ARG, "unknown boundary condition");
+  const bool wide = (c.recon == CHQ_RECON_PPM || c.recon == CHQ_RECON_PPMX || c.recon == CHQ_RECON_WENOZ);
+  const int ng_min = wide ? 3 : 2;
+  const int ng = (c.nghost > 0) ? c.nghost : ng_min;
+  if (ng < ng_min) return fail(CHQ_ERR_ARG, "nghost too small for the reconstruction method");
+  if (c.nu > 0 || c.kappa > 0 || c.eta > 0 || c.sts)
+    return fail(CHQ_ERR_ARG, "explicit diffusion / RKL2 is not available in this build");
+
+  chq_mesh *m = new chq_mesh;
+  m->cfg = c;
+  m->cfg.nghost = ng;
+  Geom &g = m->g;
+  g.nx1 = c.nx1; g.nx2 = c.nx2; g.nx3 = c.nx3; g.ng = ng;
+  g.ni = c.nx1 + 2 * ng;
+  g.nj = (c.nx2 > 1) ? c.nx2 + 2 * ng : 1;
+  g.nk = (c.nx3 > 1) ? c.nx3 + 2 * ng : 1;
+  g.is = ng; g.ie = ng + c.nx1 - 1;
+  g.js = (c.nx2 > 1) ? ng : 0; g.je = (c.nx2 > 1) ? ng + c.nx2 - 1 : 0;
+  g.ks = (c.nx3 > 1) ? ng : 0; g.ke = (c.nx3 > 1) ? ng + c.nx3 - 1 : 0;
+  g.two_d = (c.nx2 > 1);
+  g.three_d = (c.nx3 > 1);
+  g.x1min = c.x1min; g.x2min = c.x2min; g.x3min = c.x3min;
+  g.x1max = c.x1max; g.x2max = c.x2max; g.x3max = c.x3max;
+  g.dx1 = (c.x1max - c.x1min) / c.nx1;
+  g.dx2 = (c.x2max - c.x2min) / c.nx2;
+  g.dx3 = (c.x3max - c.x3min) / c.nx3;
+  g.sj = (long)align_up((size_t)g.ni + 1, 32);
+  g.sk = (long)(g.nj + 1) * g.sj;
+  g.vstride = (long)align_up((size_t)(g.nk + 1) * g.sk, 64);
+  g.nelem = g.vstride;
+  m->eos = EOSp{c.gamma, c.gamma - 1.0, c.dfloor, c.pfloor, c.de_eta, c.dual_energy};
+  m->nstage = c.integrator;
+  m->mixed = (c.precision == CHQ_MIXED);
+  m->psize = m->mixed ? sizeof(float) : sizeof(double);
+  m->seglen = kSeglen;
+
+  // flux face ranges (src/physics.hpp:85-88) and active face ranges (src/positivity.hpp:32-33)
+  for (int d = 0; d < 3; ++d) {
+    int il = g.is, iu = g.ie, jl = g.js, ju = g.je, kl = g.ks, ku = g.ke;
+    if (d == 0) iu = g.ie + 1; else if (g.nx1 > 1) { il = g.is - 1; iu = g.ie + 1; }
+    if (d == 1) ju = g.je + 1; else if (g.two_d) { jl = g.js - 1; ju = g.je + 1; }
+    if (d == 2) ku = g.ke + 1; else if (g.three_d) { kl = g.ks - 1; ku = g.ke + 1; }
+    m->lo[d][0] = kl; m->lo[d][1] = jl; m->lo[d][2] = il;
+    m->hi[d][0] = ku; m->hi[d][1] = ju; m->hi[d][2] = iu;
+    m->act_lo[d][0] = g.ks; m->act_lo[d][1] = g.js; m->act_lo[d][2] = g.is;
+    m->act_hi[d][0] = (d == 2) ? g.ke + 1 : g.ke;
+    m->act_hi[d][1] = (d == 1) ? g.je + 1 : g.je;
+    m->act_hi[d][2] = (d == 0) ? g.ie + 1 : g.ie;
+  }
+  m->active[0] = 1;
+  m->active[1] = g.two_d;
+  m->active[2] = g.three_d;
+
+  // one slab: doubles (u0, u1: 6 each; 6 face fields), P fields (w 6, bcc 3, ecc 3,
+  // fluxes 18, face EMFs 6, edge EMFs 3), the int flag array, control block and scratch
+  const size_t nel = (size_t)g.vstride;
+  const size_t dbytes = nel * sizeof(double), pbytes = nel * m->psize, ibytes = align_up(nel * sizeof(int), 256);
+  m->hst_blocks = 1184;   // 8 blocks per SM on 148 SMs
+  const size_t ctl_bytes = align_up(sizeof(StepCtl), 256);
+  const size_t hst_bytes = align_up((size_t)(m->hst_blocks * 10 + 16) * sizeof(double), 256);
+  m->slab_bytes = dbytes * 18 + pbytes * 39 + ibytes + ctl_bytes + hst_bytes;
+  cudaError_t e = cudaMalloc(&m->slab, m->slab_bytes);
+  if (e != cudaSuccess) {
+    delete m;
+    return fail(CHQ_ERR_NOMEM, std::string("device allocation of the mesh failed: ") + cudaGetErrorString(e));
+  }
+  char *p = m->slab;
+  m->u[0] = (double *)p; p += dbytes * 6;
+  m->u[1] = (double *)p; p += dbytes * 6;
+  for (int b = 0; b < 2; ++b)
+    for (int d = 0; d < 3; ++d) { m->bf[b][d] = (double *)p; p += dbytes; }
+  m->w = p; p += pbytes * 6;
+  m->bcc = p; p += pbytes * 3;
+  m->ecc = p; p += pbytes * 3;
+  for (int d = 0; d < 3; ++d) { m->flx[d] = p; p += pbytes * 6; }
+  for (int d = 0; d < 3; ++d) { m->et2[d] = p; p += pbytes; m->et1[d] = p; p += pbytes; }
+  for (int d = 0; d < 3; ++d) { m->e[d] = p; p += pbytes; }
+  m->flag = (int *)p; p += ibytes;
+  m->ctl = (StepCtl *)p; p += ctl_bytes;
+  m->hst_part = (double *)p;
+  m->hst_out = m->hst_part + (size_t)m->hst_blocks * 10;
+  e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->slab, 0, m->slab_bytes, m->stream);
+  if (e == cudaSuccess) {
+    StepCtl h{};
+    h.tlim = c.tlim;
+    h.cfl = c.cfl;
+    h.nstage = m->nstage;
+    h.mdt_bits = 0x7ff0000000000000ULL;
+    for (int s = 1; s <= m->nstage; ++s) {
+      int cur, o;
+      stage_table(m->nstage, s, h.g0[s - 1], h.g1[s - 1], h.beta[s - 1], cur, o);
+    }
+    e = cudaMemcpyAsync(m->ctl, &h, sizeof(h), cudaMemcpyHostToDevice, m->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+  if (e != cudaSuccess) {
+    chq_mesh_destroy(m);
+    return cuda_fail(e, "mesh initialisation");
+  }
+  *out = m;
+  return CHQ_OK;
+}
+
+int chq_mesh_destroy(chq_mesh *m) {
+  if (!m) return CHQ_OK;
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  for (auto &p : m->pending) { m->pool.push_back(p.b); m->pool.push_back(p.e); }
+  for (cudaEvent_t e : m->pool) cudaEventDestroy(e);
+  for (cudaEvent_t e : m->slots) if (e) cudaEventDestroy(e);
+  if (m->slab) cudaFree(m->slab);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return CHQ_OK;
+}
+
+int chq_mesh_dims(const chq_mesh *m, int dims[10]) {
+  if (!m || !dims) return fail(CHQ_ERR_ARG, "null argument");
+  const Geom &g = m->g;
+  const int v[10] = {g.nx1, g.nx2, g.nx3, g.ng, g.ni, g.nj, g.nk, m->nstage, g.two_d, g.three_d};
+  std::memcpy(dims, v, sizeof(v));
+  return CHQ_OK;
+}
+
+long long chq_mesh_bytes(const chq_mesh *m) { return m ? (long long)m->slab_bytes : 0; }
+
+long chq_array_size(const chq_mesh *m, const char *name) {
+  FieldRef f;
+  if (!m || !name || !field_by_name(const_cast<chq_mesh *>(m), name, f)) return -1;
+  return field_size(m, f);
+}
+
+int chq_upload(chq_mesh *m, const char *name, const double *host, long n, void *stream) {
+  if (!m || !name || !host) return fail(CHQ_ERR_ARG, "null argument");
+  return transfer(m, name, const_cast<double *>(host), n, true, S(m, stream));
+}
+
+int chq_download(chq_mesh *m, const char *name, double *host, long n, void *stream) {
+  if (!m || !name || !host) return fail(CHQ_ERR_ARG, "null argument");
+  return transfer(m, name, host, n, false, S(m, stream));
+}
+
+int chq_fluxes(chq_mesh *m, int dir, int cur, void *stream) {
+  if (!m || dir < 0 || dir > 2 || (cur != 0 && cur != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  if (!m->active[dir]) return fail(CHQ_ERR_ARG, "direction not active in this mesh");
+  return do_fluxes(m, cur, 1u << dir, nullptr, S(m, stream));
+}
+
+int chq_fluxes_all(chq_mesh *m, int cur, void *stream) {
+  if (!m || (cur != 0 && cur != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  return do_fluxes(m, cur, 7u, nullptr, S(m, stream));
+}
+
+int chq_corner_emf(chq_mesh *m, void *stream) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  return DISPATCH_P(m, do_corner)(m, nullptr, nullptr, S(m, stream));
+}
+
+int chq_update(chq_mesh *m, int out, double g0, double g1, double beta_dt, void *stream) {
+  if (!m || (out != 0 && out != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  return DISPATCH_P(m, do_update)(m, out, g0, g1, beta_dt, nullptr, nullptr, nullptr, S(m, stream));
+}
+
+int chq_boundaries(chq_mesh *m, int buf, void *stream) {
+  if (!m || (buf != 0 && buf != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  return do_bc(m, buf, nullptr, S(m, stream));
+}
+
+int chq_cons_to_prim(chq_mesh *m, int buf, int compute_dt, double *min_dt, void *stream) {
+  if (!m || (buf != 0 && buf != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  cudaStream_t s = S(m, stream);
+  unsigned long long *bits = &m->ctl->mdt_bits;
+  if (compute_dt) {
+    reset_bits_kernel<<<1, 1, 0, s>>>(bits);
+    CHQ_CUDA(cudaGetLastError());
+  }
+  int rc = DISPATCH_P(m, do_c2p)(m, buf, compute_dt, bits, nullptr, nullptr, s);
+  if (rc) return rc;
+  if (compute_dt && min_dt) {
+    unsigned long long h = 0;
+    CHQ_CUDA(cudaMemcpyAsync(&h, bits, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CHQ_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(min_dt, &h, sizeof(double));
+  }
+  return CHQ_OK;
+}
+
+int chq_fofc_flag(chq_mesh *m, int buf, int *nbad, void *stream) {
+  if (!m || (buf != 0 && buf != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  cudaStream_t s = S(m, stream);
+  CHQ_CUDA(cudaMemsetAsync(&m->ctl->nbad, 0, sizeof(int), s));
+  int rc = do_flag(m, buf, &m->ctl->nbad, nullptr, s);
+  if (rc) return rc;
+  if (nbad) {
+    CHQ_CUDA(cudaMemcpyAsync(nbad, &m->ctl->nbad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CHQ_CUDA(cudaStreamSynchronize(s));
+  }
+  return CHQ_OK;
+}
+
+int chq_fofc_repair(chq_mesh *m, int dir, int cur, void *stream) {
+  if (!m || dir < 0 || dir > 2 || (cur != 0 && cur != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  if (!m->active[dir]) return fail(CHQ_ERR_ARG, "direction not active in this mesh");
+  return DISPATCH_P(m, do_repair)(m, cur, 1u << dir, nullptr, nullptr, S(m, stream));
+}
+
+int chq_limit_fluxes(chq_mesh *m, int dir, double beta_dt, long *count, void *stream) {
+  if (!m || dir < 0 || dir > 2) return fail(CHQ_ERR_ARG, "bad argument");
+  if (!m->active[dir]) return fail(CHQ_ERR_ARG, "direction not active in this mesh");
+  cudaStream_t s = S(m, stream);
+  long long *cnt = &m->ctl->limiter_count;
+  long long before = 0, after = 0;
+  CHQ_CUDA(cudaMemcpyAsync(&before, cnt, sizeof(before), cudaMemcpyDeviceToHost, s));
+  int rc = DISPATCH_P(m, do_limit)(m, 1u << dir, beta_dt, nullptr, cnt, nullptr, s);
+  if (rc) return rc;
+  CHQ_CUDA(cudaMemcpyAsync(&after, cnt, sizeof(after), cudaMemcpyDeviceToHost, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  if (count) *count += (long)(after - before);
+  return CHQ_OK;
+}
+
+int chq_stage(chq_mesh *m, int cur, int out, double g0, double g1, double beta_dt, void *stream) {
+  if (!m || (cur != 0 && cur != 1) || (out != 0 && out != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  cudaStream_t s = S(m, stream);
+  CHQ_CUDA(cudaMemsetAsync(&m->ctl->nbad, 0, sizeof(int), s));
+  return run_stage(m, cur, out, g0, g1, beta_dt, nullptr, nullptr, s);
+}
+
+int chq_prime(chq_mesh *m, double t, void *stream) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  cudaStream_t s = S(m, stream);
+  ctl_prime_kernel<<<1, 1, 0, s>>>(m->ctl, t);
+  CHQ_CUDA(cudaGetLastError());
+  int rc = do_bc(m, 0, nullptr, s);
+  if (rc) return rc;
+  rc = DISPATCH_P(m, do_c2p)(m, 0, 1, &m->ctl->mdt_bits, m->ctl, nullptr, s);
+  if (rc) return rc;
+  ctl_take_dt_kernel<<<1, 1, 0, s>>>(m->ctl);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+int chq_cycles(chq_mesh *m, int n, void *stream) {
+  if (!m || n < 0) return fail(CHQ_ERR_ARG, "bad argument");
+  cudaStream_t s = S(m, stream);
+  const int *done = &m->ctl->done;
+  for (int c = 0; c < n; ++c) {
+    {
+      Prof p(m, PK_CTL, s);
+      ctl_begin_kernel<<<1, 1, 0, s>>>(m->ctl, 0);
+      m->nlaunch += 1;
+    }
+    CHQ_CUDA(cudaGetLastError());
+    for (int st = 1; st <= m->nstage; ++st) {
+      double g0, g1, beta;
+      int cur, out;
+      stage_table(m->nstage, st, g0, g1, beta, cur, out);
+      int rc = run_stage(m, cur, out, g0, g1, 0.0, &m->ctl->beta_dt[st - 1], done, s);
+      if (rc) return rc;
+      const bool last = (st == m->nstage);
+      {
+        Prof p(m, PK_C2P, s);
+        rc = DISPATCH_P(m, do_c2p)(m, out, last ? 1 : 0, &m->ctl->mdt_bits, m->ctl, done, s);
+      }
+      if (rc) return rc;
+    }
+    {
+      Prof p(m, PK_CTL, s);
+      ctl_end_kernel<<<1, 1, 0, s>>>(m->ctl);
+      m->nlaunch += 1;
+    }
+    CHQ_CUDA(cudaGetLastError());
+  }
+  return CHQ_OK;
+}
+
+int chq_clock(chq_mesh *m, double *t, int *cycle, double *dt, double *min_dt) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  StepCtl h;
+  CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+  CHQ_CUDA(cudaStreamSynchronize(m->stream));
+  if (t) *t = h.t;
+  if (cycle) *cycle = h.cycle;
+  if (dt) *dt = h.dt;
+  if (min_dt) *min_dt = h.min_dt;
+  return CHQ_OK;
+}
+
+int chq_counters(chq_mesh *m, long long *fofc, long long *limiter) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  StepCtl h;
+  CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+  CHQ_CUDA(cudaStreamSynchronize(m->stream));
+  if (fofc) *fofc = h.fofc_count + h.nbad;
+  if (limiter) *limiter = h.limiter_count;
+  return CHQ_OK;
+}
+
+int chq_history(chq_mesh *m, double out[10], void *stream) {
+  if (!m || !out) return fail(CHQ_ERR_ARG, "null argument");
+  cudaStream_t s = S(m, stream);
+  const Geom &g = m->g;
+  if (m->mixed)
+    hst_partial_kernel<float><<<m->hst_blocks, 256, 0, s>>>(g, m->u[0], as<float>(m->w), as<float>(m->bcc), m->bf[0][0],
+                                                            m->bf[0][1], m->bf[0][2], 1.0 / g.dx1, 1.0 / g.dx2,
+                                                            1.0 / g.dx3, m->hst_part);
+  else
+    hst_partial_kernel<double><<<m->hst_blocks, 256, 0, s>>>(g, m->u[0], as<double>(m->w), as<double>(m->bcc),
+                                                             m->bf[0][0], m->bf[0][1], m->bf[0][2], 1.0 / g.dx1,
+                                                             1.0 / g.dx2, 1.0 / g.dx3, m->hst_part);
+  CHQ_CUDA(cudaGetLastError());
+  hst_final_kernel<<<1, 32, 0, s>>>(m->hst_part, m->hst_blocks, m->hst_out);
+  CHQ_CUDA(cudaGetLastError());
+  double h[10];
+  CHQ_CUDA(cudaMemcpyAsync(h, m->hst_out, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  const double vol = g.dx1 * (g.two_d ? g.dx2 : 1.0) * (g.three_d ? g.dx3 : 1.0);
+  const double ncell = (double)g.nx1 * g.nx2 * g.nx3;
+  for (int q = 0; q < 8; ++q) out[q] = h[q] * vol;
+  out[8] = h[8];
+  out[9] = h[9] / ncell;
+  return CHQ_OK;
+}
+
+int chq_run_host(chq_mesh *m, double *u, double *b1, double *b2, double *b3, int ncycles, double t0, void *stream) {
+  if (!m || !u || !b1 || !b2 || !b3 || ncycles < 0) return fail(CHQ_ERR_ARG, "bad argument");
+  cudaStream_t s = S(m, stream);
+  int rc;
+  if ((rc = transfer(m, "u0", u, chq_array_size(m, "u0"), true, s))) return rc;
+  if ((rc = transfer(m, "b1f0", b1, chq_array_size(m, "b1f0"), true, s))) return rc;
+  if ((rc = transfer(m, "b2f0", b2, chq_array_size(m, "b2f0"), true, s))) return rc;
+  if ((rc = transfer(m, "b3f0", b3, chq_array_size(m, "b3f0"), true, s))) return rc;
+  if ((rc = chq_prime(m, t0, s))) return rc;
+  if ((rc = chq_cycles(m, ncycles, s))) return rc;
+  int done_cycles = 0;
+  if ((rc = transfer(m, "u0", u, chq_array_size(m, "u0"), false, s))) return rc;
+  if ((rc = transfer(m, "b1f0", b1, chq_array_size(m, "b1f0"), false, s))) return rc;
+  if ((rc = transfer(m, "b2f0", b2, chq_array_size(m, "b2f0"), false, s))) return rc;
+  if ((rc = transfer(m, "b3f0", b3, chq_array_size(m, "b3f0"), false, s))) return rc;
+  if ((rc = chq_clock(m, nullptr, &done_cycles, nullptr, nullptr))) return rc;
+  return done_cycles;
+}
+
+int chq_set_device(int device) {
+  CHQ_CUDA(cudaSetDevice(device));
+  return CHQ_OK;
+}
+
+int chq_device_count(int *count) {
+  if (!count) return fail(CHQ_ERR_ARG, "null argument");
+  CHQ_CUDA(cudaGetDeviceCount(count));
+  return CHQ_OK;
+}
+
+int chq_host_alloc(long long bytes, void **ptr) {
+  if (!ptr || bytes <= 0) return fail(CHQ_ERR_ARG, "bad argument");
+  cudaError_t e = cudaHostAlloc(ptr, (size_t)bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
+  return CHQ_OK;
+}
+
+int chq_host_free(void *ptr) {
+  if (ptr) CHQ_CUDA(cudaFreeHost(ptr));
+  return CHQ_OK;
+}
+
+int chq_event_record(chq_mesh *m, int slot) {
+  if (!m || slot < 0 || slot >= 8) return fail(CHQ_ERR_ARG, "bad argument");
+  if (!m->slots[slot]) CHQ_CUDA(cudaEventCreate(&m->slots[slot]));
+  CHQ_CUDA(cudaEventRecord(m->slots[slot], m->stream));
+  return CHQ_OK;
+}
+
+int chq_event_elapsed(chq_mesh *m, int a, int b, float *ms) {
+  if (!m || !ms || a < 0 || a >= 8 || b < 0 || b >= 8 || !m->slots[a] || !m->slots[b])
+    return fail(CHQ_ERR_ARG, "bad argument");
+  CHQ_CUDA(cudaEventSynchronize(m->slots[b]));
+  CHQ_CUDA(cudaEventElapsedTime(ms, m->slots[a], m->slots[b]));
+  return CHQ_OK;
+}
+
+long long chq_kernel_launches(const chq_mesh *m) { return m ? m->nlaunch : 0; }
+
+int chq_profile(chq_mesh *m, int enable) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  m->prof = (enable != 0);
+  return CHQ_OK;
+}
+
+int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launches[CHQ_NPROF], int reset) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  CHQ_CUDA(cudaStreamSynchronize(m->stream));
+  for (auto &p : m->pending) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, p.b, p.e) == cudaSuccess) {
+      m->prof_ms[p.kind] += t;
+      m->prof_n[p.kind] += 1;
+    }
+    m->pool.push_back(p.b);
+    m->pool.push_back(p.e);
+  }
+  m->pending.clear();
+  for (int k = 0; k < CHQ_NPROF; ++k) {
+    if (ms) ms[k] = m->prof_ms[k];
+    if (launches) launches[k] = m->prof_n[k];
+    if (reset) { m->prof_ms[k] = 0; m->prof_n[k] = 0; }
+  }
+  return CHQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,153 @@
+/* chasqui_b200 — C ABI of the B200-native per-Runge-Kutta-stage ideal-MHD path.
+ *
+ * This is the drop-in boundary for Chasqui's stage seam: every function below replaces one
+ * call inside the reference's Stage() / time loop (src/main.cpp:46-93, 200-201, 246-297),
+ * keeps its argument meaning, and runs hand-written sm_100a CUDA kernels. The mesh keeps the
+ * reference's state model: conserved u0/u1 and face fields b?f0/b?f1 as RK double buffers,
+ * primitives w, centred B bcc, cell EMF ecc, fluxes f1..f3, face EMFs e<c>x<d>, edge EMFs
+ * e1..e3 and the FOFC flag array (src/mesh.hpp:13-63).
+ *
+ * Conventions
+ *   - Every call returns CHQ_OK (0) or a negative CHQ_ERR_* code and never throws; the
+ *     message of the last failure on the calling thread is chq_last_error().
+ *   - `stream` is a cudaStream_t (NULL = the mesh's own stream). Calls are asynchronous on
+ *     that stream unless they return a host value (documented per call).
+ *   - Buffer selectors: 0 = u0 / b?f0, 1 = u1 / b?f1 (the reference's cur_is_u1/out_is_u1).
+ *   - Host arrays use the reference's packed LayoutRight shapes including ghost zones:
+ *     cells (ncomp, nk, nj, ni), faces and edges (ncomp, nk+1, nj+1, ni+1).
+ *   - Plain pointers and sizes only; no framework types cross this boundary.
+ */
+#ifndef CHQ_H_
+#define CHQ_H_
+
+#if defined(__GNUC__)
+#define CHQ_API __attribute__((visibility("default")))
+#else
+#define CHQ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHQ_OK 0
+#define CHQ_ERR_ARG (-1)     /* invalid argument or configuration */
+#define CHQ_ERR_CUDA (-2)    /* CUDA runtime error */
+#define CHQ_ERR_NOMEM (-3)   /* device allocation failed */
+#define CHQ_ERR_STATE (-4)   /* operation not valid in the mesh's current state */
+
+/* enum values are the reference's (src/defs.hpp:35-37, src/physics.hpp:20) */
+enum { CHQ_RECON_DC = 0, CHQ_RECON_PLM = 1, CHQ_RECON_PPM = 2, CHQ_RECON_WENOZ = 3, CHQ_RECON_PPMX = 4 };
+enum { CHQ_RS_HLLE = 0, CHQ_RS_HLLD = 1, CHQ_RS_LHLLD = 2 };
+enum { CHQ_BC_PERIODIC = 0, CHQ_BC_OUTFLOW = 1, CHQ_BC_REFLECT = 2 };
+/* FP64: everything in double. MIXED: primitives, reconstruction, Riemann fluxes and EMFs in
+ * float; RK accumulation of u, the face-B CT update, con2prim's pressure recovery and the
+ * dt / history reductions stay double. */
+enum { CHQ_FP64 = 0, CHQ_MIXED = 1 };
+
+typedef struct chq_config {
+  int nx1, nx2, nx3;      /* active cells; nx2 = 1 (1D) and nx3 = 1 (1D/2D) collapse axes */
+  int nghost;             /* <= 0: the reference default (3 for ppm/ppmx/wenoz, else 2) */
+  double x1min, x1max, x2min, x2max, x3min, x3max;
+  int recon, rsolver;
+  int integrator;         /* 1 rk1, 2 rk2, 3 rk3 (SSP), 4 SSPRK(4,3) (src/main.cpp:250-268) */
+  int bc1, bc2, bc3;
+  double gamma, dfloor, pfloor, cfl, de_eta, lhlld_phi;
+  int dual_energy, low_mach, flatten, characteristic, fofc, flux_limiter;
+  double nu, kappa, eta;  /* explicit diffusion coefficients (0 = off) */
+  int sts;                /* RKL2 super-time-stepping of the diffusive terms */
+  int precision;          /* CHQ_FP64 or CHQ_MIXED */
+  double tlim;            /* end time used by chq_cycles */
+} chq_config;
+
+typedef struct chq_mesh chq_mesh;
+
+/* ---- configuration and lifetime -------------------------------------------------------- */
+/* Fill the reference's defaults (src/main.cpp:116-178): ppm, hlld, rk3, cfl 0.3,
+ * gamma 5/3, dfloor 1e-10, pfloor 1e-12, flatten and fofc on, periodic boundaries. */
+CHQ_API void chq_config_defaults(chq_config *cfg);
+/* Allocate a device mesh with all fields zero (Mesh::Allocate, src/mesh.hpp:37-63). */
+CHQ_API int chq_mesh_create(const chq_config *cfg, chq_mesh **out);
+CHQ_API int chq_mesh_destroy(chq_mesh *m);
+/* dims[0..9] = nx1, nx2, nx3, ng, ni, nj, nk, nstage, two_d, three_d */
+CHQ_API int chq_mesh_dims(const chq_mesh *m, int dims[10]);
+/* device bytes held by the mesh */
+CHQ_API long long chq_mesh_bytes(const chq_mesh *m);
+CHQ_API const char *chq_last_error(void);
+
+/* ---- state transfer in the reference layout ---------------------------------------------
+ * name: u0 u1 w bcc ecc b1f0 b2f0 b3f0 b1f1 b2f1 b3f1 f1 f2 f3 e2x1 e3x1 e1x2 e3x2 e1x3
+ *       e2x3 e1 e2 e3 flag. n must equal chq_array_size(). Mixed-form float fields are
+ *       converted on the host. Both calls synchronise the stream before returning. */
+CHQ_API long chq_array_size(const chq_mesh *m, const char *name);
+CHQ_API int chq_upload(chq_mesh *m, const char *name, const double *host, long n, void *stream);
+CHQ_API int chq_download(chq_mesh *m, const char *name, double *host, long n, void *stream);
+
+/* ---- stage seam (replaces src/main.cpp:46-93 call by call) ------------------------------ */
+/* kernels::FluxesDispatch<dir> (src/physics.hpp:505-514): fluxes and face EMFs of one
+ * direction from the primitives and the face field of buffer cur. */
+CHQ_API int chq_fluxes(chq_mesh *m, int dir, int cur, void *stream);
+/* all active directions in one launch (the fused K1) */
+CHQ_API int chq_fluxes_all(chq_mesh *m, int cur, void *stream);
+/* kernels::CornerEMF (src/physics.hpp:242-297) */
+CHQ_API int chq_corner_emf(chq_mesh *m, void *stream);
+/* kernels::Update (src/physics.hpp:307-348): out = g0*(u0,b?f0) + g1*(u1,b?f1) - beta_dt*L */
+CHQ_API int chq_update(chq_mesh *m, int out, double g0, double g1, double beta_dt, void *stream);
+/* kernels::Boundaries (src/physics.hpp:354-432) on buffer buf */
+CHQ_API int chq_boundaries(chq_mesh *m, int buf, void *stream);
+/* kernels::ConsToPrim (src/physics.hpp:437-494) on buffer buf. With compute_dt and a
+ * non-NULL min_dt the call synchronises and returns min dx/(|v|+c_f) in *min_dt. */
+CHQ_API int chq_cons_to_prim(chq_mesh *m, int buf, int compute_dt, double *min_dt, void *stream);
+/* fofc::FlagBadCells (src/fofc.hpp:17-43) on buffer buf; synchronises, count in *nbad */
+CHQ_API int chq_fofc_flag(chq_mesh *m, int buf, int *nbad, void *stream);
+/* fofc::RepairFluxes<dir> (src/fofc.hpp:46-95) using the flags of the last chq_fofc_flag */
+CHQ_API int chq_fofc_repair(chq_mesh *m, int dir, int cur, void *stream);
+/* positivity::LimitFluxes<dir> (src/positivity.hpp:25-88); synchronises, adds to *count */
+CHQ_API int chq_limit_fluxes(chq_mesh *m, int dir, double beta_dt, long *count, void *stream);
+/* one whole RK stage: Stage() of src/main.cpp:46-93 (FOFC decision on the device) */
+CHQ_API int chq_stage(chq_mesh *m, int cur, int out, double g0, double g1, double beta_dt, void *stream);
+
+/* ---- whole cycles with the time step on the device (src/main.cpp:200-201, 246-297) ----- */
+/* Boundaries + ConsToPrim(dt) of u0/b?f0 and reset of the clock to t. */
+CHQ_API int chq_prime(chq_mesh *m, double t, void *stream);
+/* Up to n cycles, stopping at cfg.tlim; no host synchronisation between cycles. */
+CHQ_API int chq_cycles(chq_mesh *m, int n, void *stream);
+/* Synchronises; returns time, cycle count, last dt and the next cycle's min_dt. */
+CHQ_API int chq_clock(chq_mesh *m, double *t, int *cycle, double *dt, double *min_dt);
+/* Synchronises; FOFC corrections and limiter activations so far. */
+CHQ_API int chq_counters(chq_mesh *m, long long *fofc, long long *limiter);
+/* output::History (src/output.hpp:91-119) of u0/b?f0: mass mom1 mom2 mom3 etot ekin emag
+ * eint divB_max divB_L1 (volume-weighted like the reference). Synchronises. */
+CHQ_API int chq_history(chq_mesh *m, double out[10], void *stream);
+
+/* ---- host-buffer job entry point (end-to-end path) ---------------------------------------
+ * Upload a reference-layout state (u: 6 x cells, b1/b2/b3: faces), prime it, run n cycles
+ * and download the result state into the same host arrays. Returns the cycles done. */
+CHQ_API int chq_run_host(chq_mesh *m, double *u, double *b1, double *b2, double *b3, int ncycles, double t0,
+                 void *stream);
+
+/* ---- device, host memory and timing utilities (no reference counterpart) ----------------- */
+/* Make `device` current for this host thread's subsequent chq calls and meshes. */
+CHQ_API int chq_set_device(int device);
+CHQ_API int chq_device_count(int *count);
+/* Page-locked host memory for fast, asynchronous transfers. */
+CHQ_API int chq_host_alloc(long long bytes, void **ptr);
+CHQ_API int chq_host_free(void *ptr);
+/* Record CUDA event `slot` (0..7) on the mesh stream; elapsed device time between two slots
+ * (synchronises on the later one). */
+CHQ_API int chq_event_record(chq_mesh *m, int slot);
+CHQ_API int chq_event_elapsed(chq_mesh *m, int from_slot, int to_slot, float *ms);
+/* Per-kernel CUDA-event timing inside the stage sequence (off by default). Kinds:
+ * 0 fluxes (K1), 1 corner EMF (K2), 2 update (K3), 3 FOFC flag, 4 FOFC repair + re-run,
+ * 5 boundaries (K4), 6 con2prim + dt (K5), 7 positivity limiter, 8 step control. */
+#define CHQ_NPROF 9
+/* Number of CUDA kernels this mesh has launched so far (including early-exit launches). */
+CHQ_API long long chq_kernel_launches(const chq_mesh *m);
+CHQ_API int chq_profile(chq_mesh *m, int enable);
+/* Synchronises; totals in ms and launch counts per kind since the last reset. */
+CHQ_API int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launches[CHQ_NPROF], int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHQ_H_ */

@@ -1,0 +1,129 @@
+"""Whole-cycle parity: the device time loop (dt, FOFC decisions and counters on the device)
+against the reference's own loop, plus system-level invariants on the device.
+
+Tolerance (FP64 form): relative L1 <= 1e-12 per field after 10 cycles. The expected
+difference is exactly zero except where pow(rho, gamma) rounds differently on the device
+(entropy slot and dual-energy pressure), which stays at the 1e-15 level."""
+import numpy as np
+import pytest
+
+from tests import cases
+from tests.parity import copy_state, l1_rel, make_pair
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u0", "b1f0", "b2f0", "b3f0")
+
+CYCLE_CASES = {
+    "ot2d_64_ppm_hlld": (cases.ot(64), []),
+    "blast3d_24_ppm_hlld": (cases.blast(24), []),
+    "cpaw3d_wenoz_hlld": (cases.cpaw3d_extruded(16, 8), []),
+    "shock1d_ppm_hlld": (cases.shock_tube(128), []),
+    "loop3d_ppmx_lhlld_char": (cases.field_loop(16, 8), ["mhd.rsolver=lhlld", "mhd.characteristic=true"]),
+    "ot2d_rk4_lowmach_dual": (cases.ot(32), ["time.integrator=rk4", "mhd.low_mach=true", "mhd.dual_energy=true"]),
+    "ot2d_rk2_limiter": (cases.ot(32), ["time.integrator=rk2", "mhd.flux_limiter=true"]),
+    "blast3d_strong_fofc": (cases.blast(16), ["problem.pres_in=1e5", "problem.pres_out=1e-5", "time.cfl=0.9",
+                                             "mhd.reconstruct=ppmx"]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CYCLE_CASES))
+def test_ten_cycles_match_reference(name):
+    text, ov = CYCLE_CASES[name]
+    ref, mesh = make_pair(text, ov)
+    copy_state(ref, mesh, ("u0", "b1f0", "b2f0", "b3f0"))
+    mesh.prime(0.0)
+    assert mesh.clock()["min_dt"] == pytest.approx(ref.min_dt, rel=1e-15)
+    for c in range(10):
+        ref.cycles(1)
+        mesh.cycles(1)
+        ck = mesh.clock()
+        assert ck["cycle"] == ref.cycle
+        assert ck["t"] == pytest.approx(ref.time, rel=1e-14, abs=0)
+    errs = {f: l1_rel(mesh.get(f), ref.get(f)) for f in FIELDS}
+    assert max(errs.values()) <= 1e-12, errs
+    fofc_dev, _ = mesh.counters()
+    assert fofc_dev == ref.fofc_count
+
+
+def test_strong_blast_exercises_fofc():
+    text, ov = CYCLE_CASES["blast3d_strong_fofc"]
+    ref, mesh = make_pair(text, ov)
+    ref.cycles(10)
+    assert ref.fofc_count > 0, "the case no longer triggers first-order flux corrections"
+
+
+def test_history_matches_reference():
+    ref, mesh = make_pair(cases.blast(16), [])
+    ref.cycles(5)
+    copy_state(ref, mesh)
+    h_ref, h_dev = ref.history(), mesh.history()
+    # sums in a different order: agree to rounding; divB max is exact
+    np.testing.assert_allclose(h_dev[:8], h_ref[:8], rtol=1e-12, atol=1e-14)
+    assert abs(h_dev[8] - h_ref[8]) <= 1e-15
+    np.testing.assert_allclose(h_dev[9], h_ref[9], rtol=1e-10, atol=1e-16)
+
+
+def test_divergence_and_energy_invariants():
+    """div B stays at round-off and total energy is conserved on a periodic 3D blast."""
+    ref, mesh = make_pair(cases.blast(24), [])
+    copy_state(ref, mesh, ("u0", "b1f0", "b2f0", "b3f0"))
+    mesh.prime(0.0)
+    h0 = mesh.history()
+    mesh.cycles(20)
+    h1 = mesh.history()
+    assert h1[8] <= 5e-13, h1[8]
+    assert abs(h1[4] - h0[4]) <= 1e-12 * abs(h0[4])
+    assert abs(h1[0] - h0[0]) <= 1e-13 * abs(h0[0])
+
+
+def test_mirror_symmetry_is_bitwise_on_device():
+    """x-mirror symmetric blast (field along y): rho(x) == rho(-x) and v_x(x) == -v_x(-x)
+    bit for bit after many cycles (the reference's mirror-symmetric arithmetic)."""
+    ref, mesh = make_pair(cases.blast(24), ["problem.angle=90"])
+    copy_state(ref, mesh, ("u0", "b1f0", "b2f0", "b3f0"))
+    mesh.prime(0.0)
+    mesh.cycles(25)
+    u = mesh.get("u0")
+    ng = mesh.ng
+    act = u[:, ng:-ng, ng:-ng, ng:-ng]
+    mir = act[:, :, :, ::-1]
+    for n in (0, 2, 3, 4, 5):
+        assert np.array_equal(act[n], mir[n]), n
+    assert np.array_equal(act[1], -mir[1])
+
+
+def test_cycles_stop_exactly_at_tlim():
+    ref, mesh = make_pair(cases.ot(32), ["time.tlim=0.01"])
+    copy_state(ref, mesh, ("u0", "b1f0", "b2f0", "b3f0"))
+    mesh.prime(0.0)
+    mesh.cycles(1000)
+    n = ref.cycles(1000)
+    ck = mesh.clock()
+    assert ck["cycle"] == n and ck["t"] == ref.time == pytest.approx(0.01, abs=0)
+    assert l1_rel(mesh.get("u0"), ref.get("u0")) <= 1e-12
+
+
+def test_run_host_round_trip():
+    """The host-buffer entry point (upload, prime, cycles, download) equals the device loop."""
+    ref, mesh = make_pair(cases.ot(32), [])
+    u, b1, b2, b3 = (np.ascontiguousarray(ref.get(f)) for f in ("u0", "b1f0", "b2f0", "b3f0"))
+    n = mesh.run_host(u, b1, b2, b3, 7)
+    assert n == 7
+    ref.cycles(7)
+    assert l1_rel(u, ref.get("u0")) <= 1e-12
+    assert l1_rel(b1, ref.get("b1f0")) <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["ot2d_64_ppm_hlld", "blast3d_24_ppm_hlld", "cpaw3d_wenoz_hlld"])
+def test_mixed_form_stays_close_to_fp64(name):
+    """Mixed form (FP32 primitives/reconstruction/Riemann/EMFs, FP64 accumulation): relative
+    L1 difference from the FP64 reference after 10 cycles stays below 1e-4 per field."""
+    text, ov = CYCLE_CASES[name]
+    ref, mesh = make_pair(text, ov, precision="mixed")
+    copy_state(ref, mesh, ("u0", "b1f0", "b2f0", "b3f0"))
+    mesh.prime(0.0)
+    mesh.cycles(10)
+    ref.cycles(10)
+    errs = {f: l1_rel(mesh.get(f), ref.get(f)) for f in FIELDS}
+    assert max(errs.values()) <= 1e-4, errs
