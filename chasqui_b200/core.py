@@ -80,6 +80,13 @@ SIGNATURES = [
     ("chq_profile", C.c_int, [_P, C.c_int]),
     ("chq_profile_read", C.c_int, [_P, _D, C.POINTER(C.c_longlong), C.c_int]),
     ("chq_kernel_launches", C.c_longlong, [_P]),
+    ("chq_batch_create", C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
+    ("chq_batch_destroy", C.c_int, [_P]),
+    ("chq_batch_cycles", C.c_int, [_P, C.c_int, _P]),
+    ("chq_batch_set_graph", C.c_int, [_P, C.c_int]),
+    ("chq_batch_status", C.c_int, [_P, _D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("chq_batch_kernel_launches", C.c_longlong, [_P]),
+    ("chq_batch_stream", _P, [_P]),
 ]
 
 PROFILE_KINDS = ("fluxes", "corner_emf", "update", "fofc_flag", "fofc_repair", "boundaries", "c2p_dt", "limiter",
@@ -288,6 +295,45 @@ class Mesh:
         self.set("b1f0", b1)
         self.set("b2f0", b2)
         self.set("b3f0", b3)
+
+
+class Batch:
+    """Many primed meshes of one class stepped together, one launch per kernel kind per stage."""
+
+    def __init__(self, meshes, graph: bool = False):
+        lib = load_library()
+        self.meshes = list(meshes)
+        arr = (_P * len(self.meshes))(*[m._h for m in self.meshes])
+        h = _P()
+        _check(lib.chq_batch_create(arr, len(self.meshes), C.byref(h)))
+        self._h = h
+        if graph:
+            _check(lib.chq_batch_set_graph(h, 1))
+
+    def cycles(self, n: int):
+        _check(load_library().chq_batch_cycles(self._h, n, None))
+
+    def status(self):
+        n = len(self.meshes)
+        t = (C.c_double * n)()
+        cyc = (C.c_int * n)()
+        done = (C.c_int * n)()
+        _check(load_library().chq_batch_status(self._h, t, cyc, done))
+        return [{"t": t[j], "cycle": cyc[j], "done": bool(done[j])} for j in range(n)]
+
+    def kernel_launches(self) -> int:
+        return int(load_library().chq_batch_kernel_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().chq_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def set_device(dev: int) -> None:

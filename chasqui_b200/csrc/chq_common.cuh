@@ -70,4 +70,30 @@ template <> struct Tiny<float> { static constexpr float v = 0.0f; static constex
 // read-only cached load
 template <class T> CHQ_D T ldg(const T *p) { return __ldg(p); }
 
+// Batched launches: one launch covers the blocks of many meshes. Job j owns the launch
+// blocks [off, off + gx*gy*gz) of the 1-D grid and sees them as its own (gx, gy, gz) grid.
+struct BatchSlot {
+  long off;
+  int gx, gy, gz, pad;
+};
+
+// the job whose block range holds launch block b (offsets are prefix sums; jobs without
+// blocks share the next job's offset and are skipped)
+CHQ_D int batch_job(const BatchSlot *s, int n, long b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s[mid].off <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+CHQ_D void batch_block(const BatchSlot &sl, long b, int &bx, int &by, int &bz) {
+  const long loc = b - sl.off;
+  bx = (int)(loc % sl.gx);
+  by = (int)((loc / sl.gx) % sl.gy);
+  bz = (int)(loc / ((long)sl.gx * sl.gy));
+}
+
 }  // namespace chq

@@ -45,33 +45,96 @@ template <class P> struct FluxArgs {
 };
 
 // ---------------------------------------------------------------------------------------
-// Cell work: the (aL, aR) pair of cell `lc` (linear index) for the 8 reconstructed
-// quantities (d, u, v, w, p, by, bz, s) in the frame of direction DIR.
-template <int DIR, int R, bool CHAR, class P>
-CHQ_D void cell_states(const FluxArgs<P> &A, long lc, P aL[8], P aR[8]) {
-  constexpr int IVU = IVX + DIR, IVV = IVX + (DIR + 1) % 3, IVW = IVX + (DIR + 2) % 3;
-  constexpr int IBT1 = (DIR + 1) % 3, IBT2 = (DIR + 2) % 3;
-  constexpr int RE = Reach<R>::v;
+// Per-direction views: the 8 reconstructed quantities (d, u, v, w, p, by, bz, s) of the
+// frame of direction d and the output slots of its faces. Built once per warp; the
+// arithmetic is identical for every direction, so one code copy serves the y and z sweeps.
+template <class P> struct DirView {
+  const P *src[8];     // cell fields in face-frame order
+  const P *bx;         // cell-centred normal field (characteristic projection)
+  long st;             // stride along the sweep
+  long s1, s2;         // strides of the two transverse directions (LHLLD detector)
+  int has1, has2;
+  const double *bn;    // face-normal field of the stage's current state
+  P *out[8];           // flux slots (d, u, v, w, E, s) then E_t2, E_t1
+};
+
+template <class P> CHQ_D DirView<P> dir_view(const FluxArgs<P> &A, int d) {
+  DirView<P> v;
   const long vs = A.g.vstride;
-  const long st = (DIR == 0) ? 1 : (DIR == 1) ? A.g.sj : A.g.sk;
-  const P *src[8] = {A.w + IDN * vs, A.w + IVU * vs, A.w + IVV * vs, A.w + IVW * vs,
-                     A.w + IPR * vs, A.bcc + IBT1 * vs, A.bcc + IBT2 * vs, A.w + IENT * vs};
-  P q[8][5];
-#pragma unroll
-  for (int n = 0; n < 8; ++n) {
-#pragma unroll
-    for (int m = -RE; m <= RE; ++m) q[n][2 + m] = ldg(src[n] + lc + m * st);
-#pragma unroll
-    for (int m = RE + 1; m <= 2; ++m) { q[n][2 + m] = q[n][2 + RE]; q[n][2 - m] = q[n][2 - RE]; }
-  }
+  const int ivu = IVX + d, ivv = IVX + (d + 1) % 3, ivw = IVX + (d + 2) % 3;
+  const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+  const long strides[3] = {1, A.g.sj, A.g.sk};
+  v.src[0] = A.w + IDN * vs;
+  v.src[1] = A.w + ivu * vs;
+  v.src[2] = A.w + ivv * vs;
+  v.src[3] = A.w + ivw * vs;
+  v.src[4] = A.w + IPR * vs;
+  v.src[5] = A.bcc + t1 * vs;
+  v.src[6] = A.bcc + t2 * vs;
+  v.src[7] = A.w + IENT * vs;
+  v.bx = A.bcc + d * vs;
+  v.st = strides[d];
+  v.s1 = strides[t1];
+  v.s2 = strides[t2];
+  v.has1 = (t1 == 0) || (t1 == 1 && A.g.two_d) || (t1 == 2 && A.g.three_d);
+  v.has2 = (t2 == 0) || (t2 == 1 && A.g.two_d) || (t2 == 2 && A.g.three_d);
+  v.bn = A.bn[d];
+  P *f = A.flx[d];
+  v.out[0] = f + IDN * vs;
+  v.out[1] = f + ivu * vs;
+  v.out[2] = f + ivv * vs;
+  v.out[3] = f + ivw * vs;
+  v.out[4] = f + IEN * vs;
+  v.out[5] = f + IENT * vs;
+  v.out[6] = A.et2[d];
+  v.out[7] = A.et1[d];
+  return v;
+}
+
+// ---------------------------------------------------------------------------------------
+// Cell work: the (aL, aR) pair of cell `lc` (linear index) for the 8 reconstructed
+// quantities in the frame of the view's direction. Each quantity is reconstructed as soon
+// as its stencil is loaded, so only the cell values (for flattening and the floor
+// fallback) stay live across quantities.
+template <int R, bool CHAR, class P>
+CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, long lc, P aL[8], P aR[8]) {
+  constexpr int RE = Reach<R>::v;
+  const long st = V.st;
+  P qc[8];
+  P p5[5], um1 = P(0), up1 = P(0);
   if constexpr (!CHAR || R == R_DC) {
 #pragma unroll
-    for (int n = 0; n < 7; ++n) recon_cell<R>(q[n], aL[n], aR[n]);
+    for (int n = 0; n < 8; ++n) {
+      P q5[5];
+#pragma unroll
+      for (int m = -RE; m <= RE; ++m) q5[2 + m] = ldg(V.src[n] + lc + m * st);
+#pragma unroll
+      for (int m = RE + 1; m <= 2; ++m) { q5[2 + m] = q5[2 + RE]; q5[2 - m] = q5[2 - RE]; }
+      recon_cell<R>(q5, aL[n], aR[n]);
+      qc[n] = q5[2];
+      if (n == 1) { um1 = q5[1]; up1 = q5[3]; }
+      if (n == 4) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) p5[m] = q5[m];
+      }
+    }
   } else {
     // characteristic projection with this cell's own eigenvectors (src/physics.hpp:108-150)
+    P q[7][5];
+#pragma unroll
+    for (int n = 0; n < 7; ++n) {
+#pragma unroll
+      for (int m = -RE; m <= RE; ++m) q[n][2 + m] = ldg(V.src[n] + lc + m * st);
+#pragma unroll
+      for (int m = RE + 1; m <= 2; ++m) { q[n][2 + m] = q[n][2 + RE]; q[n][2 - m] = q[n][2 - RE]; }
+      qc[n] = q[n][2];
+    }
+    um1 = q[1][1];
+    up1 = q[1][3];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) p5[m] = q[4][m];
     Eigen7<P> E;
-    const P bx = ldg(A.bcc + DIR * vs + lc);
-    eigensystem<P>(q[0][2], q[4][2], q[5][2], q[6][2], bx, P(A.eos.gamma), E);
+    eigensystem<P>(q[0][2], q[4][2], q[5][2], q[6][2], ldg(V.bx + lc), P(A.eos.gamma), E);
     P cL[7], cR[7];
 #pragma unroll
     for (int kk = 0; kk < 7; ++kk) {
@@ -98,16 +161,23 @@ CHQ_D void cell_states(const FluxArgs<P> &A, long lc, P aL[8], P aR[8]) {
       aL[n] = accL;
       aR[n] = accR;
     }
+    // entropy scalar, always primitive
+    P q5[5];
+#pragma unroll
+    for (int m = -RE; m <= RE; ++m) q5[2 + m] = ldg(V.src[7] + lc + m * st);
+#pragma unroll
+    for (int m = RE + 1; m <= 2; ++m) { q5[2 + m] = q5[2 + RE]; q5[2 - m] = q5[2 - RE]; }
+    recon_cell<R>(q5, aL[7], aR[7]);
+    qc[7] = q5[2];
   }
-  recon_cell<R>(q[7], aL[7], aR[7]);   // entropy scalar, always primitive
   if constexpr (R == R_PPM || R == R_PPMX || R == R_WENOZ) {
     if (A.flatten) {
-      const P f = flattening<P>(q[4], q[1][1], q[1][3]);
+      const P f = flattening<P>(p5, um1, up1);
       if (f > P(0)) {
 #pragma unroll
         for (int n = 0; n < 8; ++n) {
-          aL[n] += f * (q[n][2] - aL[n]);
-          aR[n] += f * (q[n][2] - aR[n]);
+          aL[n] += f * (qc[n] - aL[n]);
+          aR[n] += f * (qc[n] - aR[n]);
         }
       }
     }
@@ -116,24 +186,22 @@ CHQ_D void cell_states(const FluxArgs<P> &A, long lc, P aL[8], P aR[8]) {
   const P dfl = P(A.eos.dfloor), pfl = P(A.eos.pfloor);
   if (aL[0] <= dfl || aL[4] <= pfl) {
 #pragma unroll
-    for (int n = 0; n < 8; ++n) aL[n] = q[n][2];
+    for (int n = 0; n < 8; ++n) aL[n] = qc[n];
   }
   if (aR[0] <= dfl || aR[4] <= pfl) {
 #pragma unroll
-    for (int n = 0; n < 8; ++n) aR[n] = q[n][2];
+    for (int n = 0; n < 8; ++n) aR[n] = qc[n];
   }
 }
 
 // ---------------------------------------------------------------------------------------
 // Face work: Riemann solve of the face `lf` (between cells lf - stride and lf).
-template <int DIR, int S, class P>
-CHQ_D void face_flux(const FluxArgs<P> &A, long lf, const P wl[8], const P wr[8]) {
-  constexpr int IVU = IVX + DIR, IVV = IVX + (DIR + 1) % 3, IVW = IVX + (DIR + 2) % 3;
-  const long vs = A.g.vstride;
+template <int S, class P>
+CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, long lf, const P wl[8], const P wr[8]) {
   const P gamma = P(A.eos.gamma), gm1 = P(A.eos.gm1);
   MState<P> L{wl[0], wl[1], wl[2], wl[3], wl[4], wl[5], wl[6]};
   MState<P> R{wr[0], wr[1], wr[2], wr[3], wr[4], wr[5], wr[6]};
-  const P b_n = P(A.bn[DIR][lf]);
+  const P b_n = P(V.bn[lf]);
   if (A.low_mach) {
     // Thornber et al. (2008) blend of the normal velocities (src/physics.hpp:170-178)
     const P cl = fast_speed(L, b_n, gamma), cr = fast_speed(R, b_n, gamma);
@@ -147,23 +215,18 @@ CHQ_D void face_flux(const FluxArgs<P> &A, long lf, const P wl[8], const P wr[8]
     hlld<false>(L, R, b_n, gamma, gm1, f, P(1), P(1));
   } else if constexpr (S == S_LHLLD) {
     // shock detector theta and low-Mach factor phi (src/physics.hpp:183-211)
-    constexpr int t1 = (DIR + 1) % 3, t2 = (DIR + 2) % 3;
-    const long st = (DIR == 0) ? 1 : (DIR == 1) ? A.g.sj : A.g.sk;
-    const long s1 = (t1 == 0) ? 1 : (t1 == 1) ? A.g.sj : A.g.sk;
-    const long s2 = (t2 == 0) ? 1 : (t2 == 1) ? A.g.sj : A.g.sk;
-    const bool has_t1 = (t1 == 0) || (t1 == 1 && A.g.two_d) || (t1 == 2 && A.g.three_d);
-    const bool has_t2 = (t2 == 0) || (t2 == 1 && A.g.two_d) || (t2 == 2 && A.g.three_d);
-    const long lL = lf - st;
+    const long lL = lf - V.st;
     const P cfmax = fmax_(fast_speed(L, b_n, gamma), fast_speed(R, b_n, gamma));
-    const P *wu = A.w + IVU * vs, *wv = A.w + IVV * vs, *ww = A.w + IVW * vs;
+    const P *wu = V.src[1], *wv = V.src[2], *ww = V.src[3];
+    const long s1 = V.s1, s2 = V.s2;
     const P du = ldg(wu + lf) - ldg(wu + lL);
     P dvw = P(0);
-    if (has_t1) {
+    if (V.has1) {
       const P d1 = fmin_(fmin_(ldg(wv + lL) - ldg(wv + lL - s1), ldg(wv + lL + s1) - ldg(wv + lL)),
                          fmin_(ldg(wv + lf) - ldg(wv + lf - s1), ldg(wv + lf + s1) - ldg(wv + lf)));
       dvw = fmin_(dvw, d1);
     }
-    if (has_t2) {
+    if (V.has2) {
       const P d2 = fmin_(fmin_(ldg(ww + lL) - ldg(ww + lL - s2), ldg(ww + lL + s2) - ldg(ww + lL)),
                          fmin_(ldg(ww + lf) - ldg(ww + lf - s2), ldg(ww + lf + s2) - ldg(ww + lf)));
       dvw = fmin_(dvw, d2);
@@ -177,17 +240,16 @@ CHQ_D void face_flux(const FluxArgs<P> &A, long lf, const P wl[8], const P wr[8]
   } else {
     hlle(L, R, b_n, gamma, gm1, f);
   }
-  P *flx = A.flx[DIR];
-  flx[IDN * vs + lf] = f[FD];
-  flx[IVU * vs + lf] = f[FMU];
-  flx[IVV * vs + lf] = f[FMV];
-  flx[IVW * vs + lf] = f[FMW];
-  flx[IEN * vs + lf] = f[FEN];
+  V.out[0][lf] = f[FD];
+  V.out[1][lf] = f[FMU];
+  V.out[2][lf] = f[FMV];
+  V.out[3][lf] = f[FMW];
+  V.out[4][lf] = f[FEN];
   // entropy flux upwinded with the mass flux, averaged at an exact zero
   const P sl = wl[7], sr = wr[7];
-  flx[IENT * vs + lf] = (f[FD] > P(0)) ? f[FD] * sl : (f[FD] < P(0)) ? f[FD] * sr : P(0.5) * (f[FD] * (sl + sr));
-  A.et2[DIR][lf] = -f[FBY];
-  A.et1[DIR][lf] = f[FBZ];
+  V.out[5][lf] = (f[FD] > P(0)) ? f[FD] * sl : (f[FD] < P(0)) ? f[FD] * sr : P(0.5) * (f[FD] * (sl + sr));
+  V.out[6][lf] = -f[FBY];
+  V.out[7][lf] = f[FBZ];
 }
 
 // ---------------------------------------------------------------------------------------
@@ -202,57 +264,91 @@ CHQ_D void sweep_x(const FluxArgs<P> &A, long wid) {
   const int j = A.lo[0][1] + (int)(row - (long)(row / nj) * nj);
   const int c = A.lo[0][2] - 1 + 31 * seg + lane;   // this lane's cell
   const bool have = (c <= A.hi[0][2]);
+  const DirView<P> V = dir_view(A, 0);
   P aL[8], aR[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) { aL[n] = P(0); aR[n] = P(0); }
   const long lc = A.g.idx(k, j, c);
-  if (have) cell_states<0, R, CHAR, P>(A, lc, aL, aR);
+  if (have) cell_states<R, CHAR, P>(A, V, lc, aL, aR);
   P wl[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) wl[n] = __shfl_up_sync(0xffffffffu, aR[n], 1);
-  if (have && lane > 0) face_flux<0, S, P>(A, lc, wl, aL);
+  if (have && lane > 0) face_flux<S, P>(A, V, lc, wl, aL);
 }
 
-template <int DIR, int R, int S, bool CHAR, class P>
-CHQ_D void sweep_yz(const FluxArgs<P> &A, long wid) {
+// y (d = 1) or z (d = 2) sweep: one code copy, direction in the view. The right state
+// carried to the next face is parked in this thread's shared-memory slot during the
+// Riemann solve, which keeps it out of the registers at the solver's peak.
+template <int R, int S, bool CHAR, class P>
+CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, long wid, P (*park)[128]) {
   const int lane = threadIdx.x & 31;
-  const int nseg = A.nseg[DIR];
+  const int nseg = A.nseg[d];
   const int nchunk = A.nchunk;
-  // warp id -> (outer transverse index, segment, i chunk)
   const int chunk = (int)(wid % nchunk);
   const long rest = wid / nchunk;
   const int seg = (int)(rest % nseg);
   const int outer = (int)(rest / nseg);
   const int i = 32 * chunk + lane;
-  if (i < A.lo[DIR][2] || i > A.hi[DIR][2]) return;
-  const int f0 = A.lo[DIR][DIR == 1 ? 1 : 0] + A.seglen * seg;
-  const int f1 = min(f0 + A.seglen - 1, A.hi[DIR][DIR == 1 ? 1 : 0]);
-  const long st = (DIR == 1) ? A.g.sj : A.g.sk;
-  long lc;
-  if (DIR == 1) lc = A.g.idx(A.lo[1][0] + outer, f0 - 1, i);
-  else lc = A.g.idx(f0 - 1, A.lo[2][1] + outer, i);
+  if (i < A.lo[d][2] || i > A.hi[d][2]) return;
+  const int sweep_lo = (d == 1) ? A.lo[1][1] : A.lo[2][0];
+  const int sweep_hi = (d == 1) ? A.hi[1][1] : A.hi[2][0];
+  const int f0 = sweep_lo + A.seglen * seg;
+  const int f1 = min(f0 + A.seglen - 1, sweep_hi);
+  const DirView<P> V = dir_view(A, d);
+  long lc = (d == 1) ? A.g.idx(A.lo[1][0] + outer, f0 - 1, i) : A.g.idx(f0 - 1, A.lo[2][1] + outer, i);
   P aL[8], aR[8], wl[8];
-  cell_states<DIR, R, CHAR, P>(A, lc, aL, aR);
+  cell_states<R, CHAR, P>(A, V, lc, aL, aR);
 #pragma unroll
   for (int n = 0; n < 8; ++n) wl[n] = aR[n];
+  const int t = threadIdx.x;
   for (int f = f0; f <= f1; ++f) {
-    lc += st;
-    cell_states<DIR, R, CHAR, P>(A, lc, aL, aR);
-    face_flux<DIR, S, P>(A, lc, wl, aL);
+    lc += V.st;
+    cell_states<R, CHAR, P>(A, V, lc, aL, aR);
 #pragma unroll
-    for (int n = 0; n < 8; ++n) wl[n] = aR[n];
+    for (int n = 0; n < 8; ++n) park[n][t] = aR[n];
+    face_flux<S, P>(A, V, lc, wl, aL);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) wl[n] = park[n][t];
+  }
+}
+
+// Resident 128-thread blocks per SM the flux kernel is compiled for (register cap). The
+// kernel is bound by FP64 / FP32 instruction latency, so more resident warps pay even with
+// some spilling to L1: measured best at 5 (FP64, 96 registers) and 6 (FP32).
+#ifndef CHQ_FLUX_MINB_D
+#define CHQ_FLUX_MINB_D 5
+#endif
+#ifndef CHQ_FLUX_MINB_F
+#define CHQ_FLUX_MINB_F 6
+#endif
+template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUX_MINB_D : CHQ_FLUX_MINB_F; };
+
+template <int R, int S, bool CHAR, class P>
+CHQ_D void flux_body(const FluxArgs<P> &A, long block, P (*park)[128]) {
+  if (A.skip && *A.skip) return;
+  const long wid = block * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long nz = A.nwarp[2], nyz = A.nwarp[2] + A.nwarp[1];
+  if (wid < nyz) {
+    const int d = (wid < nz) ? 2 : 1;
+    sweep_yz<R, S, CHAR, P>(A, d, (d == 2) ? wid : wid - nz, park);
+  } else if (wid < nyz + A.nwarp[0]) {
+    sweep_x<R, S, CHAR, P>(A, wid - nyz);
   }
 }
 
 template <int R, int S, bool CHAR, class P>
-__global__ void __launch_bounds__(128) flux_kernel(const FluxArgs<P> A) {
-  if (A.skip && *A.skip) return;
-  const long wid = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (wid < A.nwarp[2]) {
-    sweep_yz<2, R, S, CHAR, P>(A, wid);
-  } else if (wid < A.nwarp[2] + A.nwarp[1]) {
-    sweep_yz<1, R, S, CHAR, P>(A, wid - A.nwarp[2]);
-  } else if (wid < A.nwarp[2] + A.nwarp[1] + A.nwarp[0]) {
-    sweep_x<R, S, CHAR, P>(A, wid - A.nwarp[2] - A.nwarp[1]);
-  }
+__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_kernel(const FluxArgs<P> A) {
+  __shared__ P park[8][128];
+  flux_body<R, S, CHAR, P>(A, blockIdx.x, park);
+}
+
+// batched form: the blocks of many meshes in one launch (chq_batch)
+template <int R, int S, bool CHAR, class P>
+__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
+  __shared__ P park[8][128];
+  const int j = batch_job(slots, n, blockIdx.x);
+  const FluxArgs<P> A = args[j];
+  flux_body<R, S, CHAR, P>(A, (long)blockIdx.x - slots[j].off, park);
 }
 
 }  // namespace chq

@@ -31,6 +31,25 @@ cudaError_t launch_flux<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> &a, int rsolver, int
 }
 
 template <int S, bool C>
+static cudaError_t gob(const FluxArgs<CHQ_P> *a, const BatchSlot *sl, int n, unsigned nblocks, cudaStream_t s) {
+  flux_batched<CHQ_R, S, C, CHQ_P><<<nblocks, 128, 0, s>>>(a, sl, n);
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_flux_batched<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> *a, const BatchSlot *sl, int n, int rsolver,
+                                               int charac, unsigned nblocks, cudaStream_t s) {
+  if (nblocks == 0) return cudaSuccess;
+  const bool c = (charac != 0) && (CHQ_R != R_DC);
+  switch (rsolver) {
+    case S_HLLE: return c ? gob<S_HLLE, true>(a, sl, n, nblocks, s) : gob<S_HLLE, false>(a, sl, n, nblocks, s);
+    case S_HLLD: return c ? gob<S_HLLD, true>(a, sl, n, nblocks, s) : gob<S_HLLD, false>(a, sl, n, nblocks, s);
+    case S_LHLLD: return c ? gob<S_LHLLD, true>(a, sl, n, nblocks, s) : gob<S_LHLLD, false>(a, sl, n, nblocks, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int S, bool C>
 static int regs() {
   cudaFuncAttributes at{};
   if (cudaFuncGetAttributes(&at, flux_kernel<CHQ_R, S, C, CHQ_P>) != cudaSuccess) return -1;

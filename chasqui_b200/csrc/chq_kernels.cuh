@@ -33,13 +33,13 @@ template <class P> CHQ_D P upwind(P flux, P left, P right) {
   return (flux > tol) ? left : (flux < -tol) ? right : P(0.5) * (left + right);
 }
 
-template <class P> __global__ void __launch_bounds__(256) corner_emf_kernel(const EmfArgs<P> A) {
+template <class P> CHQ_D void corner_emf_body(const EmfArgs<P> &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
   if (A.need && *A.need == 0) return;
   const Geom &g = A.g;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   const long vs = g.vstride;
   const long sj = g.sj, sk = g.sk;
   if (i > g.ie + 1) return;
@@ -91,6 +91,8 @@ template <class P> __global__ void __launch_bounds__(256) corner_emf_kernel(cons
   }
 }
 
+template <class P> __global__ void __launch_bounds__(256) corner_emf_kernel(const EmfArgs<P> A) { corner_emf_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+
 // ---------------------------------------------------------------------------------------
 // K3. Each thread owns one (k, j, i) of the face/edge frame: the cell update when (k, j, i)
 // is an active cell and the x1/x2/x3 face updates when it is an active face. The reads of
@@ -132,13 +134,13 @@ template <class P> CHQ_D double new_b3(const UpdateArgs<P> &A, long l, double g0
   return g0 * A.b3a[l] + g1 * A.b3b[l] - bdt * curl;
 }
 
-template <class P> __global__ void __launch_bounds__(256) update_kernel(const UpdateArgs<P> A) {
+template <class P> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
   if (A.need && *A.need == 0) return;
   const Geom &g = A.g;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   if (i > g.ie + 1 || j > g.je + 1 || k > g.ke + 1) return;
   const double g0 = A.g0, g1 = A.g1;
   const double bdt = A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt;
@@ -175,6 +177,8 @@ template <class P> __global__ void __launch_bounds__(256) update_kernel(const Up
   }
 }
 
+template <class P> __global__ void __launch_bounds__(256) update_kernel(const UpdateArgs<P> A) { update_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+
 // ---------------------------------------------------------------------------------------
 // FOFC flag of the tentative state (src/fofc.hpp:17-43): rho <= dfloor or p <= pfloor,
 // written for every active cell, with a warp-aggregated count into *nbad.
@@ -187,12 +191,12 @@ struct FlagArgs {
   const int *done;
 };
 
-__global__ void __launch_bounds__(256) fofc_flag_kernel(const FlagArgs A) {
+CHQ_D void fofc_flag_body(const FlagArgs &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
   const Geom &g = A.g;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   int bad = 0;
   if (i <= g.ie && j <= g.je) {
     const long vs = g.vstride;
@@ -216,6 +220,8 @@ __global__ void __launch_bounds__(256) fofc_flag_kernel(const FlagArgs A) {
   const unsigned m = __ballot_sync(0xffffffffu, bad != 0);
   if (m && (threadIdx.x & 31) == 0) atomicAdd(A.nbad, __popc(m));
 }
+
+__global__ void __launch_bounds__(256) fofc_flag_kernel(const FlagArgs A) { fofc_flag_body(A, blockIdx.x, blockIdx.y, blockIdx.z); }
 
 // ---------------------------------------------------------------------------------------
 // FOFC repair: first-order (donor cell) HLLE fluxes on faces touching a flagged cell,
@@ -264,10 +270,10 @@ template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k
   A.et1[DIR][l] = f[FBZ];
 }
 
-template <class P> __global__ void __launch_bounds__(256) fofc_repair_kernel(const RepairArgs<P> A) {
+template <class P> CHQ_D void fofc_repair_body(const RepairArgs<P> &A, int bx) {
   if (A.done && *A.done) return;
   if (A.need && *A.need == 0) return;
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long t = (long)bx * blockDim.x + threadIdx.x;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (t < A.nface[d]) {
@@ -284,6 +290,8 @@ template <class P> __global__ void __launch_bounds__(256) fofc_repair_kernel(con
     t -= A.nface[d];
   }
 }
+
+template <class P> __global__ void __launch_bounds__(256) fofc_repair_kernel(const RepairArgs<P> A) { fofc_repair_body<P>(A, blockIdx.x); }
 
 // ---------------------------------------------------------------------------------------
 // Positivity flux limiter (Hu, Adams & Shu 2013) on the active faces of each direction.
@@ -373,10 +381,10 @@ template <int DIR, class P> CHQ_D int limit_face(const LimitArgs<P> &A, int k, i
   return 1;
 }
 
-template <class P> __global__ void __launch_bounds__(256) limit_kernel(const LimitArgs<P> A) {
+template <class P> CHQ_D void limit_body(const LimitArgs<P> &A, int bx) {
   if (A.done && *A.done) return;
   const double bdt = A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt;
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long t = (long)bx * blockDim.x + threadIdx.x;
   int lim = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -398,6 +406,8 @@ template <class P> __global__ void __launch_bounds__(256) limit_kernel(const Lim
   if (m && (threadIdx.x & 31) == (__ffs(__activemask()) - 1)) atomicAdd((unsigned long long *)A.count, (unsigned long long)__popc(m));
 }
 
+template <class P> __global__ void __launch_bounds__(256) limit_kernel(const LimitArgs<P> A) { limit_body<P>(A, blockIdx.x); }
+
 // ---------------------------------------------------------------------------------------
 // K4 ghost fill; DIR selects the x1, x2 or x3 slabs. Must run x1, x2, x3 in order.
 struct BcArgs {
@@ -407,14 +417,14 @@ struct BcArgs {
   const int *done;
 };
 
-template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs A) {
+template <int DIR> CHQ_D void bc_body(const BcArgs &A, int bx) {
   if (A.done && *A.done) return;
   const Geom &g = A.g;
   const long vs = g.vstride;
   const double sgn = (A.bc == BC_REFLECT) ? -1.0 : 1.0;
   if (DIR == 0) {
     // threads over (k in [0,nk], j in [0,nj], gh in [0,ng))
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long t = (long)bx * blockDim.x + threadIdx.x;
     const int gh = (int)(t % g.ng);
     const long r = t / g.ng;
     const int j = (int)(r % (g.nj + 1));
@@ -441,7 +451,7 @@ template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs
     if (A.bc == 0 && gh == 0) A.b1[row + g.ie + 1] = A.b1[row + g.is];
   } else if (DIR == 1) {
     // threads over (k in [0,nk], gh in [0,ng), i in [0,ni])
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long t = (long)bx * blockDim.x + threadIdx.x;
     const int i = (int)(t % (g.ni + 1));
     const long r = t / (g.ni + 1);
     const int gh = (int)(r % g.ng);
@@ -469,7 +479,7 @@ template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs
     if (A.bc == 0 && gh == 0) A.b2[g.idx(k, g.je + 1, i)] = A.b2[g.idx(k, g.js, i)];
   } else {
     // threads over (gh in [0,ng), j in [0,nj], i in [0,ni])
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long t = (long)bx * blockDim.x + threadIdx.x;
     const int i = (int)(t % (g.ni + 1));
     const long r = t / (g.ni + 1);
     const int j = (int)(r % (g.nj + 1));
@@ -498,6 +508,8 @@ template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs
   }
 }
 
+template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs A) { bc_body<DIR>(A, blockIdx.x); }
+
 // ---------------------------------------------------------------------------------------
 // K5
 template <class P> struct C2pArgs {
@@ -512,16 +524,16 @@ template <class P> struct C2pArgs {
   const int *done;
 };
 
-template <class P> __global__ void __launch_bounds__(256) c2p_kernel(const C2pArgs<P> A) {
+template <class P> CHQ_D void c2p_body(const C2pArgs<P> &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
   const Geom &g = A.g;
-  if (A.ctl && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+  if (A.ctl && bx == 0 && by == 0 && bz == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
     A.ctl->fofc_count += A.ctl->nbad;
     A.ctl->nbad = 0;
   }
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz;
   double mdt = __longlong_as_double(0x7ff0000000000000LL);   // +inf
   if (i < g.ni && j < g.nj && k < g.nk) {
     const long vs = g.vstride;
@@ -578,6 +590,54 @@ template <class P> __global__ void __launch_bounds__(256) c2p_kernel(const C2pAr
     for (int o = 16; o > 0; o >>= 1) mdt = fmin(mdt, __shfl_xor_sync(0xffffffffu, mdt, o));
     if ((threadIdx.x & 31) == 0) atomic_min_pos(A.mdt_bits, mdt);
   }
+}
+
+template <class P> __global__ void __launch_bounds__(256) c2p_kernel(const C2pArgs<P> A) { c2p_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+
+// ---------------------------------------------------------------------------------------
+// Batched forms: the same bodies, one launch over the blocks of many meshes (chq_batch).
+template <class P> __global__ void __launch_bounds__(256) corner_emf_batched(const EmfArgs<P> *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  const EmfArgs<P> A = args[j];
+  corner_emf_body<P>(A, bx, by, bz);
+}
+template <class P> __global__ void __launch_bounds__(256) update_batched(const UpdateArgs<P> *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  const UpdateArgs<P> A = args[j];
+  update_body<P>(A, bx, by, bz);
+}
+__global__ void __launch_bounds__(256) fofc_flag_batched(const FlagArgs *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  const FlagArgs A = args[j];
+  fofc_flag_body(A, bx, by, bz);
+}
+template <class P> __global__ void __launch_bounds__(256) fofc_repair_batched(const RepairArgs<P> *args, const BatchSlot *slots, int n) {
+  const int j = batch_job(slots, n, blockIdx.x);
+  const RepairArgs<P> A = args[j];
+  fofc_repair_body<P>(A, (int)(blockIdx.x - slots[j].off));
+}
+template <class P> __global__ void __launch_bounds__(256) limit_batched(const LimitArgs<P> *args, const BatchSlot *slots, int n) {
+  const int j = batch_job(slots, n, blockIdx.x);
+  const LimitArgs<P> A = args[j];
+  limit_body<P>(A, (int)(blockIdx.x - slots[j].off));
+}
+template <int DIR> __global__ void __launch_bounds__(256) bc_batched(const BcArgs *args, const BatchSlot *slots, int n) {
+  const int j = batch_job(slots, n, blockIdx.x);
+  const BcArgs A = args[j];
+  bc_body<DIR>(A, (int)(blockIdx.x - slots[j].off));
+}
+template <class P> __global__ void __launch_bounds__(256) c2p_batched(const C2pArgs<P> *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  const C2pArgs<P> A = args[j];
+  c2p_body<P>(A, bx, by, bz);
 }
 
 }  // namespace chq

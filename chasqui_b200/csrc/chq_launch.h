@@ -9,6 +9,10 @@ namespace chq {
 template <class P, int R>
 cudaError_t launch_flux(const FluxArgs<P> &a, int rsolver, int charac, unsigned nblocks, cudaStream_t s);
 
+template <class P, int R>
+cudaError_t launch_flux_batched(const FluxArgs<P> *args, const BatchSlot *slots, int njobs, int rsolver, int charac,
+                                unsigned nblocks, cudaStream_t s);
+
 // registers per thread of the instantiated kernel (for the launch report)
 template <class P, int R>
 int flux_regs(int rsolver, int charac);

@@ -38,10 +38,14 @@ int cuda_fail(cudaError_t e, const char *where) {
 
 }  // namespace
 
+namespace chq {
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace chq
+
 // ---------------------------------------------------------------------------------------
 // device control kernels
 namespace chq {
-__global__ void ctl_begin_kernel(StepCtl *c, int) {
+CHQ_D void ctl_begin(StepCtl *c) {
   if (c->done) return;
   if (!(c->t < c->tlim)) { c->done = 1; return; }
   double dt = c->cfl * c->min_dt;
@@ -50,11 +54,29 @@ __global__ void ctl_begin_kernel(StepCtl *c, int) {
   for (int s = 0; s < c->nstage; ++s) c->beta_dt[s] = c->beta[s] * dt;
   c->mdt_bits = 0x7ff0000000000000ULL;
 }
-__global__ void ctl_end_kernel(StepCtl *c) {
+CHQ_D void ctl_end(StepCtl *c) {
   if (c->done) return;
   c->t += c->dt;
   c->cycle += 1;
   c->min_dt = __longlong_as_double((long long)c->mdt_bits);
+}
+__global__ void ctl_begin_kernel(StepCtl *c, int) { ctl_begin(c); }
+__global__ void ctl_end_kernel(StepCtl *c) { ctl_end(c); }
+__global__ void ctl_begin_batched(StepCtl *const *c, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) ctl_begin(c[j]);
+}
+__global__ void ctl_end_batched(StepCtl *const *c, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) ctl_end(c[j]);
+}
+__global__ void batch_status_kernel(StepCtl *const *c, int n, double *out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) {
+    out[3 * j] = c[j]->t;
+    out[3 * j + 1] = (double)c[j]->cycle;
+    out[3 * j + 2] = (double)c[j]->done;
+  }
 }
 __global__ void ctl_prime_kernel(StepCtl *c, double t) {
   c->t = t;
@@ -291,8 +313,12 @@ int do_fluxes(chq_mesh *m, int cur, unsigned dirmask, const int *done, cudaStrea
 }
 
 // ---- corner EMF ----------------------------------------------------------------------
+struct Launch3 {
+  dim3 grid, block;
+};
+
 template <class P>
-int do_corner(chq_mesh *m, const int *done, const int *need, cudaStream_t s) {
+EmfArgs<P> corner_args(chq_mesh *m, const int *done, const int *need) {
   const Geom &g = m->g;
   EmfArgs<P> a{};
   a.g = g;
@@ -304,19 +330,30 @@ int do_corner(chq_mesh *m, const int *done, const int *need, cudaStream_t s) {
   a.e1 = as<P>(m->e[0]); a.e2 = as<P>(m->e[1]); a.e3 = as<P>(m->e[2]);
   a.done = done;
   a.need = need;
+  return a;
+}
+
+Launch3 corner_grid(const chq_mesh *m) {
+  const Geom &g = m->g;
   const int nxi = g.ie + 2 - g.is, nyj = g.je + 2 - g.js;
   const int nzk = g.three_d ? g.ke + 2 - g.ks : 1;
-  dim3 blk(32, 8), grd((nxi + 31) / 32, (nyj + 7) / 8, nzk);
+  return {dim3((nxi + 31) / 32, (nyj + 7) / 8, nzk), dim3(32, 8)};
+}
+
+template <class P>
+int do_corner(chq_mesh *m, const int *done, const int *need, cudaStream_t s) {
+  const EmfArgs<P> a = corner_args<P>(m, done, need);
+  const Launch3 L = corner_grid(m);
   m->nlaunch += 1;
-  corner_emf_kernel<P><<<grd, blk, 0, s>>>(a);
+  corner_emf_kernel<P><<<L.grid, L.block, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
 
 // ---- update --------------------------------------------------------------------------
 template <class P>
-int do_update(chq_mesh *m, int out, double g0, double g1, double bdt, const double *bdt_dev, const int *done,
-              const int *need, cudaStream_t s) {
+UpdateArgs<P> update_args(chq_mesh *m, int out, double g0, double g1, double bdt, const double *bdt_dev,
+                          const int *done, const int *need) {
   const Geom &g = m->g;
   UpdateArgs<P> a{};
   a.g = g;
@@ -331,15 +368,27 @@ int do_update(chq_mesh *m, int out, double g0, double g1, double bdt, const doub
   a.idx1 = 1.0 / g.dx1; a.idx2 = 1.0 / g.dx2; a.idx3 = 1.0 / g.dx3;
   a.done = done;
   a.need = need;
+  return a;
+}
+
+Launch3 update_grid(const chq_mesh *m) {
+  const Geom &g = m->g;
   const int nxi = g.ie + 2 - g.is, nyj = g.je + 2 - g.js, nzk = g.ke + 2 - g.ks;
-  dim3 blk(32, 8), grd((nxi + 31) / 32, (nyj + 7) / 8, nzk);
+  return {dim3((nxi + 31) / 32, (nyj + 7) / 8, nzk), dim3(32, 8)};
+}
+
+template <class P>
+int do_update(chq_mesh *m, int out, double g0, double g1, double bdt, const double *bdt_dev, const int *done,
+              const int *need, cudaStream_t s) {
+  const UpdateArgs<P> a = update_args<P>(m, out, g0, g1, bdt, bdt_dev, done, need);
+  const Launch3 L = update_grid(m);
   m->nlaunch += 1;
-  update_kernel<P><<<grd, blk, 0, s>>>(a);
+  update_kernel<P><<<L.grid, L.block, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
 
-int do_flag(chq_mesh *m, int buf, int *nbad_dev, const int *done, cudaStream_t s) {
+FlagArgs flag_args(chq_mesh *m, int buf, int *nbad_dev, const int *done) {
   const Geom &g = m->g;
   FlagArgs a{};
   a.g = g;
@@ -349,21 +398,31 @@ int do_flag(chq_mesh *m, int buf, int *nbad_dev, const int *done, cudaStream_t s
   a.flag = m->flag;
   a.nbad = nbad_dev;
   a.done = done;
-  dim3 blk(32, 8), grd((g.nx1 + 31) / 32, (g.je - g.js + 1 + 7) / 8, g.ke - g.ks + 1);
+  return a;
+}
+
+Launch3 flag_grid(const chq_mesh *m) {
+  const Geom &g = m->g;
+  return {dim3((g.nx1 + 31) / 32, (g.je - g.js + 1 + 7) / 8, g.ke - g.ks + 1), dim3(32, 8)};
+}
+
+int do_flag(chq_mesh *m, int buf, int *nbad_dev, const int *done, cudaStream_t s) {
+  const FlagArgs a = flag_args(m, buf, nbad_dev, done);
+  const Launch3 L = flag_grid(m);
   m->nlaunch += 1;
-  fofc_flag_kernel<<<grd, blk, 0, s>>>(a);
+  fofc_flag_kernel<<<L.grid, L.block, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
 
 template <class P>
-int do_repair(chq_mesh *m, int cur, unsigned dirmask, const int *done, const int *need, cudaStream_t s) {
+RepairArgs<P> repair_args(chq_mesh *m, int cur, unsigned dirmask, const int *done, const int *need, long &tot) {
   RepairArgs<P> a{};
   a.g = m->g;
   a.eos = m->eos;
   a.w = as<P>(m->w);
   a.bcc = as<P>(m->bcc);
-  long tot = 0;
+  tot = 0;
   for (int d = 0; d < 3; ++d) {
     a.bn[d] = m->bf[cur][d];
     a.flx[d] = as<P>(m->flx[d]);
@@ -377,6 +436,13 @@ int do_repair(chq_mesh *m, int cur, unsigned dirmask, const int *done, const int
   a.flag = m->flag;
   a.done = done;
   a.need = need;
+  return a;
+}
+
+template <class P>
+int do_repair(chq_mesh *m, int cur, unsigned dirmask, const int *done, const int *need, cudaStream_t s) {
+  long tot = 0;
+  const RepairArgs<P> a = repair_args<P>(m, cur, dirmask, done, need, tot);
   if (tot == 0) return CHQ_OK;
   m->nlaunch += 1;
   fofc_repair_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
@@ -385,8 +451,8 @@ int do_repair(chq_mesh *m, int cur, unsigned dirmask, const int *done, const int
 }
 
 template <class P>
-int do_limit(chq_mesh *m, unsigned dirmask, double bdt, const double *bdt_dev, long long *count_dev, const int *done,
-             cudaStream_t s) {
+LimitArgs<P> limit_args(chq_mesh *m, unsigned dirmask, double bdt, const double *bdt_dev, long long *count_dev,
+                        const int *done, long &tot) {
   const Geom &g = m->g;
   LimitArgs<P> a{};
   a.g = g;
@@ -398,7 +464,7 @@ int do_limit(chq_mesh *m, unsigned dirmask, double bdt, const double *bdt_dev, l
   a.dx[0] = g.dx1; a.dx[1] = g.dx2; a.dx[2] = g.dx3;
   a.beta_dt = bdt;
   a.beta_dt_dev = bdt_dev;
-  long tot = 0;
+  tot = 0;
   for (int d = 0; d < 3; ++d) {
     a.flx[d] = as<P>(m->flx[d]);
     for (int q = 0; q < 3; ++q) { a.lo[d][q] = m->act_lo[d][q]; a.hi[d][q] = m->act_hi[d][q]; }
@@ -408,11 +474,37 @@ int do_limit(chq_mesh *m, unsigned dirmask, double bdt, const double *bdt_dev, l
   }
   a.count = count_dev;
   a.done = done;
+  return a;
+}
+
+template <class P>
+int do_limit(chq_mesh *m, unsigned dirmask, double bdt, const double *bdt_dev, long long *count_dev, const int *done,
+             cudaStream_t s) {
+  long tot = 0;
+  const LimitArgs<P> a = limit_args<P>(m, dirmask, bdt, bdt_dev, count_dev, done, tot);
   if (tot == 0) return CHQ_OK;
   m->nlaunch += 1;
   limit_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
+}
+
+BcArgs bc_args(chq_mesh *m, int buf, const int *done, int dir) {
+  BcArgs a{};
+  a.g = m->g;
+  a.u = m->u[buf];
+  a.b1 = m->bf[buf][0]; a.b2 = m->bf[buf][1]; a.b3 = m->bf[buf][2];
+  a.done = done;
+  a.bc = (dir == 0) ? m->cfg.bc1 : (dir == 1) ? m->cfg.bc2 : m->cfg.bc3;
+  return a;
+}
+
+// threads of the ghost-fill launch of one direction (0 when the direction is inactive)
+long bc_threads(const chq_mesh *m, int dir) {
+  const Geom &g = m->g;
+  if (dir == 0) return (long)(g.nk + 1) * (g.nj + 1) * g.ng;
+  if (dir == 1) return g.two_d ? (long)(g.nk + 1) * g.ng * (g.ni + 1) : 0;
+  return g.three_d ? (long)g.ng * (g.nj + 1) * (g.ni + 1) : 0;
 }
 
 int do_bc(chq_mesh *m, int buf, const int *done, cudaStream_t s) {
@@ -445,8 +537,7 @@ int do_bc(chq_mesh *m, int buf, const int *done, cudaStream_t s) {
 }
 
 template <class P>
-int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done,
-           cudaStream_t s) {
+C2pArgs<P> c2p_args(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done) {
   const Geom &g = m->g;
   C2pArgs<P> a{};
   a.g = g;
@@ -458,9 +549,21 @@ int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepC
   a.mdt_bits = bits;
   a.ctl = fold;
   a.done = done;
-  dim3 blk(32, 8), grd((g.ni + 31) / 32, (g.nj + 7) / 8, g.nk);
+  return a;
+}
+
+Launch3 c2p_grid(const chq_mesh *m) {
+  const Geom &g = m->g;
+  return {dim3((g.ni + 31) / 32, (g.nj + 7) / 8, g.nk), dim3(32, 8)};
+}
+
+template <class P>
+int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done,
+           cudaStream_t s) {
+  const C2pArgs<P> a = c2p_args<P>(m, buf, compute_dt, bits, fold, done);
+  const Launch3 L = c2p_grid(m);
   m->nlaunch += 1;
-  c2p_kernel<P><<<grd, blk, 0, s>>>(a);
+  c2p_kernel<P><<<L.grid, L.block, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
@@ -579,6 +682,241 @@ int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaS
     }
   }
   return CHQ_OK;
+}
+
+}  // namespace
+
+
+// =======================================================================================
+// Batched stepping: the meshes of one class (same precision, reconstruction, Riemann
+// solver, characteristic flag, integrator, FOFC and limiter switches) advance together with
+// one launch per kernel kind per stage. Each mesh keeps its own StepCtl (dt, clock, FOFC
+// decision), so results are identical to stepping it alone.
+struct chq_batch {
+  std::vector<chq_mesh *> jobs;
+  int mixed = 0, recon = 0, rsolver = 0, charac = 0, nstage = 0, fofc = 0, limiter = 0;
+  cudaStream_t stream = nullptr;
+  char *dev = nullptr;
+  struct Kind {
+    BatchSlot *slots = nullptr;
+    long nblocks = 0;
+  };
+  Kind k_flux, k_corner, k_update, k_flag, k_repair, k_limit, k_bc[3], k_c2p;
+  void *a_flux[4] = {}, *a_update[4] = {}, *a_update_need[4] = {}, *a_repair[4] = {}, *a_limit[4] = {},
+       *a_c2p[4] = {}, *a_flag[4] = {}, *a_bc[4][3] = {};
+  void *a_corner = nullptr, *a_corner_need = nullptr;
+  StepCtl **ctls = nullptr;
+  double *status = nullptr;
+  bool use_graph = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long nlaunch = 0;
+  long long per_cycle = 0;   // launches in one captured cycle
+};
+
+namespace {
+
+struct HostTable {
+  std::vector<char> b;
+  size_t push(const void *p, size_t n) {
+    const size_t off = (b.size() + 255) & ~size_t(255);
+    b.resize(off + n);
+    std::memcpy(b.data() + off, p, n);
+    return off;
+  }
+};
+
+template <class T>
+size_t push_vec(HostTable &h, const std::vector<T> &v) {
+  return h.push(v.data(), v.size() * sizeof(T));
+}
+
+template <class F>
+size_t slots_of(HostTable &h, const std::vector<chq_mesh *> &jobs, F grid, long &total) {
+  std::vector<BatchSlot> v(jobs.size());
+  long off = 0;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const Launch3 L = grid(jobs[j]);
+    v[j] = BatchSlot{off, (int)L.grid.x, (int)L.grid.y, (int)L.grid.z, 0};
+    off += (long)L.grid.x * L.grid.y * L.grid.z;
+  }
+  total = off;
+  return push_vec(h, v);
+}
+
+Launch3 linear(long threads, int per) { return {dim3((unsigned)((threads + per - 1) / per), 1, 1), dim3(per)}; }
+
+template <class P>
+int batch_build(chq_batch *B) {
+  HostTable h;
+  const std::vector<chq_mesh *> &J = B->jobs;
+  const int n = (int)J.size();
+  size_t o_flux_s, o_corner_s, o_update_s, o_flag_s, o_repair_s, o_limit_s, o_bc_s[3], o_c2p_s;
+  o_flux_s = slots_of(h, J, [](chq_mesh *m) {
+    const FluxArgs<P> a = flux_args<P>(m, 0, 7u);
+    return linear((a.nwarp[0] + a.nwarp[1] + a.nwarp[2]) * 32, 128);
+  }, B->k_flux.nblocks);
+  o_corner_s = slots_of(h, J, [](chq_mesh *m) { return corner_grid(m); }, B->k_corner.nblocks);
+  o_update_s = slots_of(h, J, [](chq_mesh *m) { return update_grid(m); }, B->k_update.nblocks);
+  o_flag_s = slots_of(h, J, [](chq_mesh *m) { return flag_grid(m); }, B->k_flag.nblocks);
+  o_repair_s = slots_of(h, J, [](chq_mesh *m) {
+    long tot = 0;
+    repair_args<P>(m, 0, 7u, nullptr, nullptr, tot);
+    return linear(tot, 256);
+  }, B->k_repair.nblocks);
+  o_limit_s = slots_of(h, J, [](chq_mesh *m) {
+    long tot = 0;
+    limit_args<P>(m, 7u, 0.0, nullptr, nullptr, nullptr, tot);
+    return linear(tot, 256);
+  }, B->k_limit.nblocks);
+  for (int d = 0; d < 3; ++d)
+    o_bc_s[d] = slots_of(h, J, [d](chq_mesh *m) { return linear(bc_threads(m, d), 256); }, B->k_bc[d].nblocks);
+  o_c2p_s = slots_of(h, J, [](chq_mesh *m) { return c2p_grid(m); }, B->k_c2p.nblocks);
+
+  std::vector<EmfArgs<P>> corner(n), corner_need(n);
+  std::vector<StepCtl *> ctls(n);
+  for (int j = 0; j < n; ++j) {
+    chq_mesh *m = J[j];
+    corner[j] = corner_args<P>(m, &m->ctl->done, nullptr);
+    corner_need[j] = corner_args<P>(m, &m->ctl->done, &m->ctl->nbad);
+    ctls[j] = m->ctl;
+  }
+  const size_t o_corner = push_vec(h, corner), o_corner_need = push_vec(h, corner_need), o_ctls = push_vec(h, ctls);
+  size_t o_flux[4], o_update[4], o_update_need[4], o_flag[4], o_repair[4], o_limit[4], o_bc[4][3], o_c2p[4];
+  for (int st = 1; st <= B->nstage; ++st) {
+    double g0, g1, beta;
+    int cur, out;
+    stage_table(B->nstage, st, g0, g1, beta, cur, out);
+    const bool last = (st == B->nstage);
+    std::vector<FluxArgs<P>> fa(n);
+    std::vector<UpdateArgs<P>> ua(n), uan(n);
+    std::vector<FlagArgs> fl(n);
+    std::vector<RepairArgs<P>> ra(n);
+    std::vector<LimitArgs<P>> la(n);
+    std::vector<BcArgs> bc[3] = {std::vector<BcArgs>(n), std::vector<BcArgs>(n), std::vector<BcArgs>(n)};
+    std::vector<C2pArgs<P>> ca(n);
+    for (int j = 0; j < n; ++j) {
+      chq_mesh *m = J[j];
+      StepCtl *c = m->ctl;
+      fa[j] = flux_args<P>(m, cur, 7u);
+      fa[j].skip = &c->done;
+      ua[j] = update_args<P>(m, out, g0, g1, 0.0, &c->beta_dt[st - 1], &c->done, nullptr);
+      uan[j] = update_args<P>(m, out, g0, g1, 0.0, &c->beta_dt[st - 1], &c->done, &c->nbad);
+      fl[j] = flag_args(m, out, &c->nbad, &c->done);
+      long tot = 0;
+      ra[j] = repair_args<P>(m, cur, 7u, &c->done, &c->nbad, tot);
+      la[j] = limit_args<P>(m, 7u, 0.0, &c->beta_dt[st - 1], &c->limiter_count, &c->done, tot);
+      for (int d = 0; d < 3; ++d) bc[d][j] = bc_args(m, out, &c->done, d);
+      ca[j] = c2p_args<P>(m, out, last ? 1 : 0, &c->mdt_bits, c, &c->done);
+    }
+    o_flux[st - 1] = push_vec(h, fa);
+    o_update[st - 1] = push_vec(h, ua);
+    o_update_need[st - 1] = push_vec(h, uan);
+    o_flag[st - 1] = push_vec(h, fl);
+    o_repair[st - 1] = push_vec(h, ra);
+    o_limit[st - 1] = push_vec(h, la);
+    for (int d = 0; d < 3; ++d) o_bc[st - 1][d] = push_vec(h, bc[d]);
+    o_c2p[st - 1] = push_vec(h, ca);
+  }
+  const size_t o_status = h.push(std::vector<double>(3 * n + 1).data(), (3 * n + 1) * sizeof(double));
+  cudaError_t e = cudaMalloc(&B->dev, h.b.size());
+  if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("batch tables: ") + cudaGetErrorString(e));
+  e = cudaMemcpy(B->dev, h.b.data(), h.b.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "batch tables upload");
+  char *d = B->dev;
+  B->k_flux.slots = (BatchSlot *)(d + o_flux_s);
+  B->k_corner.slots = (BatchSlot *)(d + o_corner_s);
+  B->k_update.slots = (BatchSlot *)(d + o_update_s);
+  B->k_flag.slots = (BatchSlot *)(d + o_flag_s);
+  B->k_repair.slots = (BatchSlot *)(d + o_repair_s);
+  B->k_limit.slots = (BatchSlot *)(d + o_limit_s);
+  for (int q = 0; q < 3; ++q) B->k_bc[q].slots = (BatchSlot *)(d + o_bc_s[q]);
+  B->k_c2p.slots = (BatchSlot *)(d + o_c2p_s);
+  B->a_corner = d + o_corner;
+  B->a_corner_need = d + o_corner_need;
+  B->ctls = (StepCtl **)(d + o_ctls);
+  B->status = (double *)(d + o_status);
+  for (int st = 0; st < B->nstage; ++st) {
+    B->a_flux[st] = d + o_flux[st];
+    B->a_update[st] = d + o_update[st];
+    B->a_update_need[st] = d + o_update_need[st];
+    B->a_flag[st] = d + o_flag[st];
+    B->a_repair[st] = d + o_repair[st];
+    B->a_limit[st] = d + o_limit[st];
+    for (int q = 0; q < 3; ++q) B->a_bc[st][q] = d + o_bc[st][q];
+    B->a_c2p[st] = d + o_c2p[st];
+  }
+  return CHQ_OK;
+}
+
+template <class P>
+cudaError_t batch_flux(const chq_batch *B, const FluxArgs<P> *args, cudaStream_t s) {
+  const int n = (int)B->jobs.size();
+  const unsigned nb = (unsigned)B->k_flux.nblocks;
+  switch (B->recon) {
+    case R_DC: return launch_flux_batched<P, R_DC>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
+    case R_PLM: return launch_flux_batched<P, R_PLM>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
+    case R_PPM: return launch_flux_batched<P, R_PPM>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
+    case R_PPMX: return launch_flux_batched<P, R_PPMX>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
+    case R_WENOZ: return launch_flux_batched<P, R_WENOZ>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// one cycle of every member: the launch sequence of chq_cycles, batched
+template <class P>
+int batch_cycle(chq_batch *B, cudaStream_t s) {
+  const int n = (int)B->jobs.size();
+  const dim3 b2(32, 8);
+  long long &L = B->nlaunch;
+  ctl_begin_batched<<<(n + 127) / 128, 128, 0, s>>>(B->ctls, n);
+  ++L;
+  for (int st = 0; st < B->nstage; ++st) {
+    CHQ_CUDA(batch_flux<P>(B, (const FluxArgs<P> *)B->a_flux[st], s));
+    ++L;
+    if (B->limiter && B->k_limit.nblocks) {
+      limit_batched<P><<<(unsigned)B->k_limit.nblocks, 256, 0, s>>>((const LimitArgs<P> *)B->a_limit[st], B->k_limit.slots, n);
+      ++L;
+    }
+    corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner, B->k_corner.slots, n);
+    update_batched<P><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)B->a_update[st], B->k_update.slots, n);
+    L += 2;
+    if (B->fofc) {
+      fofc_flag_batched<<<(unsigned)B->k_flag.nblocks, b2, 0, s>>>((const FlagArgs *)B->a_flag[st], B->k_flag.slots, n);
+      fofc_repair_batched<P><<<(unsigned)B->k_repair.nblocks, 256, 0, s>>>((const RepairArgs<P> *)B->a_repair[st], B->k_repair.slots, n);
+      corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner_need, B->k_corner.slots, n);
+      update_batched<P><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)B->a_update_need[st], B->k_update.slots, n);
+      L += 4;
+    }
+    bc_batched<0><<<(unsigned)B->k_bc[0].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc[st][0], B->k_bc[0].slots, n);
+    ++L;
+    if (B->k_bc[1].nblocks) {
+      bc_batched<1><<<(unsigned)B->k_bc[1].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc[st][1], B->k_bc[1].slots, n);
+      ++L;
+    }
+    if (B->k_bc[2].nblocks) {
+      bc_batched<2><<<(unsigned)B->k_bc[2].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc[st][2], B->k_bc[2].slots, n);
+      ++L;
+    }
+    c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p[st], B->k_c2p.slots, n);
+    ++L;
+  }
+  ctl_end_batched<<<(n + 127) / 128, 128, 0, s>>>(B->ctls, n);
+  ++L;
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+void batch_free(chq_batch *B) {
+  if (B->stream) cudaStreamSynchronize(B->stream);
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  if (B->dev) cudaFree(B->dev);
+  if (B->stream) cudaStreamDestroy(B->stream);
+  B->exec = nullptr;
+  B->graph = nullptr;
+  B->dev = nullptr;
+  B->stream = nullptr;
 }
 
 }  // namespace
@@ -1001,6 +1339,111 @@ int chq_event_elapsed(chq_mesh *m, int a, int b, float *ms) {
   CHQ_CUDA(cudaEventElapsedTime(ms, m->slots[a], m->slots[b]));
   return CHQ_OK;
 }
+
+int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
+  if (!meshes || n < 1 || !out) return fail(CHQ_ERR_ARG, "bad argument");
+  *out = nullptr;
+  const chq_mesh *a = meshes[0];
+  for (int j = 0; j < n; ++j) {
+    const chq_mesh *m = meshes[j];
+    if (!m) return fail(CHQ_ERR_ARG, "null mesh in batch");
+    if (m->mixed != a->mixed || m->cfg.recon != a->cfg.recon || m->cfg.rsolver != a->cfg.rsolver ||
+        m->cfg.characteristic != a->cfg.characteristic || m->nstage != a->nstage || m->cfg.fofc != a->cfg.fofc ||
+        m->cfg.flux_limiter != a->cfg.flux_limiter)
+      return fail(CHQ_ERR_ARG, "batch members must share precision, reconstruction, Riemann solver, "
+                               "characteristic flag, integrator, FOFC and limiter switches");
+    for (int q = 0; q < j; ++q)
+      if (meshes[q] == m) return fail(CHQ_ERR_ARG, "a mesh appears twice in the batch");
+  }
+  chq_batch *B = new chq_batch;
+  B->jobs.assign(meshes, meshes + n);
+  B->mixed = a->mixed;
+  B->recon = a->cfg.recon;
+  B->rsolver = a->cfg.rsolver;
+  B->charac = a->cfg.characteristic;
+  B->nstage = a->nstage;
+  B->fofc = a->cfg.fofc;
+  B->limiter = a->cfg.flux_limiter;
+  int rc = B->mixed ? batch_build<float>(B) : batch_build<double>(B);
+  if (rc == CHQ_OK) {
+    cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = cuda_fail(e, "batch stream");
+  }
+  if (rc != CHQ_OK) {
+    batch_free(B);
+    delete B;
+    return rc;
+  }
+  *out = B;
+  return CHQ_OK;
+}
+
+int chq_batch_destroy(chq_batch *B) {
+  if (!B) return CHQ_OK;
+  batch_free(B);
+  delete B;
+  return CHQ_OK;
+}
+
+int chq_batch_set_graph(chq_batch *B, int enable) {
+  if (!B) return fail(CHQ_ERR_ARG, "null batch");
+  B->use_graph = (enable != 0);
+  return CHQ_OK;
+}
+
+int chq_batch_cycles(chq_batch *B, int n, void *stream) {
+  if (!B || n < 0) return fail(CHQ_ERR_ARG, "bad argument");
+  // members' own streams may still hold work (uploads, prime): order after them
+  for (chq_mesh *m : B->jobs) CHQ_CUDA(cudaStreamSynchronize(m->stream));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : B->stream;
+  if (!B->use_graph) {
+    for (int c = 0; c < n; ++c) {
+      const int rc = B->mixed ? batch_cycle<float>(B, s) : batch_cycle<double>(B, s);
+      if (rc) return rc;
+    }
+    return CHQ_OK;
+  }
+  if (!B->exec) {
+    // capture one cycle on the batch's own stream and keep the executable graph
+    const long long l0 = B->nlaunch;
+    CHQ_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = B->mixed ? batch_cycle<float>(B, B->stream) : batch_cycle<double>(B, B->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CHQ_CUDA(e);
+    B->graph = g;
+    CHQ_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+    B->per_cycle = B->nlaunch - l0;   // kernels in one cycle; the capture itself ran nothing
+    B->nlaunch = l0;
+  }
+  for (int c = 0; c < n; ++c) CHQ_CUDA(cudaGraphLaunch(B->exec, s));
+  B->nlaunch += B->per_cycle * n;
+  return CHQ_OK;
+}
+
+int chq_batch_status(chq_batch *B, double *t, int *cycle, int *done) {
+  if (!B) return fail(CHQ_ERR_ARG, "null batch");
+  const int n = (int)B->jobs.size();
+  batch_status_kernel<<<(n + 127) / 128, 128, 0, B->stream>>>(B->ctls, n, B->status);
+  CHQ_CUDA(cudaGetLastError());
+  std::vector<double> h(3 * n);
+  CHQ_CUDA(cudaMemcpyAsync(h.data(), B->status, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
+  CHQ_CUDA(cudaStreamSynchronize(B->stream));
+  for (int j = 0; j < n; ++j) {
+    if (t) t[j] = h[3 * j];
+    if (cycle) cycle[j] = (int)h[3 * j + 1];
+    if (done) done[j] = (int)h[3 * j + 2];
+  }
+  return CHQ_OK;
+}
+
+long long chq_batch_kernel_launches(const chq_batch *B) { return B ? B->nlaunch : 0; }
+
+void *chq_batch_stream(chq_batch *B) { return B ? (void *)B->stream : nullptr; }
 
 long long chq_kernel_launches(const chq_mesh *m) { return m ? m->nlaunch : 0; }
 

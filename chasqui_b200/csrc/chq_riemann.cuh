@@ -44,6 +44,26 @@ template <class T> CHQ_HD void phys_flux(const MState<T> &s, T bn, T gm1, T &e, 
   f[FBZ] = s.bz * s.u - bn * s.w;
 }
 
+// total energy and total pressure alone (the scalars phys_flux computes first)
+template <class T> CHQ_HD void energy_ptot(const MState<T> &s, T bn, T gm1, T &e, T &pt) {
+  const T vsq = s.u * s.u + s.v * s.v + s.w * s.w;
+  const T bsq = bn * bn + s.by * s.by + s.bz * s.bz;
+  e = s.p / gm1 + T(0.5) * (s.d * vsq + bsq);
+  pt = s.p + T(0.5) * bsq;
+}
+
+// the flux vector of phys_flux from already computed e and pt
+template <class T> CHQ_HD void flux_from(const MState<T> &s, T bn, T e, T pt, T f[NFLX]) {
+  const T vdotb = s.u * bn + s.v * s.by + s.w * s.bz;
+  f[FD] = s.d * s.u;
+  f[FMU] = s.d * s.u * s.u + pt - bn * bn;
+  f[FMV] = s.d * s.u * s.v - bn * s.by;
+  f[FMW] = s.d * s.u * s.w - bn * s.bz;
+  f[FEN] = (e + pt) * s.u - bn * vdotb;
+  f[FBY] = s.by * s.u - bn * s.v;
+  f[FBZ] = s.bz * s.u - bn * s.w;
+}
+
 // modified fast speed with the sound speed replaced by |v| (src/riemann.hpp:44-51)
 template <class T> CHQ_HD T flow_speed_u(const MState<T> &s, T bn) {
   const T vsq = s.u * s.u + s.v * s.v + s.w * s.w;
@@ -55,22 +75,24 @@ template <class T> CHQ_HD T flow_speed_u(const MState<T> &s, T bn) {
 }
 
 template <class T> CHQ_HD void hlle(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T f[NFLX]) {
-  T fl[NFLX], fr[NFLX], el, er, ptl, ptr;
-  phys_flux(L, bn, gm1, el, ptl, fl);
-  phys_flux(R, bn, gm1, er, ptr, fr);
+  // speeds first; the flux vectors are built only for the region that is selected
   const T cl = fast_speed(L, bn, gamma), cr = fast_speed(R, bn, gamma);
   const T sl = fmin_(L.u - cl, R.u - cr);
   const T sr = fmax_(L.u + cl, R.u + cr);
+  T el, er, ptl, ptr;
+  energy_ptot(L, bn, gm1, el, ptl);
   if (sl >= T(0)) {
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = fl[n];
+    flux_from(L, bn, el, ptl, f);
     return;
   }
+  energy_ptot(R, bn, gm1, er, ptr);
   if (sr <= T(0)) {
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = fr[n];
+    flux_from(R, bn, er, ptr, f);
     return;
   }
+  T fl[NFLX], fr[NFLX];
+  flux_from(L, bn, el, ptl, fl);
+  flux_from(R, bn, er, ptr, fr);
   const T ul[NFLX] = {L.d, L.d * L.u, L.d * L.v, L.d * L.w, el, L.by, L.bz};
   const T ur[NFLX] = {R.d, R.d * R.u, R.d * R.v, R.d * R.w, er, R.by, R.bz};
   const T inv = T(1) / (sr - sl);
@@ -91,8 +113,8 @@ CHQ_HD void star_flux(T d, T sm, T v, T w, T e, T by, T bz, T bn, T pts, T f[NFL
   f[FBZ] = bz * sm - bn * w;
 }
 
-// One side's single-star transverse velocity and field (MK05 eqs. 43-47); `lr` marks the
-// side only for readability, both calls run the identical expression sequence.
+// One side's single-star transverse velocity and field (MK05 eqs. 43-47); the left and
+// right calls run the identical expression sequence.
 template <class T>
 CHQ_HD void star_side(const MState<T> &S, T slm, T sms, T sm, T bn, T bnsq, T &vs, T &ws, T &bys, T &bzs) {
   const T den = (S.d * slm) * sms - bnsq;
@@ -112,11 +134,44 @@ CHQ_HD void star_side(const MState<T> &S, T slm, T sms, T sm, T bn, T bnsq, T &v
   }
 }
 
+// single-star flux of one side: F + S (U* - U) (HLLD) or the star state's own flux (LHLLD)
+template <bool LHLLD, class T>
+CHQ_HD void side_star_flux(const MState<T> &S, T bn, T e, T pt, T s, T ds, T sm, T vs, T ws, T bys, T bzs, T es,
+                           T pts, T f[NFLX]) {
+  if constexpr (LHLLD) {
+    star_flux(ds, sm, vs, ws, es, bys, bzs, bn, pts, f);
+  } else {
+    T fs[NFLX];
+    flux_from(S, bn, e, pt, fs);
+    const T us[NFLX] = {ds, ds * sm, ds * vs, ds * ws, es, bys, bzs};
+    const T u[NFLX] = {S.d, S.d * S.u, S.d * S.v, S.d * S.w, e, S.by, S.bz};
+#pragma unroll
+    for (int n = 0; n < NFLX; ++n) f[n] = fs[n] + s * (us[n] - u[n]);
+  }
+}
+
+// double-star flux of one side: F* + S* (U** - U*) (HLLD) or the ** state's own flux (LHLLD)
+template <bool LHLLD, class T>
+CHQ_HD void side_dstar_flux(const MState<T> &S, T bn, T e, T pt, T s, T ds, T sm, T vs, T ws, T bys, T bzs, T es,
+                            T pts, T ss, T vss, T wss, T byss, T bzss, T ess, T f[NFLX]) {
+  if constexpr (LHLLD) {
+    star_flux(ds, sm, vss, wss, ess, byss, bzss, bn, pts, f);
+  } else {
+    T fs[NFLX];
+    side_star_flux<false>(S, bn, e, pt, s, ds, sm, vs, ws, bys, bzs, es, pts, fs);
+    const T us[NFLX] = {ds, ds * sm, ds * vs, ds * ws, es, bys, bzs};
+    const T uss[NFLX] = {ds, ds * sm, ds * vss, ds * wss, ess, byss, bzss};
+#pragma unroll
+    for (int n = 0; n < NFLX; ++n) f[n] = fs[n] + ss * (uss[n] - us[n]);
+  }
+}
+
 template <bool LHLLD, class T>
 CHQ_HD void hlld(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T f[NFLX], T theta, T phi) {
-  T fl[NFLX], fr[NFLX], el, er, ptl, ptr;
-  phys_flux(L, bn, gm1, el, ptl, fl);
-  phys_flux(R, bn, gm1, er, ptr, fr);
+  // speeds and the scalars of both sides first; flux vectors only for the selected region
+  T el, er, ptl, ptr;
+  energy_ptot(L, bn, gm1, el, ptl);
+  energy_ptot(R, bn, gm1, er, ptr);
   const T cl = fast_speed(L, bn, gamma), cr = fast_speed(R, bn, gamma);
   T sl, sr;
   if constexpr (LHLLD) {
@@ -128,13 +183,11 @@ CHQ_HD void hlld(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T
     sr = fmax_(L.u + cl, R.u + cr);
   }
   if (sl >= T(0)) {
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = fl[n];
+    flux_from(L, bn, el, ptl, f);
     return;
   }
   if (sr <= T(0)) {
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = fr[n];
+    flux_from(R, bn, er, ptr, f);
     return;
   }
   const T bnsq = bn * bn;
@@ -169,44 +222,28 @@ CHQ_HD void hlld(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T
   const T sls = sm - abn / sqdl;
   const T srs = sm + abn / sqdr;
 
-  T fls[NFLX], frs[NFLX];
-  if constexpr (LHLLD) {
-    star_flux(dls, sm, vls, wls, els, byls, bzls, bn, pts, fls);
-    star_flux(drs, sm, vrs, wrs, ers, byrs, bzrs, bn, pts, frs);
-  } else {
-    const T uls[NFLX] = {dls, dls * sm, dls * vls, dls * wls, els, byls, bzls};
-    const T urs[NFLX] = {drs, drs * sm, drs * vrs, drs * wrs, ers, byrs, bzrs};
-    const T ul[NFLX] = {L.d, L.d * L.u, L.d * L.v, L.d * L.w, el, L.by, L.bz};
-    const T ur[NFLX] = {R.d, R.d * R.u, R.d * R.v, R.d * R.w, er, R.by, R.bz};
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) {
-      fls[n] = fl[n] + sl * (uls[n] - ul[n]);
-      frs[n] = fr[n] + sr * (urs[n] - ur[n]);
-    }
-  }
   // strict inequalities: with S*_L = S*_R = 0 both sides are averaged below
   if (sls > T(0)) {
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = fls[n];
+    side_star_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, f);
     return;
   }
   if (srs < T(0)) {
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = frs[n];
+    side_star_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, f);
     return;
   }
   // bn ~ 0: the double-star region collapses onto the contact
   const T bnsmall = T(1e-12) * (ptl + ptr);
   if (bnsq <= bnsmall) {
     if (sm > T(0)) {
-#pragma unroll
-      for (int n = 0; n < NFLX; ++n) f[n] = fls[n];
+      side_star_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, f);
     } else if (sm < T(0)) {
-#pragma unroll
-      for (int n = 0; n < NFLX; ++n) f[n] = frs[n];
+      side_star_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, f);
     } else {
+      T fa[NFLX], fb[NFLX];
+      side_star_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, fa);
+      side_star_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, fb);
 #pragma unroll
-      for (int n = 0; n < NFLX; ++n) f[n] = T(0.5) * (fls[n] + frs[n]);
+      for (int n = 0; n < NFLX; ++n) f[n] = T(0.5) * (fa[n] + fb[n]);
     }
     return;
   }
@@ -218,45 +255,20 @@ CHQ_HD void hlld(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T
   const T byss = ((sqdl * byrs + sqdr * byls) + (sqdl * sqdr) * ((vrs - vls) * sg)) * inv;
   const T bzss = ((sqdl * bzrs + sqdr * bzls) + (sqdl * sqdr) * ((wrs - wls) * sg)) * inv;
   const T vdotb_ss = (sm * bn + vss * byss) + wss * bzss;
-  const T elss = els - sqdl * ((vdotb_ls - vdotb_ss) * sg);
-  const T erss = ers + sqdr * ((vdotb_rs - vdotb_ss) * sg);
-
   if (sm > T(0)) {
-    if constexpr (LHLLD) {
-      star_flux(dls, sm, vss, wss, elss, byss, bzss, bn, pts, f);
-    } else {
-      const T uls[NFLX] = {dls, dls * sm, dls * vls, dls * wls, els, byls, bzls};
-      const T ulss[NFLX] = {dls, dls * sm, dls * vss, dls * wss, elss, byss, bzss};
-#pragma unroll
-      for (int n = 0; n < NFLX; ++n) f[n] = fls[n] + sls * (ulss[n] - uls[n]);
-    }
+    const T elss = els - sqdl * ((vdotb_ls - vdotb_ss) * sg);
+    side_dstar_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, sls, vss, wss, byss, bzss, elss, f);
   } else if (sm < T(0)) {
-    if constexpr (LHLLD) {
-      star_flux(drs, sm, vss, wss, erss, byss, bzss, bn, pts, f);
-    } else {
-      const T urs[NFLX] = {drs, drs * sm, drs * vrs, drs * wrs, ers, byrs, bzrs};
-      const T urss[NFLX] = {drs, drs * sm, drs * vss, drs * wss, erss, byss, bzss};
-#pragma unroll
-      for (int n = 0; n < NFLX; ++n) f[n] = frs[n] + srs * (urss[n] - urs[n]);
-    }
+    const T erss = ers + sqdr * ((vdotb_rs - vdotb_ss) * sg);
+    side_dstar_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, srs, vss, wss, byss, bzss, erss, f);
   } else {
-    T flss[NFLX], frss[NFLX];
-    if constexpr (LHLLD) {
-      star_flux(dls, sm, vss, wss, elss, byss, bzss, bn, pts, flss);
-      star_flux(drs, sm, vss, wss, erss, byss, bzss, bn, pts, frss);
-    } else {
-      const T uls[NFLX] = {dls, dls * sm, dls * vls, dls * wls, els, byls, bzls};
-      const T urs[NFLX] = {drs, drs * sm, drs * vrs, drs * wrs, ers, byrs, bzrs};
-      const T ulss[NFLX] = {dls, dls * sm, dls * vss, dls * wss, elss, byss, bzss};
-      const T urss[NFLX] = {drs, drs * sm, drs * vss, drs * wss, erss, byss, bzss};
+    const T elss = els - sqdl * ((vdotb_ls - vdotb_ss) * sg);
+    const T erss = ers + sqdr * ((vdotb_rs - vdotb_ss) * sg);
+    T fa[NFLX], fb[NFLX];
+    side_dstar_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, sls, vss, wss, byss, bzss, elss, fa);
+    side_dstar_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, srs, vss, wss, byss, bzss, erss, fb);
 #pragma unroll
-      for (int n = 0; n < NFLX; ++n) {
-        flss[n] = fls[n] + sls * (ulss[n] - uls[n]);
-        frss[n] = frs[n] + srs * (urss[n] - urs[n]);
-      }
-    }
-#pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = T(0.5) * (flss[n] + frss[n]);
+    for (int n = 0; n < NFLX; ++n) f[n] = T(0.5) * (fa[n] + fb[n]);
   }
 }
 

@@ -147,6 +147,27 @@ CHQ_API int chq_profile(chq_mesh *m, int enable);
 /* Synchronises; totals in ms and launch counts per kind since the last reset. */
 CHQ_API int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launches[CHQ_NPROF], int reset);
 
+/* ---- batched stepping of many meshes (no reference counterpart: the reference steps one
+ * mesh at a time) ---------------------------------------------------------------------------
+ * A batch groups primed meshes of one class (same precision, reconstruction, Riemann solver,
+ * characteristic flag, integrator, FOFC and limiter switches) of any sizes and dimensions
+ * and advances all of them with one launch per kernel kind per stage, the blocks of every
+ * member in the same grid. Each member keeps its own dt, clock, boundaries and FOFC
+ * decisions, and stops at its own tlim, so its results are identical to stepping it alone.
+ * Membership is fixed at creation; meshes must outlive the batch. */
+typedef struct chq_batch chq_batch;
+CHQ_API int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out);
+CHQ_API int chq_batch_destroy(chq_batch *b);
+/* n cycles of every member (asynchronous on `stream`, NULL = the batch's stream). */
+CHQ_API int chq_batch_cycles(chq_batch *b, int n, void *stream);
+/* enable: capture one whole cycle as a CUDA graph on first use and replay it. */
+CHQ_API int chq_batch_set_graph(chq_batch *b, int enable);
+/* Synchronises; per member time, cycle count and done flag (arrays of length n, any NULL). */
+CHQ_API int chq_batch_status(chq_batch *b, double *t, int *cycle, int *done);
+CHQ_API long long chq_batch_kernel_launches(const chq_batch *b);
+/* the batch's own stream (cudaStream_t) */
+CHQ_API void *chq_batch_stream(chq_batch *b);
+
 #ifdef __cplusplus
 }
 #endif
