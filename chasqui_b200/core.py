@@ -87,6 +87,8 @@ SIGNATURES = [
     ("chq_batch_status", C.c_int, [_P, _D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("chq_batch_kernel_launches", C.c_longlong, [_P]),
     ("chq_batch_stream", _P, [_P]),
+    ("chq_history_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                      _P, _P, _P, _P, _D, _P]),
 ]
 
 PROFILE_KINDS = ("fluxes", "corner_emf", "update", "fofc_flag", "fofc_repair", "boundaries", "c2p_dt", "limiter",

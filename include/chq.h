@@ -168,6 +168,27 @@ CHQ_API long long chq_batch_kernel_launches(const chq_batch *b);
 /* the batch's own stream (cudaStream_t) */
 CHQ_API void *chq_batch_stream(chq_batch *b);
 
+/* ---- history sums without any device allocation --------------------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device memory: an
+ * application whose memory belongs to its own pool or framework allocator (for example a
+ * Kokkos code that keeps its fields in its own Views), code that must not trigger the
+ * implicit device synchronisation of cudaMalloc/cudaFree inside a latency-critical loop,
+ * or a monitoring hook that only holds pointers to someone else's state. Same ten values as
+ * chq_history() (mass mom1 mom2 mom3 etot ekin emag eint divB_max divB_L1), computed from
+ * caller-owned DEVICE arrays in the reference layout: u (6, nk, nj, ni) conserved state and
+ * b1/b2/b3 (nk+1, nj+1, ni+1) face fields; the ten results are written to the HOST array
+ * `out` and the call synchronises `stream`. Velocities come from u as m / rho, so rho must
+ * be positive. Nothing is allocated: block partials live in one fixed static device array
+ * of 8192 x 10 doubles (about 640 KiB, held by every device that loads the library until
+ * the process exits), which limits meshes to nx3 * ceil(nx2 / 128) <= 8192 (e.g. 1024^3);
+ * larger ones return CHQ_ERR_ARG. The first call on each device performs a one-time set-up
+ * (it looks up that device address), so make it before any stream capture. All calls share
+ * the array: calls that overlap on the GPU (other streams or threads on the same device)
+ * race and must be serialised by the caller. */
+CHQ_API int chq_history_noalloc(int nx1, int nx2, int nx3, int ng, double dx1, double dx2, double dx3,
+                                const double *u, const double *b1, const double *b2, const double *b3,
+                                double out[10], void *stream);
+
 #ifdef __cplusplus
 }
 #endif
