@@ -142,11 +142,13 @@ def blast_config(n: int, precision: int):
                        recon=2, rsolver=1, integrator=3, cfl=0.3, fofc=1, flatten=1, precision=precision, tlim=0.2)
 
 
-def run_form(n, precision, ics_state, steps, warmup, dist, device, sample_clocks=False, profile_cycles=2):
+BLAST_PARAMS = [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 20261203.0]   # p_in, p_out, r, b0, angle, noise, seed
+
+
+def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, profile_cycles=2):
     from chasqui_b200 import Mesh
-    u, b1, b2, b3 = ics_state
     mesh = Mesh(blast_config(n, precision))
-    mesh.set_state(u, b1, b2, b3)
+    mesh.init_problem("blast", BLAST_PARAMS)
     mesh.prime(0.0)
     mesh.cycles(warmup)
     mesh.clock()
@@ -174,13 +176,15 @@ def run_form(n, precision, ics_state, steps, warmup, dist, device, sample_clocks
                   "clocks": sampler.summary() if sampler else None, "fofc": fofc}
 
 
-def e2e_host(mesh, ics_state, steps, warmup, dist):
+def e2e_host(mesh, steps, warmup, dist):
     """zone-updates/s through the host-buffer C-ABI call: each step uploads the state from
     pinned host memory, primes it, runs one cycle and downloads the new state."""
     from chasqui_b200 import PinnedArray
-    pins = [PinnedArray(a.shape) for a in ics_state]
-    for p, a in zip(pins, ics_state):
-        p.array[...] = a
+    mesh.init_problem("blast", BLAST_PARAMS)
+    names = ("u0", "b1f0", "b2f0", "b3f0")
+    pins = [PinnedArray(mesh.shape(f) if f == "u0" else mesh.shape(f)[1:]) for f in names]
+    for p, f in zip(pins, names):
+        p.array[...] = mesh.get(f)
     arrs = [p.array for p in pins]
     for _ in range(max(1, warmup)):
         mesh.run_host(*arrs, 1)
@@ -247,6 +251,73 @@ name = blast
     return times
 
 
+def ensemble(njobs: int, cycles: int, seed: int, cps: int) -> dict:
+    """njobs seeded jobs (OT 2D 64^2..1024^2, CPAW / blast 3D
+    32^3..192^3, PPM or WENO-Z, mixed precision), `cycles` cycles each: all submitted at
+    once to the batching server vs the same jobs as sequential one-job runs."""
+    from chasqui_b200 import Mesh, Server, workloads
+    jobs = workloads.draw_jobs(njobs, seed=seed, precision=1, nlim=cycles)
+    zu = sum(j["cells"] for j in jobs) * cycles
+    srv = Server(150 << 30, max_active=100000, cycles_per_step=cps)
+    t0 = time.perf_counter()
+    ids = [srv.submit(j["cfg"], j["problem"], j["params"]) for j in jobs]
+    steps = 0
+    while srv.step() > 0:
+        steps += 1
+    t_batched = time.perf_counter() - t0
+    ok = sum(srv.status(i)["state"] == "done" for i in ids)
+    srv.close()
+    t0 = time.perf_counter()
+    for j in jobs:
+        m = Mesh(j["cfg"])
+        m.init_problem(j["problem"], j["params"])
+        m.prime(0.0)
+        m.cycles(cycles)
+        m.clock()
+        m.close()
+    t_seq = time.perf_counter() - t0
+    return {"jobs": njobs, "cycles_each": cycles, "zone_updates": zu, "done": ok,
+            "batched": {"seconds": t_batched, "value": zu / t_batched, "server_steps": steps},
+            "sequential": {"seconds": t_seq, "value": zu / t_seq},
+            "speedup_batched_vs_sequential": t_seq / t_batched,
+            "timing": "host wall clock around submit-to-drain, device synchronised at the end"}
+
+
+def serving(njobs: int, rate: float, precision: int, seed: int, t_end=(0.005, 0.05), nmax2=512, nmax3=96,
+            cps=4) -> dict:
+    """BASELINE config 5, scaled: njobs requests with Poisson arrivals at `rate` jobs/s,
+    kinds and sizes from the ensemble distribution (capped at nmax2^2 / nmax3^3), end time
+    U[t_end]; submitted to the server as they arrive; time-to-solution per job."""
+    from chasqui_b200 import Server, workloads
+    jobs = workloads.draw_jobs(njobs, seed=seed, precision=precision, nmax2=nmax2, nmax3=nmax3, t_end=t_end)
+    rng = np.random.default_rng(seed + 1)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, njobs))
+    srv = Server(150 << 30, max_active=100000, cycles_per_step=cps)
+    ids = []
+    nxt = 0
+    base = srv.stats()["clock"]
+    while True:
+        now = srv.stats()["clock"] - base
+        while nxt < njobs and arrivals[nxt] <= now:
+            j = jobs[nxt]
+            ids.append(srv.submit(j["cfg"], j["problem"], j["params"]))
+            nxt += 1
+        busy = srv.step()
+        if busy == 0:
+            if nxt >= njobs:
+                break
+            time.sleep(max(0.0, min(0.01, arrivals[nxt] - (srv.stats()["clock"] - base))))
+    st = [srv.status(i) for i in ids]
+    lat = np.array([s["t_done"] - s["t_submit"] for s in st])
+    zu = sum(s["zone_updates"] for s in st)
+    wall = max(s["t_done"] for s in st) - base
+    srv.close()
+    return {"requests": njobs, "rate_jobs_per_s": rate, "precision": "mixed" if precision else "fp64",
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "zone_updates_per_s": zu / wall, "done": sum(s["state"] == "done" for s in st),
+            "t_end": list(t_end), "max_n2d": nmax2, "max_n3d": nmax3}
+
+
 def host_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -291,22 +362,26 @@ def main(argv=None):
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ens-jobs", type=int, default=256)
+    ap.add_argument("--ens-cycles", type=int, default=50)
+    ap.add_argument("--srv-jobs", type=int, default=120)
+    ap.add_argument("--srv-rates", default="10,40")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     rank, local = env_int("RANK", 0), env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return main_reference(args, rank)
 
-    from chasqui_b200 import ics, set_device
+    from chasqui_b200 import set_device
     dist = dist_init()
     world = env_int("WORLD_SIZE", 1)
     set_device(local)
     n = args.n
-    g, u, b1, b2, b3 = ics.blast_noise(n)
-    state = (u, b1, b2, b3)
     hbm, peak_kind = peaks()
 
-    mesh, r64 = run_form(n, 0, state, args.steps, args.warmup, dist, local, sample_clocks=True)
+    mesh, r64 = run_form(n, 0, args.steps, args.warmup, dist, local, sample_clocks=True)
     zones = float(n) ** 3
     value = world * zones * args.steps / (r64["ms_max"] / 1e3)
     ms_step = r64["ms_max"] / args.steps
@@ -319,10 +394,12 @@ def main(argv=None):
     tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get("fluxes_fp64_per_launch_bytes")
+            bpc = json.load(f).get("fluxes_fp64_bytes_per_cell")
+        if bpc:
+            traffic = bpc * zones   # ncu DRAM bytes of one K1 launch at 128^3, scaled by cells
     e2e = None
     if not args.no_e2e:
-        times, nbytes, job_ms = e2e_host(mesh, state, args.steps, args.warmup, dist)
+        times, nbytes, job_ms = e2e_host(mesh, args.steps, args.warmup, dist)
         per = dist_max(dist, statistics.mean(times))
         job = dist_max(dist, job_ms)
         e2e = {"value": world * zones / (per / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
@@ -335,7 +412,7 @@ def main(argv=None):
 
     mixed = None
     if not args.no_mixed:
-        meshm, rm = run_form(n, 1, state, args.steps, args.warmup, dist, local)
+        meshm, rm = run_form(n, 1, args.steps, args.warmup, dist, local)
         vm = world * zones * args.steps / (rm["ms_max"] / 1e3)
         pm = rm["prof"]
         km, kn = pm["fluxes"]
@@ -346,6 +423,14 @@ def main(argv=None):
                  "kernel_ms_per_step": {k: v[0] / 2 for k, v in pm.items()}}
         meshm.close()
         del meshm
+
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 4)
+    srv = None
+    if not args.no_serving:
+        srv = [serving(args.srv_jobs, float(r), prec, 77 + rank)
+               for r in args.srv_rates.split(",") for prec in (1, 0)]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -374,6 +459,8 @@ def main(argv=None):
             "fofc_corrections": r64["fofc"],
             "e2e": e2e,
             "mixed": mixed,
+            "ensemble": ens,
+            "serving": srv,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

@@ -6,8 +6,8 @@ is its host-side mirror: the reference's parameter semantics (`params`) and a ct
 """
 from .params import Params, ParamError, config_from_params  # noqa: F401
 from .core import (ChqError, Mesh, chq_config, default_config, make_config, load_library,  # noqa: F401
-                   LIB_PATH, SIGNATURES, FIELDS, PROFILE_KINDS, PinnedArray, set_device, device_count, Batch)
+                   LIB_PATH, SIGNATURES, FIELDS, PROFILE_KINDS, PinnedArray, set_device, device_count, Batch, Server)
 
 __all__ = ["Params", "ParamError", "config_from_params", "ChqError", "Mesh", "chq_config", "default_config",
            "make_config", "load_library", "LIB_PATH", "SIGNATURES", "FIELDS", "PROFILE_KINDS", "PinnedArray",
-           "set_device", "device_count", "Batch"]
+           "set_device", "device_count", "Batch", "Server"]

@@ -38,7 +38,7 @@ class chq_config(C.Structure):
         ("dual_energy", C.c_int), ("low_mach", C.c_int), ("flatten", C.c_int), ("characteristic", C.c_int),
         ("fofc", C.c_int), ("flux_limiter", C.c_int),
         ("nu", C.c_double), ("kappa", C.c_double), ("eta", C.c_double), ("sts", C.c_int),
-        ("precision", C.c_int), ("tlim", C.c_double),
+        ("precision", C.c_int), ("tlim", C.c_double), ("nlim", C.c_int),
     ]
 
 
@@ -51,6 +51,8 @@ SIGNATURES = [
     ("chq_mesh_destroy", C.c_int, [_P]),
     ("chq_mesh_dims", C.c_int, [_P, C.POINTER(C.c_int)]),
     ("chq_mesh_bytes", C.c_longlong, [_P]),
+    ("chq_config_bytes", C.c_longlong, [C.POINTER(chq_config)]),
+    ("chq_init_problem", C.c_int, [_P, C.c_int, _D, C.c_int, _P]),
     ("chq_last_error", C.c_char_p, []),
     ("chq_array_size", C.c_long, [_P, C.c_char_p]),
     ("chq_upload", C.c_int, [_P, C.c_char_p, _D, C.c_long, _P]),
@@ -87,6 +89,14 @@ SIGNATURES = [
     ("chq_batch_status", C.c_int, [_P, _D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("chq_batch_kernel_launches", C.c_longlong, [_P]),
     ("chq_batch_stream", _P, [_P]),
+    ("chq_server_create", C.c_int, [C.c_longlong, C.c_int, C.c_int, C.POINTER(_P)]),
+    ("chq_server_submit", C.c_int, [_P, C.POINTER(chq_config), C.c_int, _D, C.c_int, C.POINTER(C.c_longlong)]),
+    ("chq_server_step", C.c_int, [_P]),
+    ("chq_server_status", C.c_int, [_P, C.c_longlong, C.c_void_p]),
+    ("chq_server_job_mesh", _P, [_P, C.c_longlong]),
+    ("chq_server_stats", C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_longlong), _D]),
+    ("chq_server_destroy", C.c_int, [_P]),
     ("chq_history_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       _P, _P, _P, _P, _D, _P]),
 ]
@@ -204,6 +214,13 @@ class Mesh:
             raise ChqError(f"{name}: expected {n} values, got {a.size}")
         _check(load_library().chq_upload(self._h, name.encode(), _dptr(a), a.size, None))
 
+    def init_problem(self, problem: str, params) -> None:
+        """Device problem generator: 'orszag_tang' {beta}, 'cpaw' {m1,m2,m3,dens,pres,b_par,amp},
+        'blast' {pres_in,pres_out,radius,b0,angle_deg,noise_amp,seed}. Call prime() next."""
+        pid = {"orszag_tang": 0, "cpaw": 1, "blast": 2}[problem]
+        a = np.ascontiguousarray(params, dtype=np.float64)
+        _check(load_library().chq_init_problem(self._h, pid, _dptr(a), a.size, None))
+
     # ---- stage seam ----
     def fluxes(self, dir: int, cur: int = 0):
         _check(load_library().chq_fluxes(self._h, dir, cur, None))
@@ -297,6 +314,64 @@ class Mesh:
         self.set("b1f0", b1)
         self.set("b2f0", b2)
         self.set("b3f0", b3)
+
+
+class chq_job_status(C.Structure):
+    _fields_ = [("state", C.c_int), ("cycle", C.c_int), ("t", C.c_double), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_done", C.c_double), ("zone_updates", C.c_longlong),
+                ("bytes", C.c_longlong), ("history", C.c_double * 10)]
+
+
+JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+PGEN = {"orszag_tang": 0, "cpaw": 1, "blast": 2}
+
+
+class Server:
+    """Continuous-batching simulation server (chq_server_*)."""
+
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 1024, cycles_per_step: int = 4):
+        h = _P()
+        _check(load_library().chq_server_create(int(hbm_budget_bytes), max_active, cycles_per_step, C.byref(h)))
+        self._h = h
+
+    def submit(self, cfg: chq_config, problem: str, params) -> int:
+        a = np.ascontiguousarray(params, dtype=np.float64)
+        jid = C.c_longlong()
+        _check(load_library().chq_server_submit(self._h, C.byref(cfg), PGEN[problem], _dptr(a), a.size, C.byref(jid)))
+        return jid.value
+
+    def step(self) -> int:
+        return _check(load_library().chq_server_step(self._h))
+
+    def status(self, jid: int) -> dict:
+        st = chq_job_status()
+        _check(load_library().chq_server_status(self._h, jid, C.byref(st)))
+        return {"state": JOB_STATES[st.state], "cycle": st.cycle, "t": st.t, "t_submit": st.t_submit,
+                "t_start": st.t_start, "t_done": st.t_done, "zone_updates": st.zone_updates, "bytes": st.bytes,
+                "history": list(st.history)}
+
+    def job_mesh_handle(self, jid: int):
+        return load_library().chq_server_job_mesh(self._h, jid)
+
+    def stats(self) -> dict:
+        used, za = C.c_longlong(), C.c_longlong()
+        act, q = C.c_int(), C.c_int()
+        clk = C.c_double()
+        _check(load_library().chq_server_stats(self._h, C.byref(used), C.byref(act), C.byref(q), C.byref(za),
+                                               C.byref(clk)))
+        return {"used_bytes": used.value, "active": act.value, "queued": q.value, "zone_updates": za.value,
+                "clock": clk.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().chq_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

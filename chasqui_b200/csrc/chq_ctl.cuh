@@ -18,7 +18,7 @@ struct StepCtl {
   unsigned long long mdt_bits;   // running min of the c2p dt reduction (positive doubles order as integers)
   long long fofc_count, limiter_count;
   int nbad;                      // cells flagged by the FOFC test in the current stage
-  int cycle, done, nstage, dt_pending;
+  int cycle, done, nstage, nlim;   // nlim >= 0: stop after that many cycles (time.nlim)
   int err;                       // nonzero: a kernel detected an invalid launch configuration
 };
 

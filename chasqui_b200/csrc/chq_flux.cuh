@@ -314,12 +314,12 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, long wid, P (*park)[128]) {
 
 // Resident 128-thread blocks per SM the flux kernel is compiled for (register cap). The
 // kernel is bound by FP64 / FP32 instruction latency, so more resident warps pay even with
-// some spilling to L1: measured best at 5 (FP64, 96 registers) and 6 (FP32).
+// some spilling to L1: measured best at 5 (FP64, 96 registers) and 8 (FP32, 64 registers).
 #ifndef CHQ_FLUX_MINB_D
 #define CHQ_FLUX_MINB_D 5
 #endif
 #ifndef CHQ_FLUX_MINB_F
-#define CHQ_FLUX_MINB_F 6
+#define CHQ_FLUX_MINB_F 8
 #endif
 template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUX_MINB_D : CHQ_FLUX_MINB_F; };
 

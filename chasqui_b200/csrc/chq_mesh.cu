@@ -11,11 +11,13 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <cmath>
 #include "chq.h"
 #include "chq_common.cuh"
 #include "chq_ctl.cuh"
 #include "chq_kernels.cuh"
 #include "chq_launch.h"
+#include "chq_pgen.cuh"
 
 using namespace chq;
 
@@ -47,7 +49,7 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 namespace chq {
 CHQ_D void ctl_begin(StepCtl *c) {
   if (c->done) return;
-  if (!(c->t < c->tlim)) { c->done = 1; return; }
+  if (!(c->t < c->tlim) || (c->nlim >= 0 && c->cycle >= c->nlim)) { c->done = 1; return; }
   double dt = c->cfl * c->min_dt;
   if (c->t + dt > c->tlim) dt = c->tlim - c->t;
   c->dt = dt;
@@ -191,6 +193,15 @@ struct chq_mesh {
 namespace {
 
 const int kSeglen = 16;
+const int kHstBlocks = 1184;   // 8 blocks per SM on 148 SMs
+
+// bytes of one mesh slab: 18 double fields (u0, u1, 6 face fields), 39 fields of the
+// primitive type, the int flags, the control block and the history scratch
+size_t slab_size(size_t nel, size_t psize) {
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  return nel * sizeof(double) * 18 + nel * psize * 39 + up(nel * sizeof(int)) + up(sizeof(StepCtl)) +
+         up((size_t)(kHstBlocks * 10 + 16) * sizeof(double));
+}
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -945,6 +956,7 @@ void chq_config_defaults(chq_config *c) {
   c->fofc = 1;
   c->precision = CHQ_FP64;
   c->tlim = 1.0;
+  c->nlim = -1;
 }
 
 int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
@@ -1016,10 +1028,9 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   // fluxes 18, face EMFs 6, edge EMFs 3), the int flag array, control block and scratch
   const size_t nel = (size_t)g.vstride;
   const size_t dbytes = nel * sizeof(double), pbytes = nel * m->psize, ibytes = align_up(nel * sizeof(int), 256);
-  m->hst_blocks = 1184;   // 8 blocks per SM on 148 SMs
+  m->hst_blocks = kHstBlocks;
   const size_t ctl_bytes = align_up(sizeof(StepCtl), 256);
-  const size_t hst_bytes = align_up((size_t)(m->hst_blocks * 10 + 16) * sizeof(double), 256);
-  m->slab_bytes = dbytes * 18 + pbytes * 39 + ibytes + ctl_bytes + hst_bytes;
+  m->slab_bytes = slab_size(nel, m->psize);
   cudaError_t e = cudaMalloc(&m->slab, m->slab_bytes);
   if (e != cudaSuccess) {
     delete m;
@@ -1045,6 +1056,7 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   if (e == cudaSuccess) {
     StepCtl h{};
     h.tlim = c.tlim;
+    h.nlim = c.nlim;
     h.cfl = c.cfl;
     h.nstage = m->nstage;
     h.mdt_bits = 0x7ff0000000000000ULL;
@@ -1084,6 +1096,58 @@ int chq_mesh_dims(const chq_mesh *m, int dims[10]) {
 }
 
 long long chq_mesh_bytes(const chq_mesh *m) { return m ? (long long)m->slab_bytes : 0; }
+
+long long chq_config_bytes(const chq_config *c) {
+  if (!c || c->nx1 < 1 || c->nx2 < 1 || c->nx3 < 1) return -1;
+  const bool wide = (c->recon == CHQ_RECON_PPM || c->recon == CHQ_RECON_PPMX || c->recon == CHQ_RECON_WENOZ);
+  const int ng = (c->nghost > 0) ? c->nghost : (wide ? 3 : 2);
+  const long ni = c->nx1 + 2 * ng, nj = (c->nx2 > 1) ? c->nx2 + 2 * ng : 1, nk = (c->nx3 > 1) ? c->nx3 + 2 * ng : 1;
+  const size_t sj = align_up((size_t)ni + 1, 32);
+  const size_t nel = align_up((size_t)(nk + 1) * (nj + 1) * sj, 64);
+  return (long long)slab_size(nel, c->precision == CHQ_MIXED ? sizeof(float) : sizeof(double));
+}
+
+int chq_init_problem(chq_mesh *m, int problem, const double *prm, int nprm, void *stream) {
+  if (!m || (nprm > 0 && !prm) || nprm < 0 || nprm > 12) return fail(CHQ_ERR_ARG, "bad argument");
+  static const int need[3] = {1, 7, 7};
+  if (problem < 0 || problem > 2) return fail(CHQ_ERR_ARG, "unknown problem generator");
+  if (nprm < need[problem]) return fail(CHQ_ERR_ARG, "too few problem parameters");
+  PgenArgs a{};
+  a.g = m->g;
+  a.problem = problem;
+  a.gamma = m->cfg.gamma;
+  for (int q = 0; q < nprm; ++q) a.prm[q] = prm[q];
+  if (problem == PG_CPAW) {
+    const double L[3] = {m->g.x1max - m->g.x1min, m->g.x2max - m->g.x2min, m->g.x3max - m->g.x3min};
+    double kv[3], nrm = 0.0;
+    for (int q = 0; q < 3; ++q) { kv[q] = 2.0 * M_PI * prm[q] / L[q]; nrm += kv[q] * kv[q]; }
+    nrm = std::sqrt(nrm);
+    if (!(nrm > 0.0)) return fail(CHQ_ERR_ARG, "cpaw: zero wavevector");
+    for (int q = 0; q < 3; ++q) a.e1[q] = kv[q] / nrm;
+    // e2 perpendicular to e1 (prefer the x-y plane), e3 = e1 x e2
+    const double t[3] = {std::fabs(a.e1[2]) < 0.9 ? 0.0 : 1.0, 0.0, std::fabs(a.e1[2]) < 0.9 ? 1.0 : 0.0};
+    double e2[3] = {t[1] * a.e1[2] - t[2] * a.e1[1], t[2] * a.e1[0] - t[0] * a.e1[2], t[0] * a.e1[1] - t[1] * a.e1[0]};
+    const double n2 = std::sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    for (int q = 0; q < 3; ++q) a.e2[q] = e2[q] / n2;
+    a.e3[0] = a.e1[1] * a.e2[2] - a.e1[2] * a.e2[1];
+    a.e3[1] = a.e1[2] * a.e2[0] - a.e1[0] * a.e2[2];
+    a.e3[2] = a.e1[0] * a.e2[1] - a.e1[1] * a.e2[0];
+    a.kmag = nrm;
+  }
+  a.u = m->u[0];
+  a.b1 = m->bf[0][0];
+  a.b2 = m->bf[0][1];
+  a.b3 = m->bf[0][2];
+  cudaStream_t s = S(m, stream);
+  const Geom &g = m->g;
+  const long nf = (long)(g.nk + 1) * (g.nj + 1) * (g.ni + 1), nc = (long)g.nk * g.nj * g.ni;
+  pgen_faces_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  pgen_cells_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  m->nlaunch += 2;
+  return CHQ_OK;
+}
 
 long chq_array_size(const chq_mesh *m, const char *name) {
   FieldRef f;

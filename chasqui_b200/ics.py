@@ -13,9 +13,10 @@ reference-compatible reader.
 
 Primitive -> conserved conversion follows src/pgen.hpp:286-300 (face-averaged centred B,
 E = p/(gamma-1) + rho v^2/2 + B^2/2, entropy rho * p / rho^gamma) with the same operation
-order. Noise draw order: numpy Generator(PCG64(seed)).random over the active cells in C
-order (k, j, i), value 1 + amp * (2 U - 1); ghost cells are filled later by the boundary
-kernel, exactly as after the reference's Initialize().
+order. Noise: U = splitmix64(seed, n) / 2^53 for the active cell n in C order (k, j, i),
+rho = 1 + amp * (2 U - 1) — the same counter-based stream as the device generator
+(chq_init_problem), so host and device blasts are bitwise identical; ghost cells are filled
+later by the boundary kernel, exactly as after the reference's Initialize().
 """
 from __future__ import annotations
 
@@ -82,6 +83,16 @@ def _conserve(g: Grid, d, vx, vy, vz, p, b1, b2, b3, gamma):
     return u
 
 
+def splitmix_uniform(seed: int, idx: np.ndarray) -> np.ndarray:
+    """splitmix64 of (seed, idx) -> uniform doubles in [0, 1) from the top 53 bits."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (idx.astype(np.uint64) + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
 def blast_noise(n: int, seed: int = 20261203, amp: float = 1e-3, pres_in: float = 10.0, pres_out: float = 0.1,
                 radius: float = 0.1, b0: float = 1.0, angle_deg: float = 45.0, gamma: float = 5.0 / 3.0, ng: int = 3):
     g = Grid(n, n, n, ng, -0.5, 0.5, -0.5, 0.5, -0.5, 0.5)
@@ -99,9 +110,9 @@ def blast_noise(n: int, seed: int = 20261203, amp: float = 1e-3, pres_in: float 
     r = np.sqrt(x[None, None, :] ** 2 + y[None, :, None] ** 2 + z[:, None, None] ** 2)
     p = np.where(r < radius, pres_in, pres_out)
     d = np.ones((g.nk, g.nj, g.ni))
-    rng = np.random.Generator(np.random.PCG64(seed))
-    noise = rng.random((n, n, n))
-    d[g.ks:g.ks + n, g.js:g.js + n, g.is_:g.is_ + n] = 1.0 + amp * (2.0 * noise - 1.0)
+    if amp != 0.0:
+        noise = splitmix_uniform(seed, np.arange(n * n * n, dtype=np.uint64)).reshape(n, n, n)
+        d[g.ks:g.ks + n, g.js:g.js + n, g.is_:g.is_ + n] = 1.0 + amp * (2.0 * noise - 1.0)
     zero = np.zeros_like(d)
     u = _conserve(g, d, zero, zero, zero, p, b1, b2, b3, gamma)
     return g, u, b1, b2, b3

@@ -155,6 +155,7 @@ def config_from_params(pin: Params) -> dict:
         c[f"{ax}min"] = pin.get_or_add_real("mesh", f"{ax}min", 0.0)
         c[f"{ax}max"] = pin.get_or_add_real("mesh", f"{ax}max", 1.0)
     c["tlim"] = pin.get_or_add_real("time", "tlim", 1.0)
+    c["nlim"] = pin.get_or_add_int("time", "nlim", -1)
     prec = pin.get_or_add_string("mhd", "precision", "fp64")
     if prec not in ("fp64", "mixed"):
         raise ParamError("unknown precision: " + prec)

@@ -58,6 +58,7 @@ typedef struct chq_config {
   int sts;                /* RKL2 super-time-stepping of the diffusive terms */
   int precision;          /* CHQ_FP64 or CHQ_MIXED */
   double tlim;            /* end time used by chq_cycles */
+  int nlim;               /* < 0: no cycle limit; else stop after nlim cycles (time.nlim) */
 } chq_config;
 
 typedef struct chq_mesh chq_mesh;
@@ -71,8 +72,9 @@ CHQ_API int chq_mesh_create(const chq_config *cfg, chq_mesh **out);
 CHQ_API int chq_mesh_destroy(chq_mesh *m);
 /* dims[0..9] = nx1, nx2, nx3, ng, ni, nj, nk, nstage, two_d, three_d */
 CHQ_API int chq_mesh_dims(const chq_mesh *m, int dims[10]);
-/* device bytes held by the mesh */
+/* device bytes held by the mesh, and what chq_mesh_create would allocate for a config */
 CHQ_API long long chq_mesh_bytes(const chq_mesh *m);
+CHQ_API long long chq_config_bytes(const chq_config *cfg);
 CHQ_API const char *chq_last_error(void);
 
 /* ---- state transfer in the reference layout ---------------------------------------------
@@ -106,6 +108,18 @@ CHQ_API int chq_fofc_repair(chq_mesh *m, int dir, int cur, void *stream);
 CHQ_API int chq_limit_fluxes(chq_mesh *m, int dir, double beta_dt, long *count, void *stream);
 /* one whole RK stage: Stage() of src/main.cpp:46-93 (FOFC decision on the device) */
 CHQ_API int chq_stage(chq_mesh *m, int cur, int out, double g0, double g1, double beta_dt, void *stream);
+
+/* ---- problem generators on the device (src/pgen.hpp:269-307 for these problems) ---------
+ * Write the initial u0 / b?f0 of every cell and face (ghosts included); call chq_prime next.
+ *   CHQ_PGEN_ORSZAG_TANG  params {beta}: pressure beta*B0^2/2, beta <= 0: the reference's
+ *                         5/(12 pi) (src/pgen.hpp:94-111)
+ *   CHQ_PGEN_CPAW         params {m1, m2, m3, dens, pres, b_par, amp}: circularly polarised
+ *                         Alfven wave along 2 pi (m1/L1, m2/L2, m3/L3) of the mesh box
+ *   CHQ_PGEN_BLAST        params {pres_in, pres_out, radius, b0, angle_deg, noise_amp, seed}:
+ *                         src/pgen.hpp:114-135 with rho = 1 + amp (2U - 1), U from a
+ *                         splitmix64 stream of (seed, active-cell index in C order) */
+enum { CHQ_PGEN_ORSZAG_TANG = 0, CHQ_PGEN_CPAW = 1, CHQ_PGEN_BLAST = 2 };
+CHQ_API int chq_init_problem(chq_mesh *m, int problem, const double *params, int nparams, void *stream);
 
 /* ---- whole cycles with the time step on the device (src/main.cpp:200-201, 246-297) ----- */
 /* Boundaries + ConsToPrim(dt) of u0/b?f0 and reset of the clock to t. */
@@ -167,6 +181,35 @@ CHQ_API int chq_batch_status(chq_batch *b, double *t, int *cycle, int *done);
 CHQ_API long long chq_batch_kernel_launches(const chq_batch *b);
 /* the batch's own stream (cudaStream_t) */
 CHQ_API void *chq_batch_stream(chq_batch *b);
+
+/* ---- continuous-batching server (no reference counterpart) -------------------------------
+ * Jobs = a mesh configuration (tlim / nlim bound the run), a device problem generator and
+ * its parameters. chq_server_step() retires finished jobs (keeping their history sums and
+ * freeing their memory), admits queued jobs in submission order while they fit the HBM
+ * budget and the slot limit, rebuilds the batch of every class whose membership changed and
+ * launches cycles_per_step batched cycles of every class, each class on its own stream as a
+ * replayed CUDA graph. A job whose final state is not finite is reported FAILED; kernels
+ * index only their own job, so it never disturbs the others. Times are seconds on the
+ * server clock. */
+enum { CHQ_JOB_QUEUED = 0, CHQ_JOB_RUNNING = 1, CHQ_JOB_DONE = 2, CHQ_JOB_FAILED = 3 };
+typedef struct chq_job_status {
+  int state, cycle;
+  double t, t_submit, t_start, t_done;
+  long long zone_updates, bytes;
+  double history[10];    /* chq_history() of the final state (DONE jobs) */
+} chq_job_status;
+typedef struct chq_server chq_server;
+CHQ_API int chq_server_create(long long hbm_budget_bytes, int max_active, int cycles_per_step, chq_server **out);
+CHQ_API int chq_server_submit(chq_server *s, const chq_config *cfg, int problem, const double *params, int nparams,
+                              long long *job_id);
+/* One scheduling round; returns the number of running + queued jobs (0: idle) or < 0. */
+CHQ_API int chq_server_step(chq_server *s);
+CHQ_API int chq_server_status(chq_server *s, long long job_id, chq_job_status *st);
+/* The device mesh of a RUNNING job (NULL otherwise), e.g. to download its state. */
+CHQ_API chq_mesh *chq_server_job_mesh(chq_server *s, long long job_id);
+CHQ_API int chq_server_stats(chq_server *s, long long *used_bytes, int *active, int *queued, long long *zone_updates,
+                             double *clock);
+CHQ_API int chq_server_destroy(chq_server *s);
 
 /* ---- history sums without any device allocation --------------------------------------------
  * No counterpart in the reference. For callers that cannot allocate device memory: an

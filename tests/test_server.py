@@ -1,0 +1,109 @@
+"""Continuous-batching server (chq_server_*): jobs admitted against an HBM budget while
+others run, mixed classes on concurrent streams, results identical to the same job run
+alone, failures quarantined. Failure injection happens on the host side (a NaN written
+into one job's state); nothing here faults or traps the GPU."""
+import math
+
+import numpy as np
+import pytest
+
+from chasqui_b200 import ChqError, Mesh, Server, make_config
+from chasqui_b200.core import load_library
+
+pytestmark = pytest.mark.gpu
+
+
+def ot_cfg(n, nlim, **kw):
+    return make_config(nx1=n, nx2=n, nx3=1, cfl=0.4, tlim=0.5, nlim=nlim, **kw)
+
+
+def blast_cfg(n, nlim, **kw):
+    return make_config(nx1=n, nx2=n, nx3=n, x1min=-.5, x1max=.5, x2min=-.5, x2max=.5, x3min=-.5, x3max=.5,
+                       cfl=0.3, tlim=0.2, nlim=nlim, **kw)
+
+
+def cpaw_cfg(n, nlim, **kw):
+    return make_config(nx1=n, nx2=n, nx3=n, cfl=0.4, tlim=0.6, nlim=nlim, recon=3, **kw)
+
+
+JOBS = [
+    (lambda: ot_cfg(32, 12), "orszag_tang", [-1.0]),
+    (lambda: blast_cfg(16, 9), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 7.0]),
+    (lambda: ot_cfg(48, 20), "orszag_tang", [2.0]),
+    (lambda: cpaw_cfg(16, 8, precision=1), "cpaw", [1, 1, 1, 1.0, 0.1, 1.0, 0.1]),
+    (lambda: blast_cfg(12, 5, precision=1), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 9.0]),
+    (lambda: ot_cfg(24, 15, recon=3), "orszag_tang", [0.5]),
+]
+
+
+def solo_history(cfg, problem, params):
+    m = Mesh(cfg)
+    m.init_problem(problem, params)
+    m.prime(0.0)
+    while not m.clock()["cycle"] >= cfg.nlim and m.clock()["t"] < cfg.tlim:
+        m.cycles(4)
+    return m.history(), m.clock()["cycle"]
+
+
+def run_all(srv, max_steps=5000):
+    for _ in range(max_steps):
+        if srv.step() == 0:
+            return
+    raise AssertionError("server did not drain")
+
+
+def test_results_equal_solo_runs_in_any_mix():
+    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=3)
+    ids = [srv.submit(f(), p, prm) for f, p, prm in JOBS]
+    run_all(srv)
+    for jid, (f, p, prm) in zip(ids, JOBS):
+        st = srv.status(jid)
+        h, cyc = solo_history(f(), p, prm)
+        assert st["state"] == "done", st
+        assert st["cycle"] == cyc == f().nlim
+        assert np.array_equal(np.array(st["history"]), h), (p, st["history"], h)
+        assert st["t_done"] >= st["t_start"] >= st["t_submit"]
+
+
+def test_admission_respects_budget_and_drains():
+    one = load_library().chq_config_bytes(blast_cfg(16, 6))
+    srv = Server(hbm_budget_bytes=int(2.5 * one), cycles_per_step=2)
+    ids = [srv.submit(blast_cfg(16, 6), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, float(s)]) for s in range(5)]
+    seen_queued = False
+    for _ in range(2000):
+        n = srv.step()
+        s = srv.stats()
+        assert s["used_bytes"] <= int(2.5 * one)
+        assert s["active"] <= 2
+        seen_queued |= s["queued"] > 0
+        if n == 0:
+            break
+    assert seen_queued
+    assert all(srv.status(j)["state"] == "done" for j in ids)
+    assert srv.stats()["zone_updates"] == 5 * 6 * 16 ** 3
+
+
+def test_rejects_and_quarantines():
+    srv = Server(hbm_budget_bytes=1 << 20, cycles_per_step=2)
+    with pytest.raises(ChqError):
+        srv.submit(ot_cfg(256, 5), "orszag_tang", [-1.0])     # larger than the budget
+    srv = Server(hbm_budget_bytes=8 << 30, cycles_per_step=2)
+    bad = srv.submit(ot_cfg(32, 10), "orszag_tang", [])      # too few parameters -> FAILED at admission
+    good = srv.submit(ot_cfg(32, 10), "orszag_tang", [-1.0])
+    victim = srv.submit(ot_cfg(32, 10), "orszag_tang", [-1.0])
+    srv.step()
+    assert srv.status(bad)["state"] == "failed"
+    # inject a NaN into the victim's momentum (host-side failure injection)
+    import ctypes as C
+    h = srv.job_mesh_handle(victim)
+    lib = load_library()
+    n = lib.chq_array_size(h, b"u0")
+    u = np.empty(n)
+    assert lib.chq_download(h, b"u0", u.ctypes.data_as(C.POINTER(C.c_double)), n, None) == 0
+    u.reshape(6, -1)[1, 1000:1100] = math.nan
+    assert lib.chq_upload(h, b"u0", u.ctypes.data_as(C.POINTER(C.c_double)), n, None) == 0
+    run_all(srv)
+    assert srv.status(victim)["state"] == "failed"
+    assert srv.status(good)["state"] == "done"
+    h_solo, _ = solo_history(ot_cfg(32, 10), "orszag_tang", [-1.0])
+    assert np.array_equal(np.array(srv.status(good)["history"]), h_solo)
