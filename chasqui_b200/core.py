@@ -71,6 +71,7 @@ SIGNATURES = [
     ("chq_cycles", C.c_int, [_P, C.c_int, _P]),
     ("chq_clock", C.c_int, [_P, _D, C.POINTER(C.c_int), _D, _D]),
     ("chq_counters", C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    ("chq_sts_stages", C.c_longlong, [_P]),
     ("chq_history", C.c_int, [_P, _D, _P]),
     ("chq_run_host", C.c_int, [_P, _D, _D, _D, _D, C.c_int, C.c_double, _P]),
     ("chq_set_device", C.c_int, [C.c_int]),
@@ -102,7 +103,7 @@ SIGNATURES = [
 ]
 
 PROFILE_KINDS = ("fluxes", "corner_emf", "update", "fofc_flag", "fofc_repair", "boundaries", "c2p_dt", "limiter",
-                 "step_ctl")
+                 "step_ctl", "diffusion", "sts")
 
 _lib = None
 
@@ -275,6 +276,9 @@ class Mesh:
         a, b = C.c_longlong(), C.c_longlong()
         _check(load_library().chq_counters(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def sts_stages(self) -> int:
+        return int(load_library().chq_sts_stages(self._h))
 
     def history(self) -> np.ndarray:
         out = np.zeros(10)

@@ -89,6 +89,20 @@ CHQ_D int batch_job(const BatchSlot *s, int n, long b) {
   return lo;
 }
 
+// Job j's argument struct copied into the block's shared memory by all threads, so that the
+// batched bodies read their fields with uniform shared loads (the single-mesh kernels read
+// them from the constant bank) instead of holding a private copy in registers or local memory.
+template <class A> CHQ_D const A &stage_args(const A *args, int j, void *smem) {
+  static_assert(sizeof(A) % 4 == 0, "argument structs are word-sized");
+  const unsigned *src = reinterpret_cast<const unsigned *>(args + j);
+  unsigned *dst = static_cast<unsigned *>(smem);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int t = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+  for (int q = t; q < (int)(sizeof(A) / 4); q += nt) dst[q] = __ldg(src + q);
+  __syncthreads();
+  return *static_cast<const A *>(smem);
+}
+
 CHQ_D void batch_block(const BatchSlot &sl, long b, int &bx, int &by, int &bz) {
   const long loc = b - sl.off;
   bx = (int)(loc % sl.gx);

@@ -20,7 +20,19 @@ struct StepCtl {
   int nbad;                      // cells flagged by the FOFC test in the current stage
   int cycle, done, nstage, nlim;   // nlim >= 0: stop after that many cycles (time.nlim)
   int err;                       // nonzero: a kernel detected an invalid launch configuration
+  // explicit diffusion: the parabolic time-step limit joins min_dt (src/diffusion.hpp:159-174)
+  int diff_on, sts, ndim;
+  double nu, eta, kappa, gm1, dxmin;
+  unsigned long long rho_bits;   // min density of the active cells after the last con2prim
 };
+
+// dx_min^2 / (2 ndim max(nu, eta, kappa (gamma-1) / rho_min)) in the reference's order
+CHQ_D double parabolic_dt(const StepCtl *c) {
+  const double rho_min = __longlong_as_double((long long)c->rho_bits);
+  const double chi = (c->kappa > 0) ? c->kappa * c->gm1 / rho_min : 0.0;
+  const double dmax = fmax(fmax(c->nu, c->eta), chi);
+  return c->dxmin * c->dxmin / (2.0 * c->ndim * dmax);
+}
 
 // Start of a cycle: dt = cfl * min_dt, clamped to reach tlim exactly (src/main.cpp:246-248).
 __global__ void ctl_begin_kernel(StepCtl *c, int nlim_left);

@@ -346,8 +346,9 @@ __global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_kernel(const Fl
 template <int R, int S, bool CHAR, class P>
 __global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
   __shared__ P park[8][128];
+  __shared__ __align__(16) unsigned char sa[sizeof(FluxArgs<P>)];
   const int j = batch_job(slots, n, blockIdx.x);
-  const FluxArgs<P> A = args[j];
+  const FluxArgs<P> &A = stage_args(args, j, sa);
   flux_body<R, S, CHAR, P>(A, (long)blockIdx.x - slots[j].off, park);
 }
 

@@ -13,6 +13,7 @@
 #include "chq_common.cuh"
 #include "chq_riemann.cuh"
 #include "chq_ctl.cuh"
+#include "chq_diffusion.cuh"
 
 namespace chq {
 
@@ -237,6 +238,8 @@ template <class P> struct RepairArgs {
   long nface[3];
   const int *done;
   const int *need;
+  int has_diff;             // re-add the diffusive fluxes on repaired active faces
+  DiffArgs<P> diff;
 };
 
 template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k, int j, int i) {
@@ -268,6 +271,13 @@ template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k
   flx[IENT * vs + l] = (f[FD] > P(0)) ? f[FD] * sL : (f[FD] < P(0)) ? f[FD] * sR : P(0.5) * (f[FD] * (sL + sR));
   A.et2[DIR][l] = -f[FBY];
   A.et1[DIR][l] = f[FBZ];
+  // diffusive fluxes exist only on the faces of active cells (src/fofc.hpp:89-93)
+  if (A.has_diff) {
+    const bool af = (DIR == 0) ? (i >= g.is && i <= g.ie + 1 && j >= g.js && j <= g.je && k >= g.ks && k <= g.ke)
+                  : (DIR == 1) ? (j >= g.js && j <= g.je + 1 && i >= g.is && i <= g.ie && k >= g.ks && k <= g.ke)
+                               : (k >= g.ks && k <= g.ke + 1 && i >= g.is && i <= g.ie && j >= g.js && j <= g.je);
+    if (af) diff_face<DIR, P>(A.diff, k, j, i);
+  }
 }
 
 template <class P> CHQ_D void fofc_repair_body(const RepairArgs<P> &A, int bx) {
@@ -600,43 +610,50 @@ template <class P> __global__ void __launch_bounds__(256) corner_emf_batched(con
   int bx, by, bz;
   const int j = batch_job(slots, n, blockIdx.x);
   batch_block(slots[j], blockIdx.x, bx, by, bz);
-  const EmfArgs<P> A = args[j];
+  __shared__ __align__(16) unsigned char sa[sizeof(EmfArgs<P>)];
+  const EmfArgs<P> &A = stage_args(args, j, sa);
   corner_emf_body<P>(A, bx, by, bz);
 }
 template <class P> __global__ void __launch_bounds__(256) update_batched(const UpdateArgs<P> *args, const BatchSlot *slots, int n) {
   int bx, by, bz;
   const int j = batch_job(slots, n, blockIdx.x);
   batch_block(slots[j], blockIdx.x, bx, by, bz);
-  const UpdateArgs<P> A = args[j];
+  __shared__ __align__(16) unsigned char sa[sizeof(UpdateArgs<P>)];
+  const UpdateArgs<P> &A = stage_args(args, j, sa);
   update_body<P>(A, bx, by, bz);
 }
 __global__ void __launch_bounds__(256) fofc_flag_batched(const FlagArgs *args, const BatchSlot *slots, int n) {
   int bx, by, bz;
   const int j = batch_job(slots, n, blockIdx.x);
   batch_block(slots[j], blockIdx.x, bx, by, bz);
-  const FlagArgs A = args[j];
+  __shared__ __align__(16) unsigned char sa[sizeof(FlagArgs)];
+  const FlagArgs &A = stage_args(args, j, sa);
   fofc_flag_body(A, bx, by, bz);
 }
 template <class P> __global__ void __launch_bounds__(256) fofc_repair_batched(const RepairArgs<P> *args, const BatchSlot *slots, int n) {
   const int j = batch_job(slots, n, blockIdx.x);
-  const RepairArgs<P> A = args[j];
+  __shared__ __align__(16) unsigned char sa[sizeof(RepairArgs<P>)];
+  const RepairArgs<P> &A = stage_args(args, j, sa);
   fofc_repair_body<P>(A, (int)(blockIdx.x - slots[j].off));
 }
 template <class P> __global__ void __launch_bounds__(256) limit_batched(const LimitArgs<P> *args, const BatchSlot *slots, int n) {
   const int j = batch_job(slots, n, blockIdx.x);
-  const LimitArgs<P> A = args[j];
+  __shared__ __align__(16) unsigned char sa[sizeof(LimitArgs<P>)];
+  const LimitArgs<P> &A = stage_args(args, j, sa);
   limit_body<P>(A, (int)(blockIdx.x - slots[j].off));
 }
 template <int DIR> __global__ void __launch_bounds__(256) bc_batched(const BcArgs *args, const BatchSlot *slots, int n) {
   const int j = batch_job(slots, n, blockIdx.x);
-  const BcArgs A = args[j];
+  __shared__ __align__(16) unsigned char sa[sizeof(BcArgs)];
+  const BcArgs &A = stage_args(args, j, sa);
   bc_body<DIR>(A, (int)(blockIdx.x - slots[j].off));
 }
 template <class P> __global__ void __launch_bounds__(256) c2p_batched(const C2pArgs<P> *args, const BatchSlot *slots, int n) {
   int bx, by, bz;
   const int j = batch_job(slots, n, blockIdx.x);
   batch_block(slots[j], blockIdx.x, bx, by, bz);
-  const C2pArgs<P> A = args[j];
+  __shared__ __align__(16) unsigned char sa[sizeof(C2pArgs<P>)];
+  const C2pArgs<P> &A = stage_args(args, j, sa);
   c2p_body<P>(A, bx, by, bz);
 }
 

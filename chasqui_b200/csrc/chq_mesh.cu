@@ -55,12 +55,14 @@ CHQ_D void ctl_begin(StepCtl *c) {
   c->dt = dt;
   for (int s = 0; s < c->nstage; ++s) c->beta_dt[s] = c->beta[s] * dt;
   c->mdt_bits = 0x7ff0000000000000ULL;
+  c->rho_bits = 0x7ff0000000000000ULL;
 }
 CHQ_D void ctl_end(StepCtl *c) {
   if (c->done) return;
   c->t += c->dt;
   c->cycle += 1;
   c->min_dt = __longlong_as_double((long long)c->mdt_bits);
+  if (c->diff_on && !c->sts) c->min_dt = fmin(c->min_dt, parabolic_dt(c));
 }
 __global__ void ctl_begin_kernel(StepCtl *c, int) { ctl_begin(c); }
 __global__ void ctl_end_kernel(StepCtl *c) { ctl_end(c); }
@@ -88,8 +90,13 @@ __global__ void ctl_prime_kernel(StepCtl *c, double t) {
   c->fofc_count = 0;
   c->limiter_count = 0;
   c->mdt_bits = 0x7ff0000000000000ULL;
+  c->rho_bits = 0x7ff0000000000000ULL;
 }
-__global__ void ctl_take_dt_kernel(StepCtl *c) { c->min_dt = __longlong_as_double((long long)c->mdt_bits); }
+__global__ void ctl_take_dt_kernel(StepCtl *c) {
+  c->min_dt = __longlong_as_double((long long)c->mdt_bits);
+  if (c->diff_on && !c->sts) c->min_dt = fmin(c->min_dt, parabolic_dt(c));
+}
+__global__ void reset_rho_kernel(StepCtl *c) { c->rho_bits = 0x7ff0000000000000ULL; }
 __global__ void reset_bits_kernel(unsigned long long *b) { *b = 0x7ff0000000000000ULL; }
 }  // namespace chq
 
@@ -179,6 +186,14 @@ struct chq_mesh {
   int lo[3][3], hi[3][3], active[3];
   int act_lo[3][3], act_hi[3][3];
   int seglen;
+  // RKL2 work arrays (cfg.sts only): Y0..Y2, M0, Mj on cells; their face-field twins
+  double *sy[3] = {}, *sm0 = nullptr, *smj = nullptr;
+  double *sb[3][3] = {}, *smb0[3] = {}, *smbj[3] = {};
+  bool diff = false;
+  long long sts_stages = 0;
+  // set while the mesh is a member of a batch: the batch's end-of-cycles event, which every
+  // operation on the mesh's own stream waits for (not owned by the mesh)
+  cudaEvent_t batch_evt = nullptr;
   // timing
   cudaEvent_t slots[8] = {};
   bool prof = false;
@@ -197,9 +212,11 @@ const int kHstBlocks = 1184;   // 8 blocks per SM on 148 SMs
 
 // bytes of one mesh slab: 18 double fields (u0, u1, 6 face fields), 39 fields of the
 // primitive type, the int flags, the control block and the history scratch
-size_t slab_size(size_t nel, size_t psize) {
+size_t slab_size(size_t nel, size_t psize, bool sts) {
   auto up = [](size_t x) { return (x + 255) / 256 * 256; };
-  return nel * sizeof(double) * 18 + nel * psize * 39 + up(nel * sizeof(int)) + up(sizeof(StepCtl)) +
+  // RKL2: 5 cell arrays of 6 components and 5 x 3 face fields, all double
+  const size_t sts_fields = sts ? 45 : 0;
+  return nel * sizeof(double) * (18 + sts_fields) + nel * psize * 39 + up(nel * sizeof(int)) + up(sizeof(StepCtl)) +
          up((size_t)(kHstBlocks * 10 + 16) * sizeof(double));
 }
 
@@ -223,7 +240,11 @@ void stage_table(int nstage, int s, double &g0, double &g1, double &beta, int &c
   }
 }
 
-cudaStream_t S(chq_mesh *m, void *s) { return s ? static_cast<cudaStream_t>(s) : m->stream; }
+cudaStream_t S(chq_mesh *m, void *s) {
+  cudaStream_t st = s ? static_cast<cudaStream_t>(s) : m->stream;
+  if (m->batch_evt) cudaStreamWaitEvent(st, m->batch_evt, 0);
+  return st;
+}
 
 template <class P> P *as(void *p) { return static_cast<P *>(p); }
 
@@ -259,7 +280,7 @@ struct Prof {
   }
 };
 enum { PK_FLUX = 0, PK_CORNER = 1, PK_UPDATE = 2, PK_FLAG = 3, PK_REPAIR = 4, PK_BC = 5, PK_C2P = 6, PK_LIMIT = 7,
-       PK_CTL = 8 };
+       PK_CTL = 8, PK_DIFF = 9, PK_STS = 10 };
 
 // ---- fluxes --------------------------------------------------------------------------
 template <class P>
@@ -518,12 +539,12 @@ long bc_threads(const chq_mesh *m, int dir) {
   return g.three_d ? (long)g.ng * (g.nj + 1) * (g.ni + 1) : 0;
 }
 
-int do_bc(chq_mesh *m, int buf, const int *done, cudaStream_t s) {
+int do_bc_ptr(chq_mesh *m, double *u, double *b1, double *b2, double *b3, const int *done, cudaStream_t s) {
   const Geom &g = m->g;
   BcArgs a{};
   a.g = g;
-  a.u = m->u[buf];
-  a.b1 = m->bf[buf][0]; a.b2 = m->bf[buf][1]; a.b3 = m->bf[buf][2];
+  a.u = u;
+  a.b1 = b1; a.b2 = b2; a.b3 = b3;
   a.done = done;
   a.bc = m->cfg.bc1;
   long n = (long)(g.nk + 1) * (g.nj + 1) * g.ng;
@@ -547,14 +568,19 @@ int do_bc(chq_mesh *m, int buf, const int *done, cudaStream_t s) {
   return CHQ_OK;
 }
 
+int do_bc(chq_mesh *m, int buf, const int *done, cudaStream_t s) {
+  return do_bc_ptr(m, m->u[buf], m->bf[buf][0], m->bf[buf][1], m->bf[buf][2], done, s);
+}
+
 template <class P>
-C2pArgs<P> c2p_args(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done) {
+C2pArgs<P> c2p_args_ptr(chq_mesh *m, double *u, const double *b1, const double *b2, const double *b3, int compute_dt,
+                        unsigned long long *bits, StepCtl *fold, const int *done) {
   const Geom &g = m->g;
   C2pArgs<P> a{};
   a.g = g;
   a.eos = m->eos;
-  a.u = m->u[buf];
-  a.b1 = m->bf[buf][0]; a.b2 = m->bf[buf][1]; a.b3 = m->bf[buf][2];
+  a.u = u;
+  a.b1 = b1; a.b2 = b2; a.b3 = b3;
   a.w = as<P>(m->w); a.bcc = as<P>(m->bcc); a.ecc = as<P>(m->ecc);
   a.compute_dt = compute_dt;
   a.mdt_bits = bits;
@@ -563,15 +589,18 @@ C2pArgs<P> c2p_args(chq_mesh *m, int buf, int compute_dt, unsigned long long *bi
   return a;
 }
 
+template <class P>
+C2pArgs<P> c2p_args(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done) {
+  return c2p_args_ptr<P>(m, m->u[buf], m->bf[buf][0], m->bf[buf][1], m->bf[buf][2], compute_dt, bits, fold, done);
+}
+
 Launch3 c2p_grid(const chq_mesh *m) {
   const Geom &g = m->g;
   return {dim3((g.ni + 31) / 32, (g.nj + 7) / 8, g.nk), dim3(32, 8)};
 }
 
 template <class P>
-int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done,
-           cudaStream_t s) {
-  const C2pArgs<P> a = c2p_args<P>(m, buf, compute_dt, bits, fold, done);
+int launch_c2p(chq_mesh *m, const C2pArgs<P> &a, cudaStream_t s) {
   const Launch3 L = c2p_grid(m);
   m->nlaunch += 1;
   c2p_kernel<P><<<L.grid, L.block, 0, s>>>(a);
@@ -579,15 +608,121 @@ int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepC
   return CHQ_OK;
 }
 
+template <class P>
+int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done,
+           cudaStream_t s) {
+  return launch_c2p<P>(m, c2p_args<P>(m, buf, compute_dt, bits, fold, done), s);
+}
+
+// ---- explicit diffusion (src/diffusion.hpp) --------------------------------------------
+CurlB curl_of(const chq_mesh *m, const double *b1, const double *b2, const double *b3) {
+  const Geom &g = m->g;
+  CurlB J{};
+  J.b1 = b1; J.b2 = b2; J.b3 = b3;
+  J.idx1 = 1.0 / g.dx1; J.idx2 = 1.0 / g.dx2; J.idx3 = 1.0 / g.dx3;
+  J.two_d = g.two_d; J.three_d = g.three_d;
+  J.sj = g.sj; J.sk = g.sk;
+  return J;
+}
+
+template <class P>
+DiffArgs<P> diff_args(chq_mesh *m, const double *b1, const double *b2, const double *b3, const int *done, long &tot) {
+  DiffArgs<P> a{};
+  a.g = m->g;
+  a.c = DiffCoef{m->cfg.nu, m->cfg.kappa, m->cfg.eta};
+  a.w = as<P>(m->w);
+  a.bcc = as<P>(m->bcc);
+  a.J = curl_of(m, b1, b2, b3);
+  tot = 0;
+  for (int d = 0; d < 3; ++d) {
+    a.flx[d] = as<P>(m->flx[d]);
+    for (int q = 0; q < 3; ++q) { a.lo[d][q] = m->act_lo[d][q]; a.hi[d][q] = m->act_hi[d][q]; }
+    a.nface[d] = m->active[d] ? (long)(a.hi[d][0] - a.lo[d][0] + 1) * (a.hi[d][1] - a.lo[d][1] + 1) * (a.hi[d][2] - a.lo[d][2] + 1) : 0;
+    tot += a.nface[d];
+  }
+  a.done = done;
+  return a;
+}
+
+// diffusive fluxes of every active direction in one launch (diffusion::Fluxes<0..2>)
+template <class P>
+int do_diff(chq_mesh *m, const double *b1, const double *b2, const double *b3, const int *done, cudaStream_t s) {
+  long tot = 0;
+  const DiffArgs<P> a = diff_args<P>(m, b1, b2, b3, done, tot);
+  if (tot == 0) return CHQ_OK;
+  m->nlaunch += 1;
+  diff_flux_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+// eta J added to the edge EMFs (diffusion::ResistiveEMF); a no-op without resistivity
+template <class P>
+int do_res_emf(chq_mesh *m, const double *b1, const double *b2, const double *b3, const int *done, const int *need,
+               cudaStream_t s) {
+  if (!(m->cfg.eta > 0.0)) return CHQ_OK;
+  const Geom &g = m->g;
+  ResEmfArgs<P> a{};
+  a.g = g;
+  a.eta = m->cfg.eta;
+  a.J = curl_of(m, b1, b2, b3);
+  a.e1 = as<P>(m->e[0]); a.e2 = as<P>(m->e[1]); a.e3 = as<P>(m->e[2]);
+  a.ku = g.three_d ? g.ke + 1 : g.ks + 1;
+  a.ju = g.two_d ? g.je + 1 : g.js + 1;
+  a.done = done;
+  a.need = need;
+  const dim3 grid((unsigned)((g.ie + 2 - g.is + 31) / 32), (unsigned)((a.ju - g.js + 1 + 7) / 8), (unsigned)(a.ku - g.ks + 1));
+  m->nlaunch += 1;
+  resistive_emf_kernel<P><<<grid, dim3(32, 8), 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+// minimum density of the active cells into StepCtl::rho_bits (diffusion::TimeStep's reduction)
+template <class P>
+int do_rho_min(chq_mesh *m, const int *done, cudaStream_t s) {
+  const Geom &g = m->g;
+  const dim3 grid((unsigned)((g.nx1 + 31) / 32), (unsigned)((g.je - g.js + 1 + 7) / 8), (unsigned)(g.ke - g.ks + 1));
+  m->nlaunch += 1;
+  rho_min_kernel<P><<<grid, dim3(32, 8), 0, s>>>(g, as<P>(m->w), &m->ctl->rho_bits, done);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
 #define DISPATCH_P(m, call) ((m)->mixed ? call<float> : call<double>)
 
-// One RK stage (src/main.cpp:46-93) with all decisions on the device.
+// FOFC repair with the diffusive fluxes re-added on repaired active faces when `with_diff`
+template <class P>
+int do_repair_d(chq_mesh *m, int cur, bool with_diff, const int *done, const int *need, cudaStream_t s) {
+  long tot = 0;
+  RepairArgs<P> a = repair_args<P>(m, cur, 7u, done, need, tot);
+  if (tot == 0) return CHQ_OK;
+  if (with_diff) {
+    long nd = 0;
+    a.has_diff = 1;
+    a.diff = diff_args<P>(m, m->bf[cur][0], m->bf[cur][1], m->bf[cur][2], done, nd);
+  }
+  m->nlaunch += 1;
+  fofc_repair_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+// One RK stage (src/main.cpp:46-93) with all decisions on the device. With explicit
+// diffusion (diffusion.sts off) the diffusive fluxes join the hyperbolic ones before the
+// limiter and eta J joins the corner EMFs before the update, also in the FOFC re-run.
 int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, const double *bdt_dev,
               const int *done, cudaStream_t s) {
   int rc;
+  const bool dstage = m->diff && !m->cfg.sts;
+  const double *bc1 = m->bf[cur][0], *bc2 = m->bf[cur][1], *bc3 = m->bf[cur][2];
   {
     Prof p(m, PK_FLUX, s);
     if ((rc = do_fluxes(m, cur, 7u, done, s))) return rc;
+  }
+  if (dstage) {
+    Prof p(m, PK_DIFF, s);
+    if ((rc = DISPATCH_P(m, do_diff)(m, bc1, bc2, bc3, done, s))) return rc;
   }
   if (m->cfg.flux_limiter) {
     Prof p(m, PK_LIMIT, s);
@@ -596,6 +731,10 @@ int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, c
   {
     Prof p(m, PK_CORNER, s);
     if ((rc = DISPATCH_P(m, do_corner)(m, done, nullptr, s))) return rc;
+  }
+  if (dstage) {
+    Prof p(m, PK_DIFF, s);
+    if ((rc = DISPATCH_P(m, do_res_emf)(m, bc1, bc2, bc3, done, nullptr, s))) return rc;
   }
   {
     Prof p(m, PK_UPDATE, s);
@@ -608,12 +747,136 @@ int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, c
       if ((rc = do_flag(m, out, nbad, done, s))) return rc;
     }
     Prof p(m, PK_REPAIR, s);
-    if ((rc = DISPATCH_P(m, do_repair)(m, cur, 7u, done, nbad, s))) return rc;
+    if (m->mixed) rc = do_repair_d<float>(m, cur, dstage, done, nbad, s);
+    else rc = do_repair_d<double>(m, cur, dstage, done, nbad, s);
+    if (rc) return rc;
     if ((rc = DISPATCH_P(m, do_corner)(m, done, nbad, s))) return rc;
+    if (dstage && (rc = DISPATCH_P(m, do_res_emf)(m, bc1, bc2, bc3, done, nbad, s))) return rc;
     if ((rc = DISPATCH_P(m, do_update)(m, out, g0, g1, bdt, bdt_dev, done, nbad, s))) return rc;
   }
   Prof p(m, PK_BC, s);
   return do_bc(m, out, done, s);
+}
+
+// ---- RKL2 super-time-stepping (src/sts.hpp) ---------------------------------------------
+// Number of RKL2 stages covering tau under the parabolic limit dt_par (sts::Stages).
+int sts_stage_count(double tau, double dt_par) {
+  const double r = tau / dt_par;
+  const int s = static_cast<int>(std::ceil(0.5 * (-1.0 + std::sqrt(9.0 + 16.0 * r))));
+  return (s < 2) ? 2 : s;
+}
+
+double sts_b(int j) { return (j <= 2) ? 1.0 / 3.0 : (double(j) * j + j - 2.0) / (2.0 * j * (j + 1.0)); }
+
+struct StsState {
+  double *u;
+  double *b[3];
+};
+
+// M(U, B) of (cell state whose primitives are in w, face fields b) into (mu, mb): zeroed
+// flux and EMF arrays, the diffusive fluxes, eta J, then -div F and -curl E (sts::Operator)
+template <class P>
+int sts_operator(chq_mesh *m, double *const b[3], double *mu, double *const mb[3], cudaStream_t s) {
+  const Geom &g = m->g;
+  const size_t fbytes = (size_t)g.vstride * m->psize;
+  for (int d = 0; d < 3; ++d) {
+    CHQ_CUDA(cudaMemsetAsync(m->flx[d], 0, fbytes * NVAR, s));
+    CHQ_CUDA(cudaMemsetAsync(m->e[d], 0, fbytes, s));
+  }
+  int rc = do_diff<P>(m, b[0], b[1], b[2], nullptr, s);
+  if (rc) return rc;
+  if ((rc = do_res_emf<P>(m, b[0], b[1], b[2], nullptr, nullptr, s))) return rc;
+  StsDivArgs<P> a{};
+  a.g = g;
+  a.f1 = as<P>(m->flx[0]); a.f2 = as<P>(m->flx[1]); a.f3 = as<P>(m->flx[2]);
+  a.e1 = as<P>(m->e[0]); a.e2 = as<P>(m->e[1]); a.e3 = as<P>(m->e[2]);
+  a.mu = mu;
+  a.mb1 = mb[0]; a.mb2 = mb[1]; a.mb3 = mb[2];
+  a.idx1 = 1.0 / g.dx1; a.idx2 = 1.0 / g.dx2; a.idx3 = 1.0 / g.dx3;
+  const Launch3 L = update_grid(m);
+  m->nlaunch += 1;
+  sts_div_kernel<P><<<L.grid, L.block, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+// out = ((a x + b y) + c z) + (d p + e q) on active cells and update-range faces (sts::Combine)
+int sts_combine(chq_mesh *m, const StsState &out, double a, const StsState &x, double b, const StsState &y, double c,
+                const StsState &z, double d, const double *p, double *const pb[3], double e, const double *q,
+                double *const qb[3], cudaStream_t s) {
+  StsCombArgs A{};
+  A.g = m->g;
+  A.a = a; A.b = b; A.c = c; A.d = d; A.e = e;
+  A.out = out.u; A.x = x.u; A.y = y.u; A.z = z.u; A.p = p; A.q = q;
+  for (int k = 0; k < 3; ++k) {
+    A.bo[k] = out.b[k]; A.bx[k] = x.b[k]; A.by[k] = y.b[k]; A.bz[k] = z.b[k]; A.bp[k] = pb[k]; A.bq[k] = qb[k];
+  }
+  const Launch3 L = update_grid(m);
+  m->nlaunch += 1;
+  sts_combine_kernel<<<L.grid, L.block, 0, s>>>(A);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+// Advance the diffusive terms over tau from (u0, b?f0), result back in them (sts::Advance).
+// u1 / b?f1 serve as the fourth rotating buffer, as in the reference.
+template <class P>
+int sts_advance(chq_mesh *m, double tau, double dt_par, cudaStream_t s, int &nst) {
+  const Geom &g = m->g;
+  const size_t ub = (size_t)g.vstride * sizeof(double) * NVAR, fb = (size_t)g.vstride * sizeof(double);
+  nst = sts_stage_count(tau, dt_par);
+  const int ns = nst;
+  const double w1 = 4.0 / (double(ns) * ns + ns - 2.0);
+  StsState Y0{m->sy[0], {m->sb[0][0], m->sb[0][1], m->sb[0][2]}};
+  StsState Y1{m->sy[1], {m->sb[1][0], m->sb[1][1], m->sb[1][2]}};
+  StsState Y2{m->sy[2], {m->sb[2][0], m->sb[2][1], m->sb[2][2]}};
+  StsState spare{m->u[1], {m->bf[1][0], m->bf[1][1], m->bf[1][2]}};
+  double *M0 = m->sm0, *Mj = m->smj;
+  double *MB0[3] = {m->smb0[0], m->smb0[1], m->smb0[2]}, *MBj[3] = {m->smbj[0], m->smbj[1], m->smbj[2]};
+  int rc;
+  CHQ_CUDA(cudaMemcpyAsync(Y0.u, m->u[0], ub, cudaMemcpyDeviceToDevice, s));
+  for (int k = 0; k < 3; ++k) CHQ_CUDA(cudaMemcpyAsync(Y0.b[k], m->bf[0][k], fb, cudaMemcpyDeviceToDevice, s));
+  if ((rc = launch_c2p<P>(m, c2p_args_ptr<P>(m, Y0.u, Y0.b[0], Y0.b[1], Y0.b[2], 0, nullptr, nullptr, nullptr), s)))
+    return rc;
+  if ((rc = sts_operator<P>(m, Y0.b, M0, MB0, s))) return rc;
+  const double mt1 = double(sts_b(1) * w1) * tau;
+  if ((rc = sts_combine(m, Y1, 1.0, Y0, 0.0, Y0, 0.0, Y0, mt1, M0, MB0, 0.0, M0, MB0, s))) return rc;
+  if ((rc = do_bc_ptr(m, Y1.u, Y1.b[0], Y1.b[1], Y1.b[2], nullptr, s))) return rc;
+  StsState yjm2 = Y0, yjm1 = Y1, yj = Y2;
+  for (int j = 2; j <= ns; ++j) {
+    const double b_j = sts_b(j), b_jm1 = sts_b(j - 1), b_jm2 = sts_b(j - 2);
+    const double mu = (2.0 * j - 1.0) / j * b_j / b_jm1;
+    const double nu = -(j - 1.0) / j * b_j / b_jm2;
+    const double mut = mu * w1;
+    const double gt = -(1.0 - b_jm1) * mut;
+    if ((rc = launch_c2p<P>(m, c2p_args_ptr<P>(m, yjm1.u, yjm1.b[0], yjm1.b[1], yjm1.b[2], 0, nullptr, nullptr,
+                                               nullptr), s)))
+      return rc;
+    if ((rc = sts_operator<P>(m, yjm1.b, Mj, MBj, s))) return rc;
+    if ((rc = sts_combine(m, yj, mu, yjm1, nu, yjm2, 1.0 - mu - nu, Y0, mut * tau, Mj, MBj, gt * tau, M0, MB0, s)))
+      return rc;
+    if ((rc = do_bc_ptr(m, yj.u, yj.b[0], yj.b[1], yj.b[2], nullptr, s))) return rc;
+    const StsState freed = (j == 2) ? spare : yjm2;
+    yjm2 = yjm1;
+    yjm1 = yj;
+    yj = freed;
+  }
+  CHQ_CUDA(cudaMemcpyAsync(m->u[0], yjm1.u, ub, cudaMemcpyDeviceToDevice, s));
+  for (int k = 0; k < 3; ++k) CHQ_CUDA(cudaMemcpyAsync(m->bf[0][k], yjm1.b[k], fb, cudaMemcpyDeviceToDevice, s));
+  return CHQ_OK;
+}
+
+// dx_min^2 / (2 ndim max(nu, eta, chi)) on the host, same operations as parabolic_dt
+double host_parabolic_dt(const chq_mesh *m, double rho_min) {
+  const Geom &g = m->g;
+  const int ndim = 1 + g.two_d + g.three_d;
+  double dxmin = g.dx1;
+  if (g.two_d) dxmin = std::fmin(dxmin, g.dx2);
+  if (g.three_d) dxmin = std::fmin(dxmin, g.dx3);
+  const double kappa = m->cfg.kappa, gm1 = m->cfg.gamma - 1.0;
+  const double chi = (kappa > 0) ? kappa * gm1 / rho_min : 0.0;
+  const double dmax = std::fmax(std::fmax(m->cfg.nu, m->cfg.eta), chi);
+  return dxmin * dxmin / (2.0 * ndim * dmax);
 }
 
 // ---- layout conversion ---------------------------------------------------------------
@@ -718,6 +981,7 @@ struct chq_batch {
   void *a_corner = nullptr, *a_corner_need = nullptr;
   StepCtl **ctls = nullptr;
   double *status = nullptr;
+  cudaEvent_t done_evt = nullptr;   // recorded after every chq_batch_cycles call
   bool use_graph = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -920,6 +1184,10 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
 
 void batch_free(chq_batch *B) {
   if (B->stream) cudaStreamSynchronize(B->stream);
+  for (chq_mesh *m : B->jobs)
+    if (m && B->done_evt && m->batch_evt == B->done_evt) m->batch_evt = nullptr;
+  if (B->done_evt) cudaEventDestroy(B->done_evt);
+  B->done_evt = nullptr;
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
   if (B->dev) cudaFree(B->dev);
@@ -976,8 +1244,7 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   const int ng_min = wide ? 3 : 2;
   const int ng = (c.nghost > 0) ? c.nghost : ng_min;
   if (ng < ng_min) return fail(CHQ_ERR_ARG, "nghost too small for the reconstruction method");
-  if (c.nu > 0 || c.kappa > 0 || c.eta > 0 || c.sts)
-    return fail(CHQ_ERR_ARG, "explicit diffusion / RKL2 is not available in this build");
+  if (c.nu < 0 || c.kappa < 0 || c.eta < 0) return fail(CHQ_ERR_ARG, "diffusion coefficients must be >= 0");
 
   chq_mesh *m = new chq_mesh;
   m->cfg = c;
@@ -1030,7 +1297,7 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   const size_t dbytes = nel * sizeof(double), pbytes = nel * m->psize, ibytes = align_up(nel * sizeof(int), 256);
   m->hst_blocks = kHstBlocks;
   const size_t ctl_bytes = align_up(sizeof(StepCtl), 256);
-  m->slab_bytes = slab_size(nel, m->psize);
+  m->slab_bytes = slab_size(nel, m->psize, c.sts != 0);
   cudaError_t e = cudaMalloc(&m->slab, m->slab_bytes);
   if (e != cudaSuccess) {
     delete m;
@@ -1051,12 +1318,34 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   m->ctl = (StepCtl *)p; p += ctl_bytes;
   m->hst_part = (double *)p;
   m->hst_out = m->hst_part + (size_t)m->hst_blocks * 10;
+  p += align_up((size_t)(kHstBlocks * 10 + 16) * sizeof(double), 256);
+  if (c.sts) {
+    for (int q = 0; q < 3; ++q) { m->sy[q] = (double *)p; p += dbytes * 6; }
+    m->sm0 = (double *)p; p += dbytes * 6;
+    m->smj = (double *)p; p += dbytes * 6;
+    for (int q = 0; q < 3; ++q)
+      for (int d = 0; d < 3; ++d) { m->sb[q][d] = (double *)p; p += dbytes; }
+    for (int d = 0; d < 3; ++d) { m->smb0[d] = (double *)p; p += dbytes; }
+    for (int d = 0; d < 3; ++d) { m->smbj[d] = (double *)p; p += dbytes; }
+  }
+  m->diff = (c.nu > 0 || c.kappa > 0 || c.eta > 0);
   e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemsetAsync(m->slab, 0, m->slab_bytes, m->stream);
   if (e == cudaSuccess) {
     StepCtl h{};
     h.tlim = c.tlim;
     h.nlim = c.nlim;
+    h.diff_on = (c.nu > 0 || c.kappa > 0 || c.eta > 0) ? 1 : 0;
+    h.sts = c.sts ? 1 : 0;
+    h.ndim = 1 + g.two_d + g.three_d;
+    h.nu = c.nu;
+    h.eta = c.eta;
+    h.kappa = c.kappa;
+    h.gm1 = c.gamma - 1.0;
+    h.dxmin = g.dx1;
+    if (g.two_d) h.dxmin = std::fmin(h.dxmin, g.dx2);
+    if (g.three_d) h.dxmin = std::fmin(h.dxmin, g.dx3);
+    h.rho_bits = 0x7ff0000000000000ULL;
     h.cfl = c.cfl;
     h.nstage = m->nstage;
     h.mdt_bits = 0x7ff0000000000000ULL;
@@ -1077,6 +1366,7 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
 
 int chq_mesh_destroy(chq_mesh *m) {
   if (!m) return CHQ_OK;
+  if (m->batch_evt) cudaEventSynchronize(m->batch_evt);
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (auto &p : m->pending) { m->pool.push_back(p.b); m->pool.push_back(p.e); }
   for (cudaEvent_t e : m->pool) cudaEventDestroy(e);
@@ -1104,7 +1394,7 @@ long long chq_config_bytes(const chq_config *c) {
   const long ni = c->nx1 + 2 * ng, nj = (c->nx2 > 1) ? c->nx2 + 2 * ng : 1, nk = (c->nx3 > 1) ? c->nx3 + 2 * ng : 1;
   const size_t sj = align_up((size_t)ni + 1, 32);
   const size_t nel = align_up((size_t)(nk + 1) * (nj + 1) * sj, 64);
-  return (long long)slab_size(nel, c->precision == CHQ_MIXED ? sizeof(float) : sizeof(double));
+  return (long long)slab_size(nel, c->precision == CHQ_MIXED ? sizeof(float) : sizeof(double), c->sts != 0);
 }
 
 int chq_init_problem(chq_mesh *m, int problem, const double *prm, int nprm, void *stream) {
@@ -1260,6 +1550,7 @@ int chq_prime(chq_mesh *m, double t, void *stream) {
   if (rc) return rc;
   rc = DISPATCH_P(m, do_c2p)(m, 0, 1, &m->ctl->mdt_bits, m->ctl, nullptr, s);
   if (rc) return rc;
+  if (m->diff && !m->cfg.sts && (rc = DISPATCH_P(m, do_rho_min)(m, nullptr, s))) return rc;
   ctl_take_dt_kernel<<<1, 1, 0, s>>>(m->ctl);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
@@ -1269,6 +1560,7 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
   if (!m || n < 0) return fail(CHQ_ERR_ARG, "bad argument");
   cudaStream_t s = S(m, stream);
   const int *done = &m->ctl->done;
+  const bool sts = m->cfg.sts && m->diff;
   for (int c = 0; c < n; ++c) {
     {
       Prof p(m, PK_CTL, s);
@@ -1285,9 +1577,37 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
       const bool last = (st == m->nstage);
       {
         Prof p(m, PK_C2P, s);
-        rc = DISPATCH_P(m, do_c2p)(m, out, last ? 1 : 0, &m->ctl->mdt_bits, m->ctl, done, s);
+        // with RKL2 the last stage's con2prim takes no dt: the split step comes first
+        rc = DISPATCH_P(m, do_c2p)(m, out, (last && !sts) ? 1 : 0, &m->ctl->mdt_bits, m->ctl, done, s);
       }
       if (rc) return rc;
+      if (last && m->diff) {
+        Prof p(m, PK_DIFF, s);
+        if ((rc = DISPATCH_P(m, do_rho_min)(m, done, s))) return rc;
+      }
+    }
+    if (sts) {
+      // operator-split RKL2 over this cycle's dt (src/main.cpp:282-290): the stage count is
+      // a host decision, so the host reads dt and the density minimum here
+      StepCtl h;
+      CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+      CHQ_CUDA(cudaStreamSynchronize(s));
+      if (h.done) break;
+      double rho_min;
+      std::memcpy(&rho_min, &h.rho_bits, sizeof(rho_min));
+      const double dt_par = host_parabolic_dt(m, rho_min);
+      int nst = 0, rc;
+      {
+        Prof p(m, PK_STS, s);
+        rc = DISPATCH_P(m, sts_advance)(m, h.dt, dt_par, s, nst);
+        if (!rc) rc = do_bc(m, 0, nullptr, s);
+      }
+      if (rc) return rc;
+      m->sts_stages += nst;
+      {
+        Prof p(m, PK_C2P, s);
+        if ((rc = DISPATCH_P(m, do_c2p)(m, 0, 1, &m->ctl->mdt_bits, m->ctl, done, s))) return rc;
+      }
     }
     {
       Prof p(m, PK_CTL, s);
@@ -1299,11 +1619,14 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
   return CHQ_OK;
 }
 
+long long chq_sts_stages(const chq_mesh *m) { return m ? m->sts_stages : 0; }
+
 int chq_clock(chq_mesh *m, double *t, int *cycle, double *dt, double *min_dt) {
   if (!m) return fail(CHQ_ERR_ARG, "null mesh");
   StepCtl h;
-  CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
-  CHQ_CUDA(cudaStreamSynchronize(m->stream));
+  cudaStream_t s = S(m, nullptr);
+  CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
   if (t) *t = h.t;
   if (cycle) *cycle = h.cycle;
   if (dt) *dt = h.dt;
@@ -1314,8 +1637,9 @@ int chq_clock(chq_mesh *m, double *t, int *cycle, double *dt, double *min_dt) {
 int chq_counters(chq_mesh *m, long long *fofc, long long *limiter) {
   if (!m) return fail(CHQ_ERR_ARG, "null mesh");
   StepCtl h;
-  CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
-  CHQ_CUDA(cudaStreamSynchronize(m->stream));
+  cudaStream_t s = S(m, nullptr);
+  CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
   if (fofc) *fofc = h.fofc_count + h.nbad;
   if (limiter) *limiter = h.limiter_count;
   return CHQ_OK;
@@ -1392,7 +1716,7 @@ int chq_host_free(void *ptr) {
 int chq_event_record(chq_mesh *m, int slot) {
   if (!m || slot < 0 || slot >= 8) return fail(CHQ_ERR_ARG, "bad argument");
   if (!m->slots[slot]) CHQ_CUDA(cudaEventCreate(&m->slots[slot]));
-  CHQ_CUDA(cudaEventRecord(m->slots[slot], m->stream));
+  CHQ_CUDA(cudaEventRecord(m->slots[slot], S(m, nullptr)));
   return CHQ_OK;
 }
 
@@ -1406,6 +1730,9 @@ int chq_event_elapsed(chq_mesh *m, int a, int b, float *ms) {
 
 int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   if (!meshes || n < 1 || !out) return fail(CHQ_ERR_ARG, "bad argument");
+  for (int q = 0; q < n; ++q)
+    if (meshes[q] && meshes[q]->diff)
+      return fail(CHQ_ERR_ARG, "batched stepping covers the ideal-MHD stage; step diffusive meshes one by one");
   *out = nullptr;
   const chq_mesh *a = meshes[0];
   for (int j = 0; j < n; ++j) {
@@ -1431,6 +1758,7 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   int rc = B->mixed ? batch_build<float>(B) : batch_build<double>(B);
   if (rc == CHQ_OK) {
     cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->done_evt, cudaEventDisableTiming);
     if (e != cudaSuccess) rc = cuda_fail(e, "batch stream");
   }
   if (rc != CHQ_OK) {
@@ -1438,6 +1766,8 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
     delete B;
     return rc;
   }
+  // an event that has never been recorded counts as complete, so members can wait on it now
+  for (chq_mesh *m : B->jobs) m->batch_evt = B->done_evt;
   *out = B;
   return CHQ_OK;
 }
@@ -1465,6 +1795,7 @@ int chq_batch_cycles(chq_batch *B, int n, void *stream) {
       const int rc = B->mixed ? batch_cycle<float>(B, s) : batch_cycle<double>(B, s);
       if (rc) return rc;
     }
+    CHQ_CUDA(cudaEventRecord(B->done_evt, s));
     return CHQ_OK;
   }
   if (!B->exec) {
@@ -1486,6 +1817,7 @@ int chq_batch_cycles(chq_batch *B, int n, void *stream) {
   }
   for (int c = 0; c < n; ++c) CHQ_CUDA(cudaGraphLaunch(B->exec, s));
   B->nlaunch += B->per_cycle * n;
+  CHQ_CUDA(cudaEventRecord(B->done_evt, s));
   return CHQ_OK;
 }
 

@@ -130,6 +130,9 @@ CHQ_API int chq_cycles(chq_mesh *m, int n, void *stream);
 CHQ_API int chq_clock(chq_mesh *m, double *t, int *cycle, double *dt, double *min_dt);
 /* Synchronises; FOFC corrections and limiter activations so far. */
 CHQ_API int chq_counters(chq_mesh *m, long long *fofc, long long *limiter);
+/* Total RKL2 super-time-stepping stages taken so far (the reference's "super-time-stepping
+ * stages (total)" line, src/main.cpp:303); 0 unless diffusion.sts is on. */
+CHQ_API long long chq_sts_stages(const chq_mesh *m);
 /* output::History (src/output.hpp:91-119) of u0/b?f0: mass mom1 mom2 mom3 etot ekin emag
  * eint divB_max divB_L1 (volume-weighted like the reference). Synchronises. */
 CHQ_API int chq_history(chq_mesh *m, double out[10], void *stream);
@@ -153,8 +156,9 @@ CHQ_API int chq_event_record(chq_mesh *m, int slot);
 CHQ_API int chq_event_elapsed(chq_mesh *m, int from_slot, int to_slot, float *ms);
 /* Per-kernel CUDA-event timing inside the stage sequence (off by default). Kinds:
  * 0 fluxes (K1), 1 corner EMF (K2), 2 update (K3), 3 FOFC flag, 4 FOFC repair + re-run,
- * 5 boundaries (K4), 6 con2prim + dt (K5), 7 positivity limiter, 8 step control. */
-#define CHQ_NPROF 9
+ * 5 boundaries (K4), 6 con2prim + dt (K5), 7 positivity limiter, 8 step control,
+ * 9 explicit diffusion (diffusive fluxes, resistive EMF, density minimum), 10 RKL2 super-step. */
+#define CHQ_NPROF 11
 /* Number of CUDA kernels this mesh has launched so far (including early-exit launches). */
 CHQ_API long long chq_kernel_launches(const chq_mesh *m);
 CHQ_API int chq_profile(chq_mesh *m, int enable);

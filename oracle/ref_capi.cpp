@@ -222,6 +222,7 @@ int chqref_cycle(void *h) { return static_cast<RefSim *>(h)->cycle; }
 double chqref_min_dt(void *h) { return static_cast<RefSim *>(h)->min_dt; }
 long chqref_fofc_count(void *h) { return static_cast<RefSim *>(h)->ph.fofc_count; }
 long chqref_limiter_count(void *h) { return static_cast<RefSim *>(h)->ph.limiter_count; }
+long chqref_sts_stages(void *h) { return static_cast<RefSim *>(h)->ph.sts_stages; }
 void chqref_set_time(void *h, double t, double tlim) {
   RefSim *s = static_cast<RefSim *>(h);
   s->t = t;

@@ -29,6 +29,7 @@ _SIGS = [
     ("chqref_min_dt", C.c_double, [_P]),
     ("chqref_fofc_count", C.c_long, [_P]),
     ("chqref_limiter_count", C.c_long, [_P]),
+    ("chqref_sts_stages", C.c_long, [_P]),
     ("chqref_set_time", None, [_P, C.c_double, C.c_double]),
     ("chqref_array_size", C.c_long, [_P, C.c_char_p]),
     ("chqref_get", C.c_int, [_P, C.c_char_p, _D, C.c_long]),
@@ -188,6 +189,10 @@ class RefSim:
     @property
     def fofc_count(self):
         return lib().chqref_fofc_count(self._h)
+
+    @property
+    def sts_stages(self):
+        return lib().chqref_sts_stages(self._h)
 
     def set_time(self, t, tlim):
         lib().chqref_set_time(self._h, t, tlim)

@@ -154,3 +154,32 @@ def shock_tube(n=64):
 
 def field_loop(n=16, n3=1):
     return FIELD_LOOP.format(n=n, n3=n3)
+
+
+# Sinusoidal decay set-up of the reference's physics tests (diffusion_test generator,
+# src/pgen.hpp:235-266); the coefficient and the perturbed variable come as overrides.
+DIFFUSION = """
+[mesh]
+nx1 = {n1}
+nx2 = {n2}
+nx3 = {n3}
+[time]
+integrator = rk3
+cfl = 0.3
+tlim = 0.5
+[mhd]
+reconstruct = plm
+[problem]
+name = diffusion_test
+var = {var}
+axis = {axis}
+amp = 1.0e-3
+"""
+
+
+def diffusion(var="b", axis=1, n=64, n_other=8):
+    dims = [1, 1, 1]
+    for a in range(axis):
+        dims[a] = n_other
+    dims[axis - 1] = n
+    return DIFFUSION.format(n1=dims[0], n2=dims[1], n3=dims[2], var=var, axis=axis)

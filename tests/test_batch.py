@@ -1,11 +1,16 @@
 """Batched stepping (chq_batch): many meshes of one class advanced with one launch per kernel
-kind per stage. Every member must end bit for bit where it ends when stepped alone, with or
-without CUDA-graph replay, including members that reach their end time at different cycles."""
+kind per stage. In the FP64 form every member must end bit for bit where it ends when stepped
+alone, with or without CUDA-graph replay, including members that reach their end time at
+different cycles. In the mixed form the batched and the single-mesh flux kernels are two
+FP32 instantiations whose multiply-adds the compiler may fuse differently, so a member must
+end bit for bit where it ends in a batch of its own (its result never depends on its
+batch-mates) and within FP32 rounding of the single-mesh run."""
 import numpy as np
 import pytest
 
 from chasqui_b200 import Batch, ChqError, Mesh, Params, config_from_params, make_config
 from tests import cases
+from tests.parity import l1_rel
 
 pytestmark = pytest.mark.gpu
 
@@ -50,10 +55,26 @@ def test_batched_members_equal_solo(name, graph):
     b.cycles(3)
     b.cycles(4)
     st = b.status()
-    for j, m in enumerate(members):
-        assert st[j]["cycle"] == 7 and st[j]["t"] == clocks[j]["t"], (j, st[j], clocks[j])
-        for f in FIELDS:
-            assert np.array_equal(m.get(f), expect[j][f]), (name, j, f)
+    if prec == "mixed":
+        alone = []
+        for t, ov in specs:
+            m = _mesh(t, ov, prec)
+            b1 = Batch([m], graph=graph)
+            b1.cycles(7)
+            st1 = b1.status()[0]
+            alone.append(({f: m.get(f) for f in FIELDS}, st1))
+            b1.close()
+        for j, m in enumerate(members):
+            assert st[j]["cycle"] == 7 and st[j]["t"] == alone[j][1]["t"], (j, st[j], alone[j][1])
+            assert st[j]["t"] == pytest.approx(clocks[j]["t"], rel=1e-6)
+            for f in FIELDS:
+                assert np.array_equal(m.get(f), alone[j][0][f]), (name, j, f)
+                assert l1_rel(m.get(f), expect[j][f]) <= 1e-5, (name, j, f)
+    else:
+        for j, m in enumerate(members):
+            assert st[j]["cycle"] == 7 and st[j]["t"] == clocks[j]["t"], (j, st[j], clocks[j])
+            for f in FIELDS:
+                assert np.array_equal(m.get(f), expect[j][f]), (name, j, f)
     assert b.kernel_launches() > 0
     b.close()
 

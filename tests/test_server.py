@@ -1,13 +1,13 @@
 """Continuous-batching server (chq_server_*): jobs admitted against an HBM budget while
 others run, mixed classes on concurrent streams, results identical to the same job run
-alone, failures quarantined. Failure injection happens on the host side (a NaN written
+alone (see solo_history), failures quarantined. Failure injection happens on the host side (a NaN written
 into one job's state); nothing here faults or traps the GPU."""
 import math
 
 import numpy as np
 import pytest
 
-from chasqui_b200 import ChqError, Mesh, Server, make_config
+from chasqui_b200 import Batch, ChqError, Mesh, Server, make_config
 from chasqui_b200.core import load_library
 
 pytestmark = pytest.mark.gpu
@@ -37,9 +37,19 @@ JOBS = [
 
 
 def solo_history(cfg, problem, params):
+    """The job run by itself: alone on its mesh in the FP64 form (batched FP64 stepping is
+    bitwise equal to it), in a batch of its own in the mixed form (the batched FP32 flux
+    kernel may fuse multiply-adds differently from the single-mesh one)."""
     m = Mesh(cfg)
     m.init_problem(problem, params)
     m.prime(0.0)
+    if cfg.precision == 1:
+        b = Batch([m], graph=True)
+        while not b.status()[0]["done"] and b.status()[0]["cycle"] < cfg.nlim:
+            b.cycles(4)
+        cyc = b.status()[0]["cycle"]
+        b.close()
+        return m.history(), cyc
     while not m.clock()["cycle"] >= cfg.nlim and m.clock()["t"] < cfg.tlim:
         m.cycles(4)
     return m.history(), m.clock()["cycle"]
