@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <math.h>
+#include "chq_divide.cuh"
 
 #define CHQ_HD __host__ __device__ __forceinline__
 #define CHQ_D __device__ __forceinline__
@@ -40,6 +41,8 @@ struct Geom {
   long vstride;   // component stride of multi-component fields
   long nelem;     // elements of one component (= vstride)
   CHQ_HD long idx(int k, int j, int i) const { return (long)k * sk + (long)j * sj + i; }
+  // 32-bit form for offsets within one component (vstride < 2^31 is checked at mesh creation)
+  CHQ_HD int idx32(int k, int j, int i) const { return k * (int)sk + j * (int)sj + i; }
 };
 
 struct EOSp {

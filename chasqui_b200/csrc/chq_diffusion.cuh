@@ -126,13 +126,13 @@ template <int DIR, class P> CHQ_D void diff_face(const DiffArgs<P> &A, int k, in
 
 template <class P> CHQ_D void diff_flux_body(const DiffArgs<P> &A, int bx) {
   if (A.done && *A.done) return;
-  long t = (long)bx * blockDim.x + threadIdx.x;
+  int t = bx * (int)blockDim.x + (int)threadIdx.x;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (t < A.nface[d]) {
       const int ni = A.hi[d][2] - A.lo[d][2] + 1, nj = A.hi[d][1] - A.lo[d][1] + 1;
       const int i = A.lo[d][2] + (int)(t % ni);
-      const long r = t / ni;
+      const int r = t / ni;
       const int j = A.lo[d][1] + (int)(r % nj);
       const int k = A.lo[d][0] + (int)(r / nj);
       if (d == 0) diff_face<0, P>(A, k, j, i);
@@ -140,7 +140,7 @@ template <class P> CHQ_D void diff_flux_body(const DiffArgs<P> &A, int bx) {
       else diff_face<2, P>(A, k, j, i);
       return;
     }
-    t -= A.nface[d];
+    t -= (int)A.nface[d];
   }
 }
 

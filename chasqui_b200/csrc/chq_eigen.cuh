@@ -20,9 +20,9 @@ template <class T> CHQ_HD void eigensystem(T d, T p, T by, T bz, T bx, T gamma, 
   const T isqrtd = T(1) / sqrtd;
   const T asq = gamma * p / d;
   const T a = sqrt_(asq);
-  const T casq = bx * bx / d;
+  const T casq = divz(bx * bx, d);
   const T bperpsq = by * by + bz * bz;
-  const T ctsq = bperpsq / d;
+  const T ctsq = divz(bperpsq, d);
   const T tsum = asq + casq + ctsq;
   const T tdif = asq + ctsq - casq;
   const T disc = sqrt_(fmax_(tdif * tdif + T(4) * ctsq * casq, T(0)));
@@ -70,14 +70,14 @@ template <class T> CHQ_HD void eigensystem(T d, T p, T by, T bz, T bx, T gamma, 
   auto &Lm = E.L;
   const T norm = T(0.5) / asq;
   const T ncff = norm * cff, ncss = norm * css, nqf = norm * qf, nqs = norm * qs;
-  const T naf = norm * af / d, nas = norm * as / d;
-  Lm[0][1] = -ncff; Lm[0][2] = nqs * bety; Lm[0][3] = nqs * betz; Lm[0][4] = norm * alf / d; Lm[0][5] = nas * bety; Lm[0][6] = nas * betz;
+  const T naf = divz(norm * af, d), nas = divz(norm * as, d);
+  Lm[0][1] = -ncff; Lm[0][2] = nqs * bety; Lm[0][3] = nqs * betz; Lm[0][4] = divz(norm * alf, d); Lm[0][5] = nas * bety; Lm[0][6] = nas * betz;
   Lm[1][2] = -T(0.5) * betz; Lm[1][3] = T(0.5) * bety; Lm[1][5] = -T(0.5) * betz * s * isqrtd; Lm[1][6] = T(0.5) * bety * s * isqrtd;
-  Lm[2][1] = -ncss; Lm[2][2] = -nqf * bety; Lm[2][3] = -nqf * betz; Lm[2][4] = norm * als / d; Lm[2][5] = -naf * bety; Lm[2][6] = -naf * betz;
+  Lm[2][1] = -ncss; Lm[2][2] = -nqf * bety; Lm[2][3] = -nqf * betz; Lm[2][4] = divz(norm * als, d); Lm[2][5] = -naf * bety; Lm[2][6] = -naf * betz;
   Lm[3][0] = T(1); Lm[3][4] = -T(1) / asq;
-  Lm[4][1] = ncss; Lm[4][2] = nqf * bety; Lm[4][3] = nqf * betz; Lm[4][4] = norm * als / d; Lm[4][5] = -naf * bety; Lm[4][6] = -naf * betz;
+  Lm[4][1] = ncss; Lm[4][2] = nqf * bety; Lm[4][3] = nqf * betz; Lm[4][4] = divz(norm * als, d); Lm[4][5] = -naf * bety; Lm[4][6] = -naf * betz;
   Lm[5][2] = T(0.5) * betz; Lm[5][3] = -T(0.5) * bety; Lm[5][5] = -T(0.5) * betz * s * isqrtd; Lm[5][6] = T(0.5) * bety * s * isqrtd;
-  Lm[6][1] = ncff; Lm[6][2] = -nqs * bety; Lm[6][3] = -nqs * betz; Lm[6][4] = norm * alf / d; Lm[6][5] = nas * bety; Lm[6][6] = nas * betz;
+  Lm[6][1] = ncff; Lm[6][2] = -nqs * bety; Lm[6][3] = -nqs * betz; Lm[6][4] = divz(norm * alf, d); Lm[6][5] = nas * bety; Lm[6][6] = nas * betz;
 }
 
 }  // namespace chq

@@ -51,8 +51,8 @@ template <class P> struct FluxArgs {
 template <class P> struct DirView {
   const P *src[8];     // cell fields in face-frame order
   const P *bx;         // cell-centred normal field (characteristic projection)
-  long st;             // stride along the sweep
-  long s1, s2;         // strides of the two transverse directions (LHLLD detector)
+  int st;              // stride along the sweep (offsets within a component fit in 32 bits)
+  int s1, s2;          // strides of the two transverse directions (LHLLD detector)
   int has1, has2;
   const double *bn;    // face-normal field of the stage's current state
   P *out[8];           // flux slots (d, u, v, w, E, s) then E_t2, E_t1
@@ -63,7 +63,7 @@ template <class P> CHQ_D DirView<P> dir_view(const FluxArgs<P> &A, int d) {
   const long vs = A.g.vstride;
   const int ivu = IVX + d, ivv = IVX + (d + 1) % 3, ivw = IVX + (d + 2) % 3;
   const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
-  const long strides[3] = {1, A.g.sj, A.g.sk};
+  const int strides[3] = {1, (int)A.g.sj, (int)A.g.sk};
   v.src[0] = A.w + IDN * vs;
   v.src[1] = A.w + ivu * vs;
   v.src[2] = A.w + ivv * vs;
@@ -97,9 +97,9 @@ template <class P> CHQ_D DirView<P> dir_view(const FluxArgs<P> &A, int d) {
 // as its stencil is loaded, so only the cell values (for flattening and the floor
 // fallback) stay live across quantities.
 template <int R, bool CHAR, class P>
-CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, long lc, P aL[8], P aR[8]) {
+CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8], P aR[8]) {
   constexpr int RE = Reach<R>::v;
-  const long st = V.st;
+  const int st = V.st;
   P qc[8];
   P p5[5], um1 = P(0), up1 = P(0);
   if constexpr (!CHAR || R == R_DC) {
@@ -197,7 +197,7 @@ CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, long lc, P aL[
 // ---------------------------------------------------------------------------------------
 // Face work: Riemann solve of the face `lf` (between cells lf - stride and lf).
 template <int S, class P>
-CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, long lf, const P wl[8], const P wr[8]) {
+CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, int lf, const P wl[8], const P wr[8]) {
   const P gamma = P(A.eos.gamma), gm1 = P(A.eos.gm1);
   MState<P> L{wl[0], wl[1], wl[2], wl[3], wl[4], wl[5], wl[6]};
   MState<P> R{wr[0], wr[1], wr[2], wr[3], wr[4], wr[5], wr[6]};
@@ -205,7 +205,7 @@ CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, long lf, const P
   if (A.low_mach) {
     // Thornber et al. (2008) blend of the normal velocities (src/physics.hpp:170-178)
     const P cl = fast_speed(L, b_n, gamma), cr = fast_speed(R, b_n, gamma);
-    const P z = fmin_(P(1), fmax_(fabs_(L.u) / cl, fabs_(R.u) / cr));
+    const P z = fmin_(P(1), fmax_(divz(fabs_(L.u), cl), divz(fabs_(R.u), cr)));
     const P um = P(0.5) * (L.u + R.u), ud = P(0.5) * (z * (L.u - R.u));
     L.u = um + ud;
     R.u = um - ud;
@@ -215,10 +215,10 @@ CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, long lf, const P
     hlld<false>(L, R, b_n, gamma, gm1, f, P(1), P(1));
   } else if constexpr (S == S_LHLLD) {
     // shock detector theta and low-Mach factor phi (src/physics.hpp:183-211)
-    const long lL = lf - V.st;
+    const int lL = lf - V.st;
     const P cfmax = fmax_(fast_speed(L, b_n, gamma), fast_speed(R, b_n, gamma));
     const P *wu = V.src[1], *wv = V.src[2], *ww = V.src[3];
-    const long s1 = V.s1, s2 = V.s2;
+    const int s1 = V.s1, s2 = V.s2;
     const P du = ldg(wu + lf) - ldg(wu + lL);
     P dvw = P(0);
     if (V.has1) {
@@ -234,7 +234,7 @@ CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, long lf, const P
     const P ratio = fmin_(P(1), (-fmin_(du, P(0)) + cfmax) / (-dvw + cfmax));
     const P r2 = ratio * ratio;
     const P theta = r2 * r2;
-    const P chi = fmin_(P(1), fmax_(flow_speed_u(L, b_n), flow_speed_u(R, b_n)) / cfmax);
+    const P chi = fmin_(P(1), divz(fmax_(flow_speed_u(L, b_n), flow_speed_u(R, b_n)), cfmax));
     const P phi = (A.lhlld_phi >= 0.0) ? P(A.lhlld_phi) : chi * (P(2) - chi);
     hlld<true>(L, R, b_n, gamma, gm1, f, theta, phi);
   } else {
@@ -254,21 +254,21 @@ CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, long lf, const P
 
 // ---------------------------------------------------------------------------------------
 template <int R, int S, bool CHAR, class P>
-CHQ_D void sweep_x(const FluxArgs<P> &A, long wid) {
+CHQ_D void sweep_x(const FluxArgs<P> &A, int wid) {
   const int lane = threadIdx.x & 31;
   const int nseg = A.nseg[0];
-  const long row = wid / nseg;
+  const int row = wid / nseg;
   const int seg = (int)(wid - row * nseg);
   const int nj = A.hi[0][1] - A.lo[0][1] + 1;
   const int k = A.lo[0][0] + (int)(row / nj);
-  const int j = A.lo[0][1] + (int)(row - (long)(row / nj) * nj);
+  const int j = A.lo[0][1] + (row - (row / nj) * nj);
   const int c = A.lo[0][2] - 1 + 31 * seg + lane;   // this lane's cell
   const bool have = (c <= A.hi[0][2]);
   const DirView<P> V = dir_view(A, 0);
   P aL[8], aR[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) { aL[n] = P(0); aR[n] = P(0); }
-  const long lc = A.g.idx(k, j, c);
+  const int lc = A.g.idx32(k, j, c);
   if (have) cell_states<R, CHAR, P>(A, V, lc, aL, aR);
   P wl[8];
 #pragma unroll
@@ -280,12 +280,12 @@ CHQ_D void sweep_x(const FluxArgs<P> &A, long wid) {
 // carried to the next face is parked in this thread's shared-memory slot during the
 // Riemann solve, which keeps it out of the registers at the solver's peak.
 template <int R, int S, bool CHAR, class P>
-CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, long wid, P (*park)[128]) {
+CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128]) {
   const int lane = threadIdx.x & 31;
   const int nseg = A.nseg[d];
   const int nchunk = A.nchunk;
   const int chunk = (int)(wid % nchunk);
-  const long rest = wid / nchunk;
+  const int rest = wid / nchunk;
   const int seg = (int)(rest % nseg);
   const int outer = (int)(rest / nseg);
   const int i = 32 * chunk + lane;
@@ -295,18 +295,19 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, long wid, P (*park)[128]) {
   const int f0 = sweep_lo + A.seglen * seg;
   const int f1 = min(f0 + A.seglen - 1, sweep_hi);
   const DirView<P> V = dir_view(A, d);
-  long lc = (d == 1) ? A.g.idx(A.lo[1][0] + outer, f0 - 1, i) : A.g.idx(f0 - 1, A.lo[2][1] + outer, i);
-  P aL[8], aR[8], wl[8];
-  cell_states<R, CHAR, P>(A, V, lc, aL, aR);
+  // cell f0-1 first (its right state only), then cell f and face f for f = f0..f1; one copy
+  // of the cell code in the loop keeps the kernel's instruction footprint small
+  int lc = (d == 1) ? A.g.idx32(A.lo[1][0] + outer, f0 - 1, i) : A.g.idx32(f0 - 1, A.lo[2][1] + outer, i);
+  P wl[8];
 #pragma unroll
-  for (int n = 0; n < 8; ++n) wl[n] = aR[n];
+  for (int n = 0; n < 8; ++n) wl[n] = P(0);
   const int t = threadIdx.x;
-  for (int f = f0; f <= f1; ++f) {
-    lc += V.st;
+  for (int f = f0 - 1; f <= f1; ++f, lc += V.st) {
+    P aL[8], aR[8];
     cell_states<R, CHAR, P>(A, V, lc, aL, aR);
 #pragma unroll
     for (int n = 0; n < 8; ++n) park[n][t] = aR[n];
-    face_flux<S, P>(A, V, lc, wl, aL);
+    if (f >= f0) face_flux<S, P>(A, V, lc, wl, aL);
 #pragma unroll
     for (int n = 0; n < 8; ++n) wl[n] = park[n][t];
   }
@@ -314,24 +315,24 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, long wid, P (*park)[128]) {
 
 // Resident 128-thread blocks per SM the flux kernel is compiled for (register cap). The
 // kernel is bound by FP64 / FP32 instruction latency, so more resident warps pay even with
-// some spilling to L1: measured best at 5 (FP64, 96 registers) and 8 (FP32, 64 registers).
+// some spilling to L1: measured best at 5 (FP64, 96 registers) and 10 (FP32, 48 registers).
 #ifndef CHQ_FLUX_MINB_D
 #define CHQ_FLUX_MINB_D 5
 #endif
 #ifndef CHQ_FLUX_MINB_F
-#define CHQ_FLUX_MINB_F 8
+#define CHQ_FLUX_MINB_F 10
 #endif
 template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUX_MINB_D : CHQ_FLUX_MINB_F; };
 
 template <int R, int S, bool CHAR, class P>
 CHQ_D void flux_body(const FluxArgs<P> &A, long block, P (*park)[128]) {
   if (A.skip && *A.skip) return;
-  const long wid = block * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const long nz = A.nwarp[2], nyz = A.nwarp[2] + A.nwarp[1];
+  const int wid = (int)block * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5);
+  const int nz = (int)A.nwarp[2], nyz = (int)(A.nwarp[2] + A.nwarp[1]);
   if (wid < nyz) {
     const int d = (wid < nz) ? 2 : 1;
     sweep_yz<R, S, CHAR, P>(A, d, (d == 2) ? wid : wid - nz, park);
-  } else if (wid < nyz + A.nwarp[0]) {
+  } else if (wid < nyz + (int)A.nwarp[0]) {
     sweep_x<R, S, CHAR, P>(A, wid - nyz);
   }
 }

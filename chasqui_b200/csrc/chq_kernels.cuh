@@ -208,7 +208,7 @@ CHQ_D void fofc_flag_body(const FlagArgs &A, int bx, int by, int bz) {
     const double d = A.u[IDN * vs + l];
     bool b = (d <= A.eos.dfloor);
     if (!b) {
-      const double ke = 0.5 * (sqr(A.u[IM1 * vs + l]) + sqr(A.u[IM2 * vs + l]) + sqr(A.u[IM3 * vs + l])) / d;
+      const double ke = divz(0.5 * (sqr(A.u[IM1 * vs + l]) + sqr(A.u[IM2 * vs + l]) + sqr(A.u[IM3 * vs + l])), d);
       const double eint = A.u[IEN * vs + l] - ke - 0.5 * (bx * bx + by * by + bz * bz);
       double p = A.eos.gm1 * eint;
       if (A.eos.dual_energy && eint < A.eos.de_eta * fabs(A.u[IEN * vs + l]))
@@ -283,13 +283,13 @@ template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k
 template <class P> CHQ_D void fofc_repair_body(const RepairArgs<P> &A, int bx) {
   if (A.done && *A.done) return;
   if (A.need && *A.need == 0) return;
-  long t = (long)bx * blockDim.x + threadIdx.x;
+  int t = bx * (int)blockDim.x + (int)threadIdx.x;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (t < A.nface[d]) {
       const int ni = A.hi[d][2] - A.lo[d][2] + 1, nj = A.hi[d][1] - A.lo[d][1] + 1;
       const int i = A.lo[d][2] + (int)(t % ni);
-      const long r = t / ni;
+      const int r = t / ni;
       const int j = A.lo[d][1] + (int)(r % nj);
       const int k = A.lo[d][0] + (int)(r / nj);
       if (d == 0) repair_face<0, P>(A, k, j, i);
@@ -297,7 +297,7 @@ template <class P> CHQ_D void fofc_repair_body(const RepairArgs<P> &A, int bx) {
       else repair_face<2, P>(A, k, j, i);
       return;
     }
-    t -= A.nface[d];
+    t -= (int)A.nface[d];
   }
 }
 
@@ -369,8 +369,8 @@ template <int DIR, class P> CHQ_D int limit_face(const LimitArgs<P> &A, int k, i
       b[n] = uR[n] + lam2 * (f[n] - fR[n]);
     }
     if (a[0] < dfl || b[0] < dfl) return false;
-    const P ea = a[4] - P(0.5) * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) / a[0] - emL;
-    const P eb = b[4] - P(0.5) * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]) / b[0] - emR;
+    const P ea = a[4] - divz(P(0.5) * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]), a[0]) - emL;
+    const P eb = b[4] - divz(P(0.5) * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]), b[0]) - emR;
     P pa = gm1 * ea, pb = gm1 * eb;
     if (A.eos.dual_energy) {
       const P sa = (uL[5] - lam2 * (f[5] - fL[5])) / a[0], sb = (uR[5] + lam2 * (f[5] - fR[5])) / b[0];
@@ -394,14 +394,14 @@ template <int DIR, class P> CHQ_D int limit_face(const LimitArgs<P> &A, int k, i
 template <class P> CHQ_D void limit_body(const LimitArgs<P> &A, int bx) {
   if (A.done && *A.done) return;
   const double bdt = A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt;
-  long t = (long)bx * blockDim.x + threadIdx.x;
+  int t = bx * (int)blockDim.x + (int)threadIdx.x;
   int lim = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (t >= 0 && t < A.nface[d]) {
       const int ni = A.hi[d][2] - A.lo[d][2] + 1, nj = A.hi[d][1] - A.lo[d][1] + 1;
       const int i = A.lo[d][2] + (int)(t % ni);
-      const long r = t / ni;
+      const int r = t / ni;
       const int j = A.lo[d][1] + (int)(r % nj);
       const int k = A.lo[d][0] + (int)(r / nj);
       if (d == 0) lim = limit_face<0, P>(A, k, j, i, bdt);
@@ -409,7 +409,7 @@ template <class P> CHQ_D void limit_body(const LimitArgs<P> &A, int bx) {
       else lim = limit_face<2, P>(A, k, j, i, bdt);
       t = -1;
     } else if (t >= 0) {
-      t -= A.nface[d];
+      t -= (int)A.nface[d];
     }
   }
   const unsigned m = __ballot_sync(__activemask(), lim != 0);
@@ -434,9 +434,9 @@ template <int DIR> CHQ_D void bc_body(const BcArgs &A, int bx) {
   const double sgn = (A.bc == BC_REFLECT) ? -1.0 : 1.0;
   if (DIR == 0) {
     // threads over (k in [0,nk], j in [0,nj], gh in [0,ng))
-    const long t = (long)bx * blockDim.x + threadIdx.x;
+    const int t = bx * (int)blockDim.x + (int)threadIdx.x;
     const int gh = (int)(t % g.ng);
-    const long r = t / g.ng;
+    const int r = t / g.ng;
     const int j = (int)(r % (g.nj + 1));
     const int k = (int)(r / (g.nj + 1));
     if (k > g.nk) return;
@@ -461,9 +461,9 @@ template <int DIR> CHQ_D void bc_body(const BcArgs &A, int bx) {
     if (A.bc == 0 && gh == 0) A.b1[row + g.ie + 1] = A.b1[row + g.is];
   } else if (DIR == 1) {
     // threads over (k in [0,nk], gh in [0,ng), i in [0,ni])
-    const long t = (long)bx * blockDim.x + threadIdx.x;
+    const int t = bx * (int)blockDim.x + (int)threadIdx.x;
     const int i = (int)(t % (g.ni + 1));
-    const long r = t / (g.ni + 1);
+    const int r = t / (g.ni + 1);
     const int gh = (int)(r % g.ng);
     const int k = (int)(r / g.ng);
     if (k > g.nk) return;
@@ -489,9 +489,9 @@ template <int DIR> CHQ_D void bc_body(const BcArgs &A, int bx) {
     if (A.bc == 0 && gh == 0) A.b2[g.idx(k, g.je + 1, i)] = A.b2[g.idx(k, g.js, i)];
   } else {
     // threads over (gh in [0,ng), j in [0,nj], i in [0,ni])
-    const long t = (long)bx * blockDim.x + threadIdx.x;
+    const int t = bx * (int)blockDim.x + (int)threadIdx.x;
     const int i = (int)(t % (g.ni + 1));
-    const long r = t / (g.ni + 1);
+    const int r = t / (g.ni + 1);
     const int j = (int)(r % (g.nj + 1));
     const int gh = (int)(r / (g.nj + 1));
     if (gh >= g.ng) return;

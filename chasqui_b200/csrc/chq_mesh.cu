@@ -1267,6 +1267,11 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   g.sj = (long)align_up((size_t)g.ni + 1, 32);
   g.sk = (long)(g.nj + 1) * g.sj;
   g.vstride = (long)align_up((size_t)(g.nk + 1) * g.sk, 64);
+  // kernels index within one component with 32-bit offsets (any mesh that fits in HBM does)
+  if (g.vstride >= (1L << 31) - 64) {
+    delete m;
+    return fail(CHQ_ERR_ARG, "mesh too large: one component exceeds 2^31 elements");
+  }
   g.nelem = g.vstride;
   m->eos = EOSp{c.gamma, c.gamma - 1.0, c.dfloor, c.pfloor, c.de_eta, c.dual_energy};
   m->nstage = c.integrator;

@@ -31,7 +31,7 @@ template <class T> CHQ_HD T mc_slope(T qm, T q0, T qp) {
 
 // CW84 interface value between cells a and b (src/recon.hpp:42-44)
 template <class T> CHQ_HD T ppm_face(T qa, T qb, T dqa, T dqb) {
-  return T(0.5) * (qa + qb) + (dqa - dqb) / T(6);
+  return T(0.5) * (qa + qb) + div6(dqa - dqb);
 }
 
 // CW84 parabola monotonisation of one cell (src/recon.hpp:47-57)
@@ -43,7 +43,7 @@ template <class T> CHQ_HD void ppm_limit(T q, T &qL, T &qR) {
   }
   const T d = qR - qL;
   const T c = q - T(0.5) * (qL + qR);
-  const T d2over6 = d * d / T(6);
+  const T d2over6 = div6(d * d);
   if (d * c > d2over6) qL = T(3) * q - T(2) * qR;
   else if (d * c < -d2over6) qR = T(3) * q - T(2) * qL;
 }
@@ -58,7 +58,7 @@ template <class T> CHQ_HD T ppmx_face(T qm1, T q0, T qp1, T qp2) {
     const T d2r = (q0 + qp2) - T(2) * qp1;
     T d2lim = T(0);
     if (d2 * d2l > T(0) && d2 * d2r > T(0)) d2lim = sgn(d2) * fmin_(fmin_(C * fabs_(d2l), C * fabs_(d2r)), fabs_(d2));
-    qf = T(0.5) * (q0 + qp1) - d2lim / T(6);
+    qf = T(0.5) * (q0 + qp1) - div6(d2lim);
   }
   return qf;
 }
@@ -76,7 +76,7 @@ template <class T> CHQ_HD void ppmx_limit(T qm2, T qm1, T q, T qp1, T qp2, T &qL
     T d2lim = T(0);
     if (d2 * d2c > T(0) && d2 * d2l > T(0) && d2 * d2r > T(0))
       d2lim = sgn(d2) * fmin_(fmin_(C * fabs_(d2l), C * fabs_(d2r)), fmin_(C * fabs_(d2c), fabs_(d2)));
-    const T rho = (fabs_(d2) > T(1e-12) * (fabs_(q) + fabs_(qm1) + fabs_(qp1)) + Tiny<T>::v) ? d2lim / d2 : T(0);
+    const T rho = (fabs_(d2) > T(1e-12) * (fabs_(q) + fabs_(qm1) + fabs_(qp1)) + Tiny<T>::v) ? divz(d2lim, d2) : T(0);
     if (rho < T(1) - T(1e-12)) {
       qL = q - rho * dqm;
       qR = q + rho * dqp;
@@ -96,13 +96,13 @@ template <class T> CHQ_HD T wenoz_right(T fm2, T fm1, T f0, T fp1, T fp2) {
   const T b1 = c13 * sqr((fm1 + fp1) - T(2) * f0) + T(0.25) * sqr(fm1 - fp1);
   const T b2 = c13 * sqr((fp2 + f0) - T(2) * fp1) + T(0.25) * sqr((T(3) * f0 + fp2) - T(4) * fp1);
   const T tau = fabs_(b0 - b2);
-  const T a0 = T(0.1) * (T(1) + tau / (b0 + eps));
-  const T a1 = T(0.6) * (T(1) + tau / (b1 + eps));
-  const T a2 = T(0.3) * (T(1) + tau / (b2 + eps));
+  const T a0 = T(0.1) * (T(1) + divz(tau, b0 + eps));
+  const T a1 = T(0.6) * (T(1) + divz(tau, b1 + eps));
+  const T a2 = T(0.3) * (T(1) + divz(tau, b2 + eps));
   const T inv = T(1) / (a0 + a1 + a2);
-  const T q0 = (T(2) * fm2 - T(7) * fm1 + T(11) * f0) / T(6);
-  const T q1 = (-fm1 + T(5) * f0 + T(2) * fp1) / T(6);
-  const T q2 = (T(2) * f0 + T(5) * fp1 - fp2) / T(6);
+  const T q0 = div6(T(2) * fm2 - T(7) * fm1 + T(11) * f0);
+  const T q1 = div6(-fm1 + T(5) * f0 + T(2) * fp1);
+  const T q2 = div6(T(2) * f0 + T(5) * fp1 - fp2);
   return inv * (a0 * q0 + a1 * q1 + a2 * q2);
 }
 

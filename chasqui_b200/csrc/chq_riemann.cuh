@@ -24,7 +24,7 @@ template <class T> CHQ_HD T fast_speed(const MState<T> &s, T bn, T gamma) {
   const T bsq = bn * bn + s.by * s.by + s.bz * s.bz;
   const T gp = gamma * s.p;
   const T a = (gp + bsq) / s.d;
-  const T disc = a * a - T(4) * gp * bn * bn / (s.d * s.d);
+  const T disc = a * a - divz(T(4) * gp * bn * bn, s.d * s.d);
   return sqrt_(T(0.5) * (a + sqrt_(fmax_(disc, T(0)))));
 }
 
@@ -67,8 +67,8 @@ template <class T> CHQ_HD void flux_from(const MState<T> &s, T bn, T e, T pt, T 
 // modified fast speed with the sound speed replaced by |v| (src/riemann.hpp:44-51)
 template <class T> CHQ_HD T flow_speed_u(const MState<T> &s, T bn) {
   const T vsq = s.u * s.u + s.v * s.v + s.w * s.w;
-  const T casq = (bn * bn + s.by * s.by + s.bz * s.bz) / s.d;
-  const T caxsq = bn * bn / s.d;
+  const T casq = divz(bn * bn + s.by * s.by + s.bz * s.bz, s.d);
+  const T caxsq = divz(bn * bn, s.d);
   const T a = casq + vsq;
   const T disc = a * a - T(4) * vsq * caxsq;
   return sqrt_(T(0.5) * (a + sqrt_(fmax_(disc, T(0)))));
@@ -125,7 +125,7 @@ CHQ_HD void star_side(const MState<T> &S, T slm, T sms, T sm, T bn, T bnsq, T &v
     bys = S.by;
     bzs = S.bz;
   } else {
-    const T num_v = (bn * (sm - S.u)) / den;
+    const T num_v = divz(bn * (sm - S.u), den);
     vs = S.v - S.by * num_v;
     ws = S.w - S.bz * num_v;
     const T num_b = ((S.d * slm) * slm - bnsq) / den;
@@ -219,8 +219,8 @@ CHQ_HD void hlld(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T
   // Alfven waves bounding the double-star region (MK05 eq. 51)
   const T sqdl = sqrt_(dls), sqdr = sqrt_(drs);
   const T abn = fabs_(bn);
-  const T sls = sm - abn / sqdl;
-  const T srs = sm + abn / sqdr;
+  const T sls = sm - divz(abn, sqdl);
+  const T srs = sm + divz(abn, sqdr);
 
   // strict inequalities: with S*_L = S*_R = 0 both sides are averaged below
   if (sls > T(0)) {
