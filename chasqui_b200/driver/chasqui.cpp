@@ -1,0 +1,292 @@
+// chasqui_b200 — command-line driver, a drop-in for the reference's `chasqui` binary:
+//
+//   chasqui -i input.in [-r restart.rst] [block.key=value ...]
+//
+// Same input keys and defaults, problem generators, outputs (.vtk, .hst, .rst, _errors.dat)
+// and end-of-run lines as the reference driver (src/main.cpp:95-329); the time loop runs on
+// the device through the C ABI (include/chq.h): whole cycles are queued with chq_cycles and
+// dt, the FOFC and limiter counts stay on the device. The host reads the clock once per
+// cycle only while outputs are scheduled, otherwise once per `time.ndiag` cycles (at most 256).
+// Gravity and cooling source terms (src/srcterms.hpp) are outside this path: enabling them
+// is an error. `mhd.precision = mixed` selects the mixed FP32/FP64 form. `--write-ic FILE`
+// writes the problem generator's initial state as a restart file and exits without a GPU.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "chq.h"
+#include "outputs.hpp"
+#include "params.hpp"
+#include "problems.hpp"
+
+namespace {
+
+void check(int rc, const char *what) {
+  if (rc != CHQ_OK) throw std::runtime_error(std::string(what) + ": " + chq_last_error());
+}
+
+int parse_bc(const std::string &s) {
+  if (s == "periodic") return CHQ_BC_PERIODIC;
+  if (s == "outflow") return CHQ_BC_OUTFLOW;
+  if (s == "reflect") return CHQ_BC_REFLECT;
+  throw std::runtime_error("unknown boundary condition: " + s);
+}
+
+std::vector<double> download(chq_mesh *m, const char *name) {
+  std::vector<double> v((size_t)chq_array_size(m, name));
+  check(chq_download(m, name, v.data(), (long)v.size(), nullptr), name);
+  return v;
+}
+
+void upload(chq_mesh *m, const char *name, const std::vector<double> &v) {
+  check(chq_upload(m, name, v.data(), (long)v.size(), nullptr), name);
+}
+
+int run(int argc, char **argv) {
+  chqd::Params pin;
+  std::string input, rstfile, icfile;
+  for (int a = 1; a < argc; ++a) {
+    if (!std::strcmp(argv[a], "-i") && a + 1 < argc) input = argv[++a];
+    else if (!std::strcmp(argv[a], "-r") && a + 1 < argc) rstfile = argv[++a];
+    else if (!std::strcmp(argv[a], "--write-ic") && a + 1 < argc) icfile = argv[++a];
+  }
+  if (input.empty()) {
+    std::cerr << "usage: chasqui -i input.in [-r restart.rst] [block.key=value ...]\n";
+    return 1;
+  }
+  pin.read_file(input);
+  for (int a = 1; a < argc; ++a) {
+    if (!std::strcmp(argv[a], "-i") || !std::strcmp(argv[a], "-r") || !std::strcmp(argv[a], "--write-ic")) {
+      ++a;
+      continue;
+    }
+    if (std::strchr(argv[a], '=')) pin.override_with(argv[a]);
+  }
+
+  // ---- configuration (keys and defaults of src/main.cpp:113-185) ----
+  chq_config cfg;
+  chq_config_defaults(&cfg);
+  const std::string r = pin.str("mhd", "reconstruct", "ppm");
+  cfg.recon = (r == "dc") ? CHQ_RECON_DC : (r == "plm") ? CHQ_RECON_PLM : (r == "ppm") ? CHQ_RECON_PPM
+            : (r == "ppmx") ? CHQ_RECON_PPMX : (r == "wenoz") ? CHQ_RECON_WENOZ : -1;
+  if (cfg.recon < 0) throw std::runtime_error("unknown reconstruct: " + r);
+  const std::string rs = pin.str("mhd", "rsolver", "hlld");
+  cfg.rsolver = (rs == "hlld") ? CHQ_RS_HLLD : (rs == "lhlld") ? CHQ_RS_LHLLD : (rs == "hlle") ? CHQ_RS_HLLE : -1;
+  if (cfg.rsolver < 0) throw std::runtime_error("unknown rsolver: " + rs);
+  cfg.characteristic = pin.boolean("mhd", "characteristic", false);
+  cfg.lhlld_phi = pin.real("mhd", "lhlld_phi", -1.0);
+  cfg.dual_energy = pin.boolean("mhd", "dual_energy", false);
+  cfg.de_eta = pin.real("mhd", "de_eta", 1.0e-3);
+  const std::string ti = pin.str("time", "integrator", "rk3");
+  cfg.integrator = (ti == "rk1") ? 1 : (ti == "rk2") ? 2 : (ti == "rk3") ? 3 : (ti == "rk4" || ti == "ssprk43") ? 4 : -1;
+  if (cfg.integrator < 0) throw std::runtime_error("unknown integrator: " + ti);
+  cfg.low_mach = pin.boolean("mhd", "low_mach", false);
+  cfg.flatten = pin.boolean("mhd", "flatten", true);
+  cfg.cfl = pin.real("time", "cfl", 0.3);
+  cfg.gamma = pin.real("mhd", "gamma", 5.0 / 3.0);
+  cfg.dfloor = pin.real("mhd", "dfloor", 1.0e-10);
+  cfg.pfloor = pin.real("mhd", "pfloor", 1.0e-12);
+  cfg.bc1 = parse_bc(pin.str("mesh", "bc_x1", "periodic"));
+  cfg.bc2 = parse_bc(pin.str("mesh", "bc_x2", "periodic"));
+  cfg.bc3 = parse_bc(pin.str("mesh", "bc_x3", "periodic"));
+  cfg.fofc = pin.boolean("mhd", "fofc", true);
+  cfg.flux_limiter = pin.boolean("mhd", "flux_limiter", false);
+  cfg.sts = pin.boolean("diffusion", "sts", false);
+  cfg.nu = pin.real("diffusion", "nu", 0.0);
+  cfg.kappa = pin.real("diffusion", "kappa", 0.0);
+  cfg.eta = pin.real("diffusion", "eta", 0.0);
+  const bool grav = pin.boolean("gravity", "uniform", false) || pin.boolean("gravity", "point_mass", false);
+  const bool cool = pin.boolean("cooling", "enabled", false);
+  if (grav || cool)
+    throw std::runtime_error("gravity and cooling source terms are not part of the device stage path");
+  const std::string prec = pin.str("mhd", "precision", "fp64");
+  cfg.precision = (prec == "fp64") ? CHQ_FP64 : (prec == "mixed") ? CHQ_MIXED : -1;
+  if (cfg.precision < 0) throw std::runtime_error("unknown precision: " + prec + " (fp64 or mixed)");
+
+  chqd::Grid g{};
+  g.nx1 = pin.integer("mesh", "nx1");
+  g.nx2 = pin.integer("mesh", "nx2", 1);
+  g.nx3 = pin.integer("mesh", "nx3", 1);
+  const bool wide = cfg.recon == CHQ_RECON_PPM || cfg.recon == CHQ_RECON_PPMX || cfg.recon == CHQ_RECON_WENOZ;
+  const int ng_min = wide ? 3 : 2;
+  g.ng = pin.integer("mesh", "nghost", ng_min);
+  if (g.ng < ng_min) throw std::runtime_error("nghost too small for the reconstruction method");
+  g.x1min = pin.real("mesh", "x1min", 0.0); g.x1max = pin.real("mesh", "x1max", 1.0);
+  g.x2min = pin.real("mesh", "x2min", 0.0); g.x2max = pin.real("mesh", "x2max", 1.0);
+  g.x3min = pin.real("mesh", "x3min", 0.0); g.x3max = pin.real("mesh", "x3max", 1.0);
+  g.setup();
+  cfg.nx1 = g.nx1; cfg.nx2 = g.nx2; cfg.nx3 = g.nx3; cfg.nghost = g.ng;
+  cfg.x1min = g.x1min; cfg.x1max = g.x1max; cfg.x2min = g.x2min; cfg.x2max = g.x2max;
+  cfg.x3min = g.x3min; cfg.x3max = g.x3max;
+
+  const double tlim = pin.real("time", "tlim", 1.0);
+  const int nlim = pin.integer("time", "nlim", -1);
+  const int ndiag = pin.integer("time", "ndiag", 100);
+  const std::string problem = pin.str("problem", "name");
+  const std::string basename = pin.str("output", "basename", problem);
+  const double dt_vtk = pin.real("output", "vtk_dt", -1.0);
+  const double dt_hst = pin.real("output", "hst_dt", -1.0);
+  const double dt_rst = pin.real("output", "rst_dt", -1.0);
+  const bool compute_error = pin.boolean("output", "compute_error", false);
+  cfg.tlim = tlim;
+  cfg.nlim = nlim;
+
+  std::cout << "# Chasqui MHD\n";
+  pin.print(std::cout);
+  std::cout << "# execution space: CUDA sm_100a (chasqui_b200 device stage path, "
+            << (cfg.precision == CHQ_MIXED ? "mixed FP32/FP64" : "FP64") << ")\n";
+
+  // ---- initial conditions or restart ----
+  double t = 0.0;
+  int cycle = 0;
+  chqd::HostState h(g);
+  if (rstfile.empty()) {
+    chqd::initialize(problem, pin, g, cfg.gamma, h);
+  } else {
+    chqd::read_restart(g, rstfile, t, cycle, h.u, h.b1, h.b2, h.b3);
+    std::cout << "# restarted from " << rstfile << " at t = " << t << ", cycle = " << cycle << "\n";
+  }
+  if (!icfile.empty()) {
+    chqd::write_restart(g, icfile, t, cycle, h.u, h.b1, h.b2, h.b3);
+    std::cout << "# initial state written to " << icfile << "\n";
+    return 0;
+  }
+
+  chq_mesh *m = nullptr;
+  check(chq_mesh_create(&cfg, &m), "mesh");
+  struct Guard {
+    chq_mesh *m;
+    ~Guard() { chq_mesh_destroy(m); }
+  } guard{m};
+  upload(m, "u0", h.u);
+  upload(m, "b1f0", h.b1);
+  upload(m, "b2f0", h.b2);
+  upload(m, "b3f0", h.b3);
+  check(chq_prime(m, t, nullptr), "prime");   // boundaries, con2prim and the first dt
+
+  std::vector<double> u_init, bcc_init;
+  if (compute_error) {
+    u_init = download(m, "u0");
+    bcc_init = download(m, "bcc");
+  }
+
+  // ---- outputs ----
+  int nvtk = 0, nrst = 0;
+  double next_vtk = t, next_hst = t, next_rst = t + dt_rst;
+  std::ofstream hst;
+  if (dt_hst > 0) {
+    hst.open(basename + ".hst", rstfile.empty() ? std::ios::out : std::ios::app);
+    if (rstfile.empty()) hst << "# time dt mass mom1 mom2 mom3 etot ekin emag eint divB_max divB_L1\n";
+  }
+  auto do_outputs = [&](double dt, bool force, bool final_dump) {
+    const double eps = 1e-10 * (tlim > 0 ? tlim : 1.0);
+    if (dt_vtk > 0 && (t >= next_vtk - eps || force)) {
+      char fn[512];
+      std::snprintf(fn, sizeof(fn), "%s.%04d.vtk", basename.c_str(), nvtk++);
+      chqd::write_vtk(g, download(m, "w"), download(m, "bcc"), fn, t, cycle);
+      next_vtk += dt_vtk;
+    }
+    if (dt_hst > 0 && (t >= next_hst - eps || force)) {
+      double hv[10];
+      check(chq_history(m, hv, nullptr), "history");
+      hst << std::setprecision(12) << t << " " << dt;
+      for (double v : hv) hst << " " << v;
+      hst << "\n";
+      hst.flush();
+      next_hst += dt_hst;
+    }
+    if (dt_rst > 0 && (t >= next_rst - eps || final_dump)) {
+      char fn[512];
+      std::snprintf(fn, sizeof(fn), "%s.%04d.rst", basename.c_str(), nrst++);
+      chqd::write_restart(g, fn, t, cycle, download(m, "u0"), download(m, "b1f0"), download(m, "b2f0"),
+                          download(m, "b3f0"));
+      next_rst += dt_rst;
+    }
+  };
+  if (rstfile.empty()) do_outputs(0.0, true, false);
+
+  // ---- time loop on the device ----
+  const bool outputs_on = dt_vtk > 0 || dt_hst > 0 || dt_rst > 0;
+  const int cycle0 = cycle;
+  {
+    double tt, dd, mm;
+    int cc;
+    check(chq_clock(m, &tt, &cc, &dd, &mm), "clock");   // the device is idle when the clock starts
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  while (true) {
+    int chunk = 1;
+    if (!outputs_on) {
+      chunk = 256;
+      if (ndiag > 0) chunk = std::min(chunk, ndiag - (cycle % ndiag));
+    }
+    check(chq_cycles(m, chunk, nullptr), "cycles");
+    double tdev = 0.0, dt = 0.0, mdt = 0.0;
+    int cdev = 0;
+    check(chq_clock(m, &tdev, &cdev, &dt, &mdt), "clock");
+    const int advanced = cycle0 + cdev - cycle;
+    t = tdev;
+    cycle = cycle0 + cdev;
+    if (advanced == 0) break;
+    if (ndiag > 0 && cycle % ndiag == 0)
+      std::cout << "cycle=" << cycle << " time=" << std::setprecision(8) << t << " dt=" << dt << "\n";
+    do_outputs(dt, false, false);
+    if (advanced < chunk) break;
+  }
+  const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (outputs_on) do_outputs(0.0, true, true);
+
+  const double zones = (double)g.nx1 * g.nx2 * g.nx3;
+  const int ncyc = cycle - cycle0;
+  std::cout << "# cycles = " << ncyc << ", time = " << t << ", wall = " << wall << " s\n";
+  std::cout << "# zone-cycles/second = " << std::scientific << zones * ncyc / wall << "\n";
+  long long nfofc = 0, nlimit = 0;
+  check(chq_counters(m, &nfofc, &nlimit), "counters");
+  if (cfg.fofc) std::cout << "# first-order flux corrections applied: " << nfofc << "\n";
+  if (cfg.flux_limiter) std::cout << "# positivity flux limiter activations: " << nlimit << "\n";
+  if (cfg.sts) std::cout << "# super-time-stepping stages (total): " << chq_sts_stages(m) << "\n";
+
+  if (compute_error) {
+    const std::vector<double> u = download(m, "u0"), b = download(m, "bcc");
+    const size_t nc = g.cells();
+    double err[9] = {0}, tot = 0;
+    for (int k = g.ks; k <= g.ke; ++k)
+      for (int j = g.js; j <= g.je; ++j)
+        for (int i = g.is; i <= g.ie; ++i) {
+          const size_t l = g.c(k, j, i);
+          for (int n = 0; n < 6; ++n) err[n] += std::fabs(u[n * nc + l] - u_init[n * nc + l]);
+          for (int n = 0; n < 3; ++n) err[6 + n] += std::fabs(b[n * nc + l] - bcc_init[n * nc + l]);
+        }
+    std::cout << "# L1 errors vs initial state (rho m1 m2 m3 E rho*s B1 B2 B3 | total):\n# ";
+    for (double &e : err) {
+      e /= zones;
+      tot += e;
+      std::cout << e << " ";
+    }
+    std::cout << "| " << tot << "\n";
+    std::ofstream ef(basename + "_errors.dat", std::ios::app);
+    ef << g.nx1 << " " << g.nx2 << " " << g.nx3 << " " << std::scientific << std::setprecision(8);
+    for (double e : err) ef << e << " ";
+    ef << tot << "\n";
+  }
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  try {
+    return run(argc, argv);
+  } catch (const std::exception &e) {
+    std::cerr << "chasqui: " << e.what() << "\n";
+    return 1;
+  }
+}
