@@ -150,6 +150,9 @@ def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, pro
     mesh = Mesh(blast_config(n, precision))
     mesh.init_problem("blast", BLAST_PARAMS)
     mesh.prime(0.0)
+    # flux-kernel march length picked by the library's autotuner on this state (the default
+    # is 16; the per-length launch times are reported beside the choice)
+    tune = mesh.autotune()
     mesh.cycles(warmup)
     mesh.clock()
     l0 = mesh.kernel_launches()
@@ -173,7 +176,16 @@ def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, pro
     mesh.profile(False)
     fofc, _ = mesh.counters()
     return mesh, {"ms": ms, "ms_max": ms_max, "launches": launches, "clock": ck, "prof": prof,
-                  "clocks": sampler.summary() if sampler else None, "fofc": fofc}
+                  "clocks": sampler.summary() if sampler else None, "fofc": fofc, "tune": tune}
+
+
+def tune_summary(tune):
+    """autotuned vs default march length of the flux kernel (ms per launch per length)"""
+    ms = tune["ms"]
+    out = {"default_seglen": 16, "seglen": tune["seglen"], "flux_ms_per_launch": {str(k): v for k, v in ms.items()}}
+    if ms.get(16, -1) > 0 and ms.get(tune["seglen"], -1) > 0:
+        out["speedup_vs_default"] = ms[16] / ms[tune["seglen"]]
+    return out
 
 
 def e2e_host(mesh, steps, warmup, dist):
@@ -420,7 +432,8 @@ def main(argv=None):
                  "hbm_frac_step": (zones * args.steps / (rm["ms"] / 1e3)) * 3 * BYTES_STEP["mixed"] / 1e9 / hbm,
                  "k1_gbs": BYTES_K1["mixed"] * zones / ((km / max(kn, 1)) / 1e3) / 1e9,
                  "speedup_vs_fp64": vm / value,
-                 "kernel_ms_per_step": {k: v[0] / 2 for k, v in pm.items()}}
+                 "kernel_ms_per_step": {k: v[0] / 2 for k, v in pm.items()},
+                 "autotune": tune_summary(rm["tune"])}
         meshm.close()
         del meshm
 
@@ -457,6 +470,7 @@ def main(argv=None):
             "gpu_launches": r64["launches"],
             "clocks": r64["clocks"],
             "fofc_corrections": r64["fofc"],
+            "autotune": tune_summary(r64["tune"]),
             "e2e": e2e,
             "mixed": mixed,
             "ensemble": ens,

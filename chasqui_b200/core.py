@@ -72,6 +72,9 @@ SIGNATURES = [
     ("chq_clock", C.c_int, [_P, _D, C.POINTER(C.c_int), _D, _D]),
     ("chq_counters", C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     ("chq_sts_stages", C.c_longlong, [_P]),
+    ("chq_autotune", C.c_int, [_P, C.POINTER(C.c_int), _D]),
+    ("chq_set_seglen", C.c_int, [_P, C.c_int]),
+    ("chq_get_seglen", C.c_int, [_P]),
     ("chq_history", C.c_int, [_P, _D, _P]),
     ("chq_run_host", C.c_int, [_P, _D, _D, _D, _D, C.c_int, C.c_double, _P]),
     ("chq_set_device", C.c_int, [C.c_int]),
@@ -101,6 +104,9 @@ SIGNATURES = [
     ("chq_history_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       _P, _P, _P, _P, _D, _P]),
 ]
+
+TUNE_LENGTHS = (4, 8, 16, 32, 64)   # CHQ_TUNE_LENGTHS
+TUNE_NLEN = len(TUNE_LENGTHS)
 
 PROFILE_KINDS = ("fluxes", "corner_emf", "update", "fofc_flag", "fofc_repair", "boundaries", "c2p_dt", "limiter",
                  "step_ctl", "diffusion", "sts")
@@ -279,6 +285,22 @@ class Mesh:
 
     def sts_stages(self) -> int:
         return int(load_library().chq_sts_stages(self._h))
+
+    def autotune(self) -> dict:
+        """Pick the y/z march length of the flux kernel by timing it on this mesh's state
+        (call after prime). Returns {"seglen": best, "ms": {length: ms per launch}}."""
+        best = C.c_int()
+        ms = np.zeros(TUNE_NLEN)
+        _check(load_library().chq_autotune(self._h, C.byref(best), _dptr(ms)))
+        return {"seglen": best.value, "ms": {L: float(t) for L, t in zip(TUNE_LENGTHS, ms)}}
+
+    @property
+    def seglen(self) -> int:
+        return int(load_library().chq_get_seglen(self._h))
+
+    @seglen.setter
+    def seglen(self, n: int) -> None:
+        _check(load_library().chq_set_seglen(self._h, int(n)))
 
     def history(self) -> np.ndarray:
         out = np.zeros(10)

@@ -12,6 +12,8 @@
 #include <vector>
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include "chq.h"
 #include "chq_common.cuh"
 #include "chq_ctl.cuh"
@@ -1847,6 +1849,77 @@ long long chq_batch_kernel_launches(const chq_batch *B) { return B ? B->nlaunch 
 void *chq_batch_stream(chq_batch *B) { return B ? (void *)B->stream : nullptr; }
 
 long long chq_kernel_launches(const chq_mesh *m) { return m ? m->nlaunch : 0; }
+
+int chq_set_seglen(chq_mesh *m, int seglen) {
+  if (!m || seglen < 1 || seglen > 1024) return fail(CHQ_ERR_ARG, "march length must be in [1, 1024]");
+  m->seglen = seglen;
+  return CHQ_OK;
+}
+
+int chq_get_seglen(const chq_mesh *m) { return m ? m->seglen : 0; }
+
+int chq_autotune(chq_mesh *m, int *seglen, double ms[CHQ_TUNE_NLEN]) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  static std::mutex mu;
+  static std::map<std::vector<int>, int> cache;
+  const std::vector<int> key = {m->mixed, m->cfg.recon, m->cfg.rsolver, m->cfg.characteristic,
+                                m->g.nx1, m->g.nx2, m->g.nx3};
+  const int cand[CHQ_TUNE_NLEN] = CHQ_TUNE_LENGTHS;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    const auto it = cache.find(key);
+    if (it != cache.end()) {
+      m->seglen = it->second;
+      if (seglen) *seglen = it->second;
+      if (ms)
+        for (int q = 0; q < CHQ_TUNE_NLEN; ++q) ms[q] = -1.0;
+      return CHQ_OK;
+    }
+  }
+  cudaStream_t s = S(m, nullptr);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CHQ_CUDA(cudaEventCreate(&e0));
+  CHQ_CUDA(cudaEventCreate(&e1));
+  const int keep = m->seglen;
+  int best = keep;
+  double best_ms = 1e300;
+  int rc = CHQ_OK;
+  for (int q = 0; q < CHQ_TUNE_NLEN && rc == CHQ_OK; ++q) {
+    m->seglen = cand[q];
+    const int reps = 3;
+    rc = do_fluxes(m, 0, 7u, nullptr, s);   // warm-up (fluxes are scratch: the state is unchanged)
+    if (rc == CHQ_OK) cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && rc == CHQ_OK; ++r) rc = do_fluxes(m, 0, 7u, nullptr, s);
+    if (rc != CHQ_OK) break;
+    cudaEventRecord(e1, s);
+    float t = 0.f;
+    cudaError_t err = cudaEventSynchronize(e1);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+    if (err != cudaSuccess) {
+      rc = cuda_fail(err, "autotune timing");
+      break;
+    }
+    const double per = t / reps;
+    if (ms) ms[q] = per;
+    if (per < best_ms) {
+      best_ms = per;
+      best = cand[q];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != CHQ_OK) {
+    m->seglen = keep;
+    return rc;
+  }
+  m->seglen = best;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = best;
+  }
+  if (seglen) *seglen = best;
+  return CHQ_OK;
+}
 
 int chq_profile(chq_mesh *m, int enable) {
   if (!m) return fail(CHQ_ERR_ARG, "null mesh");

@@ -162,6 +162,22 @@ CHQ_API int chq_event_elapsed(chq_mesh *m, int from_slot, int to_slot, float *ms
 /* Number of CUDA kernels this mesh has launched so far (including early-exit launches). */
 CHQ_API long long chq_kernel_launches(const chq_mesh *m);
 CHQ_API int chq_profile(chq_mesh *m, int enable);
+
+/* ---- flux-kernel autotuning (no reference counterpart: the reference has one fixed
+ * Kokkos range policy) ---------------------------------------------------------------------
+ * March length = faces each thread of the y/z sweeps carries its cell states across. The
+ * default is 16. chq_autotune times the flux kernel of this mesh's scheme on its current
+ * state (call it after chq_prime) for every candidate in CHQ_TUNE_LENGTHS, keeps the fastest
+ * on the mesh, and returns it with the per-candidate ms per launch (ms may be NULL). The
+ * choice is cached for the process per (precision, reconstruction, Riemann solver,
+ * characteristic flag, nx1, nx2, nx3); a later mesh with the same key takes it without
+ * timing (ms then holds -1). Synchronises the mesh stream. Results are bitwise independent
+ * of the length. */
+#define CHQ_TUNE_NLEN 5
+#define CHQ_TUNE_LENGTHS {4, 8, 16, 32, 64}
+CHQ_API int chq_autotune(chq_mesh *m, int *seglen, double ms[CHQ_TUNE_NLEN]);
+CHQ_API int chq_set_seglen(chq_mesh *m, int seglen);
+CHQ_API int chq_get_seglen(const chq_mesh *m);
 /* Synchronises; totals in ms and launch counts per kind since the last reset. */
 CHQ_API int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launches[CHQ_NPROF], int reset);
 

@@ -84,8 +84,7 @@ def _run(exe, args, cwd):
 def read_restart(path):
     with open(path, "rb") as f:
         magic, nx1, nx2, nx3, ng, cycle = struct.unpack("<6i", f.read(24))
-        f.read(4)
-        (time,) = struct.unpack("<d", f.read(8))
+        (time,) = struct.unpack("<d", f.read(8))   # offset 24 is already 8-aligned
         (rs,) = struct.unpack("<i", f.read(4))
         f.read(4)
         data = np.frombuffer(f.read(), dtype=np.float64)
