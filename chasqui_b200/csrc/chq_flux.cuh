@@ -96,10 +96,9 @@ template <class P> CHQ_D DirView<P> dir_view(const FluxArgs<P> &A, int d) {
 // quantities in the frame of the view's direction. Each quantity is reconstructed as soon
 // as its stencil is loaded, so only the cell values (for flattening and the floor
 // fallback) stay live across quantities.
-template <int R, bool CHAR, class P>
-CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8], P aR[8]) {
+template <int R, bool CHAR, class P, class Stencil>
+CHQ_D void cell_states_from(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8], P aR[8], const Stencil &ld) {
   constexpr int RE = Reach<R>::v;
-  const int st = V.st;
   P qc[8];
   P p5[5], um1 = P(0), up1 = P(0);
   if constexpr (!CHAR || R == R_DC) {
@@ -107,7 +106,7 @@ CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8
     for (int n = 0; n < 8; ++n) {
       P q5[5];
 #pragma unroll
-      for (int m = -RE; m <= RE; ++m) q5[2 + m] = ldg(V.src[n] + lc + m * st);
+      ld(n, q5);
 #pragma unroll
       for (int m = RE + 1; m <= 2; ++m) { q5[2 + m] = q5[2 + RE]; q5[2 - m] = q5[2 - RE]; }
       recon_cell<R>(q5, aL[n], aR[n]);
@@ -124,7 +123,7 @@ CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8
 #pragma unroll
     for (int n = 0; n < 7; ++n) {
 #pragma unroll
-      for (int m = -RE; m <= RE; ++m) q[n][2 + m] = ldg(V.src[n] + lc + m * st);
+      ld(n, q[n]);
 #pragma unroll
       for (int m = RE + 1; m <= 2; ++m) { q[n][2 + m] = q[n][2 + RE]; q[n][2 - m] = q[n][2 - RE]; }
       qc[n] = q[n][2];
@@ -164,7 +163,7 @@ CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8
     // entropy scalar, always primitive
     P q5[5];
 #pragma unroll
-    for (int m = -RE; m <= RE; ++m) q5[2 + m] = ldg(V.src[7] + lc + m * st);
+    ld(7, q5);
 #pragma unroll
     for (int m = RE + 1; m <= 2; ++m) { q5[2 + m] = q5[2 + RE]; q5[2 - m] = q5[2 - RE]; }
     recon_cell<R>(q5, aL[7], aR[7]);
@@ -193,6 +192,54 @@ CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8
     for (int n = 0; n < 8; ++n) aR[n] = qc[n];
   }
 }
+
+// Stencil sources of cell_states_from: q5[2-RE .. 2+RE] of quantity n of the cell.
+// Global: cached loads along the sweep (the x-sweep, whose stencil lies in the lanes' lines).
+template <int RE, class P> struct GlobalStencil {
+  const DirView<P> &V;
+  int lc;
+  CHQ_D void operator()(int n, P q5[5]) const {
+#pragma unroll
+    for (int m = -RE; m <= RE; ++m) q5[2 + m] = ldg(V.src[n] + lc + m * V.st);
+  }
+};
+
+template <int R, bool CHAR, class P>
+CHQ_D void cell_states(const FluxArgs<P> &A, const DirView<P> &V, int lc, P aL[8], P aR[8]) {
+  cell_states_from<R, CHAR, P>(A, V, lc, aL, aR, GlobalStencil<Reach<R>::v, P>{V, lc});
+}
+
+// asynchronous global -> shared copies of one element (cp.async, completed per thread)
+CHQ_D void cp_async_elem(double *dst, const double *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+CHQ_D void cp_async_elem(float *dst, const float *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+CHQ_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+CHQ_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Marching window: one shared-memory column per thread and quantity, 2RE+1 slots. For the
+// current cell c, slots 0..2RE-1 hold q[c-RE .. c+RE-1] and slot 2RE holds q[c+RE], copied
+// asynchronously one step earlier. Reading the stencil shifts the window down by one slot
+// (every slot value is consumed by that shift before the next copy into slot 2RE is issued,
+// so the copy cannot overtake the read) and starts the copy of q[c+RE+1] for the next cell.
+template <int RE, class P> struct WindowStencil {
+  P *col;            // this thread's column: slot m of quantity n at col[(n*(2RE+1) + m) * 128]
+  const DirView<P> &V;
+  int lc;
+  bool prefetch;     // false on the last cell of the march
+  CHQ_D void operator()(int n, P q5[5]) const {
+    P *w = col + n * (2 * RE + 1) * 128;
+#pragma unroll
+    for (int m = 0; m <= 2 * RE; ++m) q5[2 - RE + m] = w[m * 128];
+#pragma unroll
+    for (int m = 0; m < 2 * RE; ++m) w[m * 128] = q5[3 - RE + m];
+    if (prefetch) cp_async_elem(w + 2 * RE * 128, V.src[n] + lc + (RE + 1) * V.st);
+  }
+};
 
 // ---------------------------------------------------------------------------------------
 // Face work: Riemann solve of the face `lf` (between cells lf - stride and lf).
@@ -278,9 +325,12 @@ CHQ_D void sweep_x(const FluxArgs<P> &A, int wid) {
 
 // y (d = 1) or z (d = 2) sweep: one code copy, direction in the view. The right state
 // carried to the next face is parked in this thread's shared-memory slot during the
-// Riemann solve, which keeps it out of the registers at the solver's peak.
-template <int R, int S, bool CHAR, class P>
-CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128]) {
+// Riemann solve, which keeps it out of the registers at the solver's peak. With WIN the
+// stencil comes from the thread's marching window in shared memory (WindowStencil): one
+// asynchronous copy per quantity and cell, issued a whole cell ahead, instead of 2RE+1
+// cached loads whose lines a y/z march cannot keep in L1.
+template <int R, int S, bool CHAR, bool WIN, class P>
+CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128], P *win) {
   const int lane = threadIdx.x & 31;
   const int nseg = A.nseg[d];
   const int nchunk = A.nchunk;
@@ -302,9 +352,29 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128]) {
 #pragma unroll
   for (int n = 0; n < 8; ++n) wl[n] = P(0);
   const int t = threadIdx.x;
+  constexpr int RE = Reach<R>::v;
+  constexpr bool use_win = WIN && (RE > 0);
+  P *col = use_win ? win + t : nullptr;
+  if constexpr (use_win) {
+    // window of cell f0-1: q[c-RE .. c+RE-1] now, q[c+RE] asynchronously
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      P *w = col + n * (2 * RE + 1) * 128;
+#pragma unroll
+      for (int m = 0; m < 2 * RE; ++m) w[m * 128] = ldg(V.src[n] + lc + (m - RE) * V.st);
+      cp_async_elem(w + 2 * RE * 128, V.src[n] + lc + RE * V.st);
+    }
+    cp_async_commit();
+  }
   for (int f = f0 - 1; f <= f1; ++f, lc += V.st) {
     P aL[8], aR[8];
-    cell_states<R, CHAR, P>(A, V, lc, aL, aR);
+    if constexpr (use_win) {
+      cp_async_wait_all();
+      cell_states_from<R, CHAR, P>(A, V, lc, aL, aR, WindowStencil<RE, P>{col, V, lc, f < f1});
+      cp_async_commit();
+    } else {
+      cell_states<R, CHAR, P>(A, V, lc, aL, aR);
+    }
 #pragma unroll
     for (int n = 0; n < 8; ++n) park[n][t] = aR[n];
     if (f >= f0) face_flux<S, P>(A, V, lc, wl, aL);
@@ -324,33 +394,68 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128]) {
 #endif
 template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUX_MINB_D : CHQ_FLUX_MINB_F; };
 
+// Single-mesh launches split by sweep: the x-sweep kernel needs no shared window, so it keeps
+// the full L1 and the register cap above; the y/z kernel holds 8 + 8(2RE+1) shared columns
+// per thread (48 KB per block in FP64 PPM / PPMX / WENO-Z), which sets its residency.
+#ifndef CHQ_FLUXYZ_MINB_D
+#define CHQ_FLUXYZ_MINB_D 4
+#endif
+#ifndef CHQ_FLUXYZ_MINB_F
+#define CHQ_FLUXYZ_MINB_F 9
+#endif
+template <class P> struct FluxYzMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUXYZ_MINB_D : CHQ_FLUXYZ_MINB_F; };
+
+template <int R, class P> __host__ __device__ constexpr size_t flux_yz_smem() {
+  return (size_t)(8 + ((Reach<R>::v > 0) ? 8 * (2 * Reach<R>::v + 1) : 0)) * 128 * sizeof(P);
+}
+
 template <int R, int S, bool CHAR, class P>
-CHQ_D void flux_body(const FluxArgs<P> &A, long block, P (*park)[128]) {
+__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_x_kernel(const FluxArgs<P> A) {
   if (A.skip && *A.skip) return;
-  const int wid = (int)block * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5);
+  const int wid = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
+  if (wid < (int)A.nwarp[0]) sweep_x<R, S, CHAR, P>(A, wid);
+}
+
+template <int R, int S, bool CHAR, class P>
+__global__ void __launch_bounds__(128, FluxYzMinBlocks<P>::v) flux_yz_kernel(const FluxArgs<P> A) {
+  extern __shared__ __align__(16) unsigned char flux_dsm[];
+  P (*park)[128] = reinterpret_cast<P (*)[128]>(flux_dsm);
+  P *win = reinterpret_cast<P *>(flux_dsm) + 8 * 128;
+  if (A.skip && *A.skip) return;
+  const int wid = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
   const int nz = (int)A.nwarp[2], nyz = (int)(A.nwarp[2] + A.nwarp[1]);
-  if (wid < nyz) {
-    const int d = (wid < nz) ? 2 : 1;
-    sweep_yz<R, S, CHAR, P>(A, d, (d == 2) ? wid : wid - nz, park);
-  } else if (wid < nyz + (int)A.nwarp[0]) {
-    sweep_x<R, S, CHAR, P>(A, wid - nyz);
-  }
+  if (wid < nz) sweep_yz<R, S, CHAR, true, P>(A, 2, wid, park, win);
+  else if (wid < nyz) sweep_yz<R, S, CHAR, true, P>(A, 1, wid - nz, park, win);
 }
 
+// batched forms: the blocks of many meshes in one launch per sweep kind (chq_batch); each
+// block copies its mesh's arguments to shared memory first
 template <int R, int S, bool CHAR, class P>
-__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_kernel(const FluxArgs<P> A) {
-  __shared__ P park[8][128];
-  flux_body<R, S, CHAR, P>(A, blockIdx.x, park);
-}
-
-// batched form: the blocks of many meshes in one launch (chq_batch)
-template <int R, int S, bool CHAR, class P>
-__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
-  __shared__ P park[8][128];
+__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_x_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
   __shared__ __align__(16) unsigned char sa[sizeof(FluxArgs<P>)];
   const int j = batch_job(slots, n, blockIdx.x);
   const FluxArgs<P> &A = stage_args(args, j, sa);
-  flux_body<R, S, CHAR, P>(A, (long)blockIdx.x - slots[j].off, park);
+  if (A.skip && *A.skip) return;
+  const int wid = (int)(blockIdx.x - slots[j].off) * 4 + (int)(threadIdx.x >> 5);
+  if (wid < (int)A.nwarp[0]) sweep_x<R, S, CHAR, P>(A, wid);
+}
+
+template <int R, class P> __host__ __device__ constexpr size_t flux_yz_batched_smem() {
+  return flux_yz_smem<R, P>() + (sizeof(FluxArgs<P>) + 15) / 16 * 16;
+}
+
+template <int R, int S, bool CHAR, class P>
+__global__ void __launch_bounds__(128, FluxYzMinBlocks<P>::v) flux_yz_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
+  extern __shared__ __align__(16) unsigned char flux_dsm[];
+  P (*park)[128] = reinterpret_cast<P (*)[128]>(flux_dsm);
+  P *win = reinterpret_cast<P *>(flux_dsm) + 8 * 128;
+  const int j = batch_job(slots, n, blockIdx.x);
+  const FluxArgs<P> &A = stage_args(args, j, flux_dsm + flux_yz_smem<R, P>());
+  if (A.skip && *A.skip) return;
+  const int wid = (int)(blockIdx.x - slots[j].off) * 4 + (int)(threadIdx.x >> 5);
+  const int nz = (int)A.nwarp[2], nyz = (int)(A.nwarp[2] + A.nwarp[1]);
+  if (wid < nz) sweep_yz<R, S, CHAR, true, P>(A, 2, wid, park, win);
+  else if (wid < nyz) sweep_yz<R, S, CHAR, true, P>(A, 1, wid - nz, park, win);
 }
 
 }  // namespace chq

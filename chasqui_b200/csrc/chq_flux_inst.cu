@@ -11,9 +11,33 @@
 
 namespace chq {
 
+// per-device one-time opt-in to the dynamic shared memory of a y/z kernel
+template <class K>
+static cudaError_t allow_smem(K kern, size_t smem, bool *ready) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && ready[dev]) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess && dev >= 0 && dev < 64) ready[dev] = true;
+  return e;
+}
+
+// y/z sweeps (shared marching window, dynamic shared memory) then the x-sweep, one stream
 template <int S, bool C>
-static cudaError_t go(const FluxArgs<CHQ_P> &a, unsigned nblocks, cudaStream_t s) {
-  flux_kernel<CHQ_R, S, C, CHQ_P><<<nblocks, 128, 0, s>>>(a);
+static cudaError_t go(const FluxArgs<CHQ_P> &a, unsigned, cudaStream_t s) {
+  const unsigned nyz = (unsigned)((a.nwarp[1] + a.nwarp[2] + 3) / 4), nx = (unsigned)((a.nwarp[0] + 3) / 4);
+  if (nyz) {
+    constexpr size_t smem = flux_yz_smem<CHQ_R, CHQ_P>();
+    static bool ready[64] = {};
+    const cudaError_t ea = allow_smem(flux_yz_kernel<CHQ_R, S, C, CHQ_P>, smem, ready);
+    if (ea != cudaSuccess) return ea;
+    flux_yz_kernel<CHQ_R, S, C, CHQ_P><<<nyz, 128, smem, s>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (nx) flux_x_kernel<CHQ_R, S, C, CHQ_P><<<nx, 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -31,20 +55,30 @@ cudaError_t launch_flux<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> &a, int rsolver, int
 }
 
 template <int S, bool C>
-static cudaError_t gob(const FluxArgs<CHQ_P> *a, const BatchSlot *sl, int n, unsigned nblocks, cudaStream_t s) {
-  flux_batched<CHQ_R, S, C, CHQ_P><<<nblocks, 128, 0, s>>>(a, sl, n);
+static cudaError_t gob(const FluxArgs<CHQ_P> *a, const BatchSlot *sx, const BatchSlot *syz, int n, unsigned nbx,
+                       unsigned nbyz, cudaStream_t s) {
+  if (nbyz) {
+    constexpr size_t smem = flux_yz_batched_smem<CHQ_R, CHQ_P>();
+    static bool ready[64] = {};
+    const cudaError_t e = allow_smem(flux_yz_batched<CHQ_R, S, C, CHQ_P>, smem, ready);
+    if (e != cudaSuccess) return e;
+    flux_yz_batched<CHQ_R, S, C, CHQ_P><<<nbyz, 128, smem, s>>>(a, syz, n);
+    const cudaError_t e2 = cudaGetLastError();
+    if (e2 != cudaSuccess) return e2;
+  }
+  if (nbx) flux_x_batched<CHQ_R, S, C, CHQ_P><<<nbx, 128, 0, s>>>(a, sx, n);
   return cudaGetLastError();
 }
 
 template <>
-cudaError_t launch_flux_batched<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> *a, const BatchSlot *sl, int n, int rsolver,
-                                               int charac, unsigned nblocks, cudaStream_t s) {
-  if (nblocks == 0) return cudaSuccess;
+cudaError_t launch_flux_batched<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> *a, const BatchSlot *sx, const BatchSlot *syz, int n,
+                                               int rsolver, int charac, unsigned nbx, unsigned nbyz, cudaStream_t s) {
+  if (nbx == 0 && nbyz == 0) return cudaSuccess;
   const bool c = (charac != 0) && (CHQ_R != R_DC);
   switch (rsolver) {
-    case S_HLLE: return c ? gob<S_HLLE, true>(a, sl, n, nblocks, s) : gob<S_HLLE, false>(a, sl, n, nblocks, s);
-    case S_HLLD: return c ? gob<S_HLLD, true>(a, sl, n, nblocks, s) : gob<S_HLLD, false>(a, sl, n, nblocks, s);
-    case S_LHLLD: return c ? gob<S_LHLLD, true>(a, sl, n, nblocks, s) : gob<S_LHLLD, false>(a, sl, n, nblocks, s);
+    case S_HLLE: return c ? gob<S_HLLE, true>(a, sx, syz, n, nbx, nbyz, s) : gob<S_HLLE, false>(a, sx, syz, n, nbx, nbyz, s);
+    case S_HLLD: return c ? gob<S_HLLD, true>(a, sx, syz, n, nbx, nbyz, s) : gob<S_HLLD, false>(a, sx, syz, n, nbx, nbyz, s);
+    case S_LHLLD: return c ? gob<S_LHLLD, true>(a, sx, syz, n, nbx, nbyz, s) : gob<S_LHLLD, false>(a, sx, syz, n, nbx, nbyz, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -52,7 +86,7 @@ cudaError_t launch_flux_batched<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> *a, const Ba
 template <int S, bool C>
 static int regs() {
   cudaFuncAttributes at{};
-  if (cudaFuncGetAttributes(&at, flux_kernel<CHQ_R, S, C, CHQ_P>) != cudaSuccess) return -1;
+  if (cudaFuncGetAttributes(&at, flux_yz_kernel<CHQ_R, S, C, CHQ_P>) != cudaSuccess) return -1;
   return at.numRegs;
 }
 

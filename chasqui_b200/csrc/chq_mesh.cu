@@ -977,7 +977,7 @@ struct chq_batch {
     BatchSlot *slots = nullptr;
     long nblocks = 0;
   };
-  Kind k_flux, k_corner, k_update, k_flag, k_repair, k_limit, k_bc[3], k_c2p;
+  Kind k_flux, k_flux_yz, k_corner, k_update, k_flag, k_repair, k_limit, k_bc[3], k_c2p;
   void *a_flux[4] = {}, *a_update[4] = {}, *a_update_need[4] = {}, *a_repair[4] = {}, *a_limit[4] = {},
        *a_c2p[4] = {}, *a_flag[4] = {}, *a_bc[4][3] = {};
   void *a_corner = nullptr, *a_corner_need = nullptr;
@@ -1031,8 +1031,12 @@ int batch_build(chq_batch *B) {
   size_t o_flux_s, o_corner_s, o_update_s, o_flag_s, o_repair_s, o_limit_s, o_bc_s[3], o_c2p_s;
   o_flux_s = slots_of(h, J, [](chq_mesh *m) {
     const FluxArgs<P> a = flux_args<P>(m, 0, 7u);
-    return linear((a.nwarp[0] + a.nwarp[1] + a.nwarp[2]) * 32, 128);
+    return linear(a.nwarp[0] * 32, 128);
   }, B->k_flux.nblocks);
+  const size_t o_flux_yz_s = slots_of(h, J, [](chq_mesh *m) {
+    const FluxArgs<P> a = flux_args<P>(m, 0, 7u);
+    return linear((a.nwarp[1] + a.nwarp[2]) * 32, 128);
+  }, B->k_flux_yz.nblocks);
   o_corner_s = slots_of(h, J, [](chq_mesh *m) { return corner_grid(m); }, B->k_corner.nblocks);
   o_update_s = slots_of(h, J, [](chq_mesh *m) { return update_grid(m); }, B->k_update.nblocks);
   o_flag_s = slots_of(h, J, [](chq_mesh *m) { return flag_grid(m); }, B->k_flag.nblocks);
@@ -1102,6 +1106,7 @@ int batch_build(chq_batch *B) {
   if (e != cudaSuccess) return cuda_fail(e, "batch tables upload");
   char *d = B->dev;
   B->k_flux.slots = (BatchSlot *)(d + o_flux_s);
+  B->k_flux_yz.slots = (BatchSlot *)(d + o_flux_yz_s);
   B->k_corner.slots = (BatchSlot *)(d + o_corner_s);
   B->k_update.slots = (BatchSlot *)(d + o_update_s);
   B->k_flag.slots = (BatchSlot *)(d + o_flag_s);
@@ -1129,13 +1134,14 @@ int batch_build(chq_batch *B) {
 template <class P>
 cudaError_t batch_flux(const chq_batch *B, const FluxArgs<P> *args, cudaStream_t s) {
   const int n = (int)B->jobs.size();
-  const unsigned nb = (unsigned)B->k_flux.nblocks;
+  const unsigned nbx = (unsigned)B->k_flux.nblocks, nbyz = (unsigned)B->k_flux_yz.nblocks;
+  const BatchSlot *sx = B->k_flux.slots, *syz = B->k_flux_yz.slots;
   switch (B->recon) {
-    case R_DC: return launch_flux_batched<P, R_DC>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
-    case R_PLM: return launch_flux_batched<P, R_PLM>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
-    case R_PPM: return launch_flux_batched<P, R_PPM>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
-    case R_PPMX: return launch_flux_batched<P, R_PPMX>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
-    case R_WENOZ: return launch_flux_batched<P, R_WENOZ>(args, B->k_flux.slots, n, B->rsolver, B->charac, nb, s);
+    case R_DC: return launch_flux_batched<P, R_DC>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
+    case R_PLM: return launch_flux_batched<P, R_PLM>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
+    case R_PPM: return launch_flux_batched<P, R_PPM>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
+    case R_PPMX: return launch_flux_batched<P, R_PPMX>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
+    case R_WENOZ: return launch_flux_batched<P, R_WENOZ>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
     default: return cudaErrorInvalidValue;
   }
 }
