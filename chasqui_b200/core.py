@@ -101,6 +101,7 @@ SIGNATURES = [
     ("chq_server_stats", C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_longlong), _D]),
     ("chq_server_destroy", C.c_int, [_P]),
+    ("chq_server_set_lanes", C.c_int, [_P, C.c_int]),
     ("chq_history_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       _P, _P, _P, _P, _D, _P]),
 ]
@@ -355,10 +356,11 @@ PGEN = {"orszag_tang": 0, "cpaw": 1, "blast": 2}
 class Server:
     """Continuous-batching simulation server (chq_server_*)."""
 
-    def __init__(self, hbm_budget_bytes: int, max_active: int = 1024, cycles_per_step: int = 4):
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 1024, cycles_per_step: int = 4, lanes: int = 8):
         h = _P()
         _check(load_library().chq_server_create(int(hbm_budget_bytes), max_active, cycles_per_step, C.byref(h)))
         self._h = h
+        _check(load_library().chq_server_set_lanes(h, int(lanes)))
 
     def submit(self, cfg: chq_config, problem: str, params) -> int:
         a = np.ascontiguousarray(params, dtype=np.float64)

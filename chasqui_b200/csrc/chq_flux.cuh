@@ -221,23 +221,29 @@ CHQ_D void cp_async_elem(float *dst, const float *src) {
 CHQ_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 CHQ_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Threads per block of the y/z kernels (the stride of their shared-memory columns).
+#ifndef CHQ_FLUXYZ_THREADS
+#define CHQ_FLUXYZ_THREADS 128
+#endif
+constexpr int kYzThreads = CHQ_FLUXYZ_THREADS;
+
 // Marching window: one shared-memory column per thread and quantity, 2RE+1 slots. For the
 // current cell c, slots 0..2RE-1 hold q[c-RE .. c+RE-1] and slot 2RE holds q[c+RE], copied
 // asynchronously one step earlier. Reading the stencil shifts the window down by one slot
 // (every slot value is consumed by that shift before the next copy into slot 2RE is issued,
 // so the copy cannot overtake the read) and starts the copy of q[c+RE+1] for the next cell.
 template <int RE, class P> struct WindowStencil {
-  P *col;            // this thread's column: slot m of quantity n at col[(n*(2RE+1) + m) * 128]
+  P *col;            // this thread's column: slot m of quantity n at col[(n*(2RE+1) + m) * kYzThreads]
   const DirView<P> &V;
   int lc;
   bool prefetch;     // false on the last cell of the march
   CHQ_D void operator()(int n, P q5[5]) const {
-    P *w = col + n * (2 * RE + 1) * 128;
+    P *w = col + n * (2 * RE + 1) * kYzThreads;
 #pragma unroll
-    for (int m = 0; m <= 2 * RE; ++m) q5[2 - RE + m] = w[m * 128];
+    for (int m = 0; m <= 2 * RE; ++m) q5[2 - RE + m] = w[m * kYzThreads];
 #pragma unroll
-    for (int m = 0; m < 2 * RE; ++m) w[m * 128] = q5[3 - RE + m];
-    if (prefetch) cp_async_elem(w + 2 * RE * 128, V.src[n] + lc + (RE + 1) * V.st);
+    for (int m = 0; m < 2 * RE; ++m) w[m * kYzThreads] = q5[3 - RE + m];
+    if (prefetch) cp_async_elem(w + 2 * RE * kYzThreads, V.src[n] + lc + (RE + 1) * V.st);
   }
 };
 
@@ -330,7 +336,7 @@ CHQ_D void sweep_x(const FluxArgs<P> &A, int wid) {
 // asynchronous copy per quantity and cell, issued a whole cell ahead, instead of 2RE+1
 // cached loads whose lines a y/z march cannot keep in L1.
 template <int R, int S, bool CHAR, bool WIN, class P>
-CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128], P *win) {
+CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   const int lane = threadIdx.x & 31;
   const int nseg = A.nseg[d];
   const int nchunk = A.nchunk;
@@ -359,10 +365,10 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128], P *win
     // window of cell f0-1: q[c-RE .. c+RE-1] now, q[c+RE] asynchronously
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
-      P *w = col + n * (2 * RE + 1) * 128;
+      P *w = col + n * (2 * RE + 1) * kYzThreads;
 #pragma unroll
-      for (int m = 0; m < 2 * RE; ++m) w[m * 128] = ldg(V.src[n] + lc + (m - RE) * V.st);
-      cp_async_elem(w + 2 * RE * 128, V.src[n] + lc + RE * V.st);
+      for (int m = 0; m < 2 * RE; ++m) w[m * kYzThreads] = ldg(V.src[n] + lc + (m - RE) * V.st);
+      cp_async_elem(w + 2 * RE * kYzThreads, V.src[n] + lc + RE * V.st);
     }
     cp_async_commit();
   }
@@ -376,10 +382,10 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P (*park)[128], P *win
       cell_states<R, CHAR, P>(A, V, lc, aL, aR);
     }
 #pragma unroll
-    for (int n = 0; n < 8; ++n) park[n][t] = aR[n];
+    for (int n = 0; n < 8; ++n) park[n * kYzThreads + t] = aR[n];
     if (f >= f0) face_flux<S, P>(A, V, lc, wl, aL);
 #pragma unroll
-    for (int n = 0; n < 8; ++n) wl[n] = park[n][t];
+    for (int n = 0; n < 8; ++n) wl[n] = park[n * kYzThreads + t];
   }
 }
 
@@ -406,7 +412,7 @@ template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) ==
 template <class P> struct FluxYzMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUXYZ_MINB_D : CHQ_FLUXYZ_MINB_F; };
 
 template <int R, class P> __host__ __device__ constexpr size_t flux_yz_smem() {
-  return (size_t)(8 + ((Reach<R>::v > 0) ? 8 * (2 * Reach<R>::v + 1) : 0)) * 128 * sizeof(P);
+  return (size_t)(8 + ((Reach<R>::v > 0) ? 8 * (2 * Reach<R>::v + 1) : 0)) * kYzThreads * sizeof(P);
 }
 
 template <int R, int S, bool CHAR, class P>
@@ -417,12 +423,12 @@ __global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_x_kernel(const 
 }
 
 template <int R, int S, bool CHAR, class P>
-__global__ void __launch_bounds__(128, FluxYzMinBlocks<P>::v) flux_yz_kernel(const FluxArgs<P> A) {
+__global__ void __launch_bounds__(kYzThreads, FluxYzMinBlocks<P>::v) flux_yz_kernel(const FluxArgs<P> A) {
   extern __shared__ __align__(16) unsigned char flux_dsm[];
-  P (*park)[128] = reinterpret_cast<P (*)[128]>(flux_dsm);
-  P *win = reinterpret_cast<P *>(flux_dsm) + 8 * 128;
+  P *park = reinterpret_cast<P *>(flux_dsm);
+  P *win = park + 8 * kYzThreads;
   if (A.skip && *A.skip) return;
-  const int wid = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
+  const int wid = (int)blockIdx.x * (kYzThreads / 32) + (int)(threadIdx.x >> 5);
   const int nz = (int)A.nwarp[2], nyz = (int)(A.nwarp[2] + A.nwarp[1]);
   if (wid < nz) sweep_yz<R, S, CHAR, true, P>(A, 2, wid, park, win);
   else if (wid < nyz) sweep_yz<R, S, CHAR, true, P>(A, 1, wid - nz, park, win);
@@ -445,14 +451,14 @@ template <int R, class P> __host__ __device__ constexpr size_t flux_yz_batched_s
 }
 
 template <int R, int S, bool CHAR, class P>
-__global__ void __launch_bounds__(128, FluxYzMinBlocks<P>::v) flux_yz_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
+__global__ void __launch_bounds__(kYzThreads, FluxYzMinBlocks<P>::v) flux_yz_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
   extern __shared__ __align__(16) unsigned char flux_dsm[];
-  P (*park)[128] = reinterpret_cast<P (*)[128]>(flux_dsm);
-  P *win = reinterpret_cast<P *>(flux_dsm) + 8 * 128;
+  P *park = reinterpret_cast<P *>(flux_dsm);
+  P *win = park + 8 * kYzThreads;
   const int j = batch_job(slots, n, blockIdx.x);
   const FluxArgs<P> &A = stage_args(args, j, flux_dsm + flux_yz_smem<R, P>());
   if (A.skip && *A.skip) return;
-  const int wid = (int)(blockIdx.x - slots[j].off) * 4 + (int)(threadIdx.x >> 5);
+  const int wid = (int)(blockIdx.x - slots[j].off) * (kYzThreads / 32) + (int)(threadIdx.x >> 5);
   const int nz = (int)A.nwarp[2], nyz = (int)(A.nwarp[2] + A.nwarp[1]);
   if (wid < nz) sweep_yz<R, S, CHAR, true, P>(A, 2, wid, park, win);
   else if (wid < nyz) sweep_yz<R, S, CHAR, true, P>(A, 1, wid - nz, park, win);

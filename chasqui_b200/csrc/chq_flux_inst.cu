@@ -27,13 +27,14 @@ static cudaError_t allow_smem(K kern, size_t smem, bool *ready) {
 // y/z sweeps (shared marching window, dynamic shared memory) then the x-sweep, one stream
 template <int S, bool C>
 static cudaError_t go(const FluxArgs<CHQ_P> &a, unsigned, cudaStream_t s) {
-  const unsigned nyz = (unsigned)((a.nwarp[1] + a.nwarp[2] + 3) / 4), nx = (unsigned)((a.nwarp[0] + 3) / 4);
+  constexpr int wpb = kYzThreads / 32;
+  const unsigned nyz = (unsigned)((a.nwarp[1] + a.nwarp[2] + wpb - 1) / wpb), nx = (unsigned)((a.nwarp[0] + 3) / 4);
   if (nyz) {
     constexpr size_t smem = flux_yz_smem<CHQ_R, CHQ_P>();
     static bool ready[64] = {};
     const cudaError_t ea = allow_smem(flux_yz_kernel<CHQ_R, S, C, CHQ_P>, smem, ready);
     if (ea != cudaSuccess) return ea;
-    flux_yz_kernel<CHQ_R, S, C, CHQ_P><<<nyz, 128, smem, s>>>(a);
+    flux_yz_kernel<CHQ_R, S, C, CHQ_P><<<nyz, kYzThreads, smem, s>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -62,7 +63,7 @@ static cudaError_t gob(const FluxArgs<CHQ_P> *a, const BatchSlot *sx, const Batc
     static bool ready[64] = {};
     const cudaError_t e = allow_smem(flux_yz_batched<CHQ_R, S, C, CHQ_P>, smem, ready);
     if (e != cudaSuccess) return e;
-    flux_yz_batched<CHQ_R, S, C, CHQ_P><<<nbyz, 128, smem, s>>>(a, syz, n);
+    flux_yz_batched<CHQ_R, S, C, CHQ_P><<<nbyz, kYzThreads, smem, s>>>(a, syz, n);
     const cudaError_t e2 = cudaGetLastError();
     if (e2 != cudaSuccess) return e2;
   }

@@ -1035,7 +1035,7 @@ int batch_build(chq_batch *B) {
   }, B->k_flux.nblocks);
   const size_t o_flux_yz_s = slots_of(h, J, [](chq_mesh *m) {
     const FluxArgs<P> a = flux_args<P>(m, 0, 7u);
-    return linear((a.nwarp[1] + a.nwarp[2]) * 32, 128);
+    return linear((a.nwarp[1] + a.nwarp[2]) * 32, kYzThreads);
   }, B->k_flux_yz.nblocks);
   o_corner_s = slots_of(h, J, [](chq_mesh *m) { return corner_grid(m); }, B->k_corner.nblocks);
   o_update_s = slots_of(h, J, [](chq_mesh *m) { return update_grid(m); }, B->k_update.nblocks);
@@ -1851,6 +1851,7 @@ int chq_batch_status(chq_batch *B, double *t, int *cycle, int *done) {
 }
 
 long long chq_batch_kernel_launches(const chq_batch *B) { return B ? B->nlaunch : 0; }
+
 
 void *chq_batch_stream(chq_batch *B) { return B ? (void *)B->stream : nullptr; }
 

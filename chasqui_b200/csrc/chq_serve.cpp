@@ -6,9 +6,12 @@
 //      sums are kept, their device memory is freed),
 //   2. admits queued jobs in submission order while they fit the HBM budget and the slot
 //      limit (a job that does not fit does not block smaller ones behind it),
-//   3. rebuilds the batch of every class whose membership changed, and
-//   4. launches `cycles_per_step` batched cycles of every class, each class on its own
-//      stream (replayed as a CUDA graph), so classes run concurrently on the device.
+//   3. rebuilds the batch of every lane whose membership changed, and
+//   4. launches `cycles_per_step` batched cycles of every lane. A class (jobs that share a
+//      kernel instantiation) is spread over up to `lanes` batches, a new job joining the lane
+//      with the fewest cells; each lane has its own stream and replays a CUDA graph, so the
+//      flux kernel of one lane overlaps the memory-bound kernels of another. Batching alone
+//      serialises every job through the same kernel sequence.
 // Each job keeps its own dt and clock on the device, so its result is the same alone and in
 // any mix. Times are seconds on the server's steady clock.
 #include <chrono>
@@ -41,16 +44,19 @@ struct Job {
   double hist[10] = {};
 };
 
-using ClassKey = std::tuple<int, int, int, int, int, int, int>;
+// (precision, reconstruction, Riemann solver, characteristic, integrator, FOFC, limiter, lane)
+using ClassKey = std::tuple<int, int, int, int, int, int, int, int>;
 
-ClassKey key_of(const chq_config &c) {
-  return ClassKey{c.precision, c.recon, c.rsolver, c.characteristic, c.integrator, c.fofc, c.flux_limiter};
+ClassKey key_of(const chq_config &c, int lane) {
+  return ClassKey{c.precision, c.recon, c.rsolver, c.characteristic, c.integrator, c.fofc, c.flux_limiter, lane};
 }
 
 struct Group {
   std::vector<Job *> members;
   chq_batch *batch = nullptr;
   bool dirty = false;
+  long long cells = 0;
+  std::vector<chq_mesh *> retired;   // finished members' meshes, freed after their batch is dropped
 };
 
 int err(int code, const std::string &m) {
@@ -62,7 +68,7 @@ int err(int code, const std::string &m) {
 
 struct chq_server {
   long long budget = 0, used = 0;
-  int max_active = 0, cycles_per_step = 1;
+  int max_active = 0, cycles_per_step = 1, lanes = 8;
   long long next_id = 1;
   std::map<long long, Job *> jobs;
   std::vector<Job *> queue;
@@ -98,16 +104,25 @@ int retire_finished(chq_server *S) {
       if (rc) return rc;
       bool finite = true;
       for (double v : j->hist) finite = finite && (v == v) && (v - v == 0.0);
-      chq_mesh_destroy(j->mesh);
+      g.retired.push_back(j->mesh);   // freed below, after the batch that lists it
       j->mesh = nullptr;
       S->used -= j->bytes;
       // a state that went non-finite is quarantined: its neighbours in the batch never
       // read it (every kernel indexes its own job only)
       j->state = finite ? CHQ_JOB_DONE : CHQ_JOB_FAILED;
       j->t_done = now;
+      g.cells -= j->cells;
       g.dirty = true;
     }
     g.members.swap(keep);
+    if (!g.retired.empty()) {
+      // the batch lists the finished meshes: drop it (the rebuild makes a new one) before
+      // their memory is freed
+      if (g.batch) chq_batch_destroy(g.batch);
+      g.batch = nullptr;
+      for (chq_mesh *m : g.retired) chq_mesh_destroy(m);
+      g.retired.clear();
+    }
   }
   return CHQ_OK;
 }
@@ -137,8 +152,19 @@ void admit(chq_server *S) {
     S->used += j->bytes;
     j->state = CHQ_JOB_RUNNING;
     j->t_start = S->now();
-    Group &g = S->groups[key_of(j->cfg)];
+    int lane = 0;
+    long long least = -1;
+    for (int q = 0; q < S->lanes; ++q) {
+      const auto it = S->groups.find(key_of(j->cfg, q));
+      const long long c = (it == S->groups.end()) ? 0 : it->second.cells;
+      if (least < 0 || c < least) {
+        least = c;
+        lane = q;
+      }
+    }
+    Group &g = S->groups[key_of(j->cfg, lane)];
     g.members.push_back(j);
+    g.cells += j->cells;
     g.dirty = true;
     ++active;
   }
@@ -153,6 +179,8 @@ int rebuild(chq_server *S) {
       chq_batch_destroy(g.batch);
       g.batch = nullptr;
     }
+    for (chq_mesh *m : g.retired) chq_mesh_destroy(m);
+    g.retired.clear();
     g.dirty = false;
     if (g.members.empty()) continue;
     std::vector<chq_mesh *> ms;
@@ -256,10 +284,18 @@ int chq_server_stats(chq_server *S, long long *used_bytes, int *active, int *que
   return CHQ_OK;
 }
 
+int chq_server_set_lanes(chq_server *S, int lanes) {
+  if (!S || lanes < 1 || lanes > 64) return err(CHQ_ERR_ARG, "lanes must be in [1, 64]");
+  S->lanes = lanes;
+  return CHQ_OK;
+}
+
 int chq_server_destroy(chq_server *S) {
   if (!S) return CHQ_OK;
-  for (auto &kv : S->groups)
+  for (auto &kv : S->groups) {
     if (kv.second.batch) chq_batch_destroy(kv.second.batch);
+    for (chq_mesh *m : kv.second.retired) chq_mesh_destroy(m);
+  }
   for (auto &kv : S->jobs) {
     if (kv.second->mesh) chq_mesh_destroy(kv.second->mesh);
     delete kv.second;

@@ -207,10 +207,11 @@ CHQ_API void *chq_batch_stream(chq_batch *b);
  * its parameters. chq_server_step() retires finished jobs (keeping their history sums and
  * freeing their memory), admits queued jobs in submission order while they fit the HBM
  * budget and the slot limit, rebuilds the batch of every class whose membership changed and
- * launches cycles_per_step batched cycles of every class, each class on its own stream as a
- * replayed CUDA graph. A job whose final state is not finite is reported FAILED; kernels
- * index only their own job, so it never disturbs the others. Times are seconds on the
- * server clock. */
+ * launches cycles_per_step batched cycles of every class. Each class is split into up to
+ * `lanes` batches (default 8) of balanced cell counts, each on its own stream as a replayed
+ * CUDA graph, so that the memory-bound kernels of one lane overlap the flux kernel of another.
+ * A job whose final state is not finite is reported FAILED; kernels index only their own
+ * job, so it never disturbs the others. Times are seconds on the server clock. */
 enum { CHQ_JOB_QUEUED = 0, CHQ_JOB_RUNNING = 1, CHQ_JOB_DONE = 2, CHQ_JOB_FAILED = 3 };
 typedef struct chq_job_status {
   int state, cycle;
@@ -230,6 +231,8 @@ CHQ_API chq_mesh *chq_server_job_mesh(chq_server *s, long long job_id);
 CHQ_API int chq_server_stats(chq_server *s, long long *used_bytes, int *active, int *queued, long long *zone_updates,
                              double *clock);
 CHQ_API int chq_server_destroy(chq_server *s);
+/* concurrent batches (streams) per class, 1..64; takes effect for newly admitted jobs */
+CHQ_API int chq_server_set_lanes(chq_server *s, int lanes);
 
 /* ---- history sums without any device allocation --------------------------------------------
  * No counterpart in the reference. For callers that cannot allocate device memory: an
