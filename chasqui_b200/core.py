@@ -39,6 +39,10 @@ class chq_config(C.Structure):
         ("fofc", C.c_int), ("flux_limiter", C.c_int),
         ("nu", C.c_double), ("kappa", C.c_double), ("eta", C.c_double), ("sts", C.c_int),
         ("precision", C.c_int), ("tlim", C.c_double), ("nlim", C.c_int),
+        ("gravity_uniform", C.c_int), ("gravity_point", C.c_int),
+        ("g1", C.c_double), ("g2", C.c_double), ("g3", C.c_double), ("gm", C.c_double),
+        ("gx0", C.c_double), ("gy0", C.c_double), ("gz0", C.c_double), ("rsoft", C.c_double),
+        ("cooling", C.c_int), ("lambda0", C.c_double), ("cool_alpha", C.c_double), ("tfloor", C.c_double),
     ]
 
 
@@ -57,6 +61,8 @@ SIGNATURES = [
     ("chq_array_size", C.c_long, [_P, C.c_char_p]),
     ("chq_upload", C.c_int, [_P, C.c_char_p, _D, C.c_long, _P]),
     ("chq_download", C.c_int, [_P, C.c_char_p, _D, C.c_long, _P]),
+    ("chq_snapshot", C.c_int, [_P, C.c_int, C.POINTER(C.c_char_p), C.POINTER(_D), C.POINTER(C.c_long)]),
+    ("chq_snapshot_wait", C.c_int, [_P]),
     ("chq_fluxes", C.c_int, [_P, C.c_int, C.c_int, _P]),
     ("chq_fluxes_all", C.c_int, [_P, C.c_int, _P]),
     ("chq_corner_emf", C.c_int, [_P, _P]),
@@ -209,6 +215,23 @@ class Mesh:
         return (nc, self.nk + 1, self.nj + 1, self.ni + 1)
 
     # ---- transfer ----
+    def snapshot(self, names) -> dict:
+        """Start a non-stalling output snapshot of `names` (chq_snapshot) into new page-locked
+        host arrays and return them; they are valid after snapshot_wait()."""
+        pins = {n: PinnedArray(self.shape(n)) for n in names}
+        keys = (C.c_char_p * len(names))(*[n.encode() for n in names])
+        ptrs = (_D * len(names))(*[_dptr(pins[n].array) for n in names])
+        sizes = (C.c_long * len(names))(*[pins[n].array.size for n in names])
+        _check(load_library().chq_snapshot(self._h, len(names), keys, ptrs, sizes))
+        self._snap = pins   # keep the buffers alive while the copy is in flight
+        return pins
+
+    def snapshot_wait(self) -> dict:
+        _check(load_library().chq_snapshot_wait(self._h))
+        pins = getattr(self, "_snap", {})
+        self._snap = {}
+        return {n: (p.array if p.array.shape[0] > 1 else p.array[0]) for n, p in pins.items()}
+
     def get(self, name: str) -> np.ndarray:
         shp = self.shape(name)
         out = np.empty(shp, dtype=np.float64)

@@ -99,8 +99,16 @@ template <class P> __global__ void __launch_bounds__(256) corner_emf_kernel(cons
 // is an active cell and the x1/x2/x3 face updates when it is an active face. The reads of
 // ua/ub/b?a/b?b precede this thread's writes to the same elements and no other thread
 // touches them, so the RK aliasing of out with a or b is safe.
+// gravity source of the update epilogue (src/srcterms.hpp:10-41)
+struct GravityP {
+  int on, point;
+  double g1, g2, g3, gm, x0, y0, z0, rsoft;
+};
+
 template <class P> struct UpdateArgs {
   Geom g;
+  GravityP grav;
+  const P *w;                // stage primitives (gravity only)
   EOSp eos;
   const P *f1, *f2, *f3, *e1, *e2, *e3;
   const double *ua, *ub;
@@ -158,6 +166,26 @@ template <class P> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by
       if (g.three_d) divf += ((double)ldg(A.f3 + ln + g.sk) - (double)ldg(A.f3 + ln)) * A.idx3;
       un[n] = g0 * A.ua[ln] + g1 * A.ub[ln] - bdt * divf;
     }
+    if (A.grav.on) {
+      // ApplyGravity on the updated state with the stage primitives and beta*dt
+      const GravityP &gr = A.grav;
+      double a1 = gr.g1, a2 = gr.g2, a3 = gr.g3;
+      if (gr.point) {
+        const double dx = (g.x1min + (i - g.is + 0.5) * g.dx1) - gr.x0;
+        const double dy = g.two_d ? (g.x2min + (j - g.js + 0.5) * g.dx2) - gr.y0 : 0.0;
+        const double dz = g.three_d ? (g.x3min + (k - g.ks + 0.5) * g.dx3) - gr.z0 : 0.0;
+        const double r2 = dx * dx + dy * dy + dz * dz + gr.rsoft * gr.rsoft;
+        const double f = -gr.gm / (r2 * sqrt(r2));
+        a1 += f * dx;
+        a2 += f * dy;
+        a3 += f * dz;
+      }
+      const double d = (double)A.w[IDN * vs + l];
+      un[IM1] += bdt * d * a1;
+      un[IM2] += bdt * d * a2;
+      un[IM3] += bdt * d * a3;
+      un[IEN] += bdt * d * ((double)A.w[IVX * vs + l] * a1 + (double)A.w[IVY * vs + l] * a2 + (double)A.w[IVZ * vs + l] * a3);
+    }
   }
   double nb1 = 0, nb2 = 0, nb3 = 0;
   if (j <= g.je && k <= g.ke) nb1 = new_b1(A, l, g0, g1, bdt);
@@ -179,6 +207,43 @@ template <class P> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by
 }
 
 template <class P> __global__ void __launch_bounds__(256) update_kernel(const UpdateArgs<P> A) { update_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+
+// ---------------------------------------------------------------------------------------
+// Optically thin cooling after the step (src/srcterms.hpp:43-71): dT/dt = -(gamma-1) rho
+// lambda0 T^alpha integrated exactly over this cycle's dt (read from the step control) with
+// the primitives of the step's end state, applied to the conserved energy of active cells.
+template <class P> struct CoolArgs {
+  Geom g;
+  double gm1, lambda0, alpha, tfloor;
+  double *u;
+  const P *w;
+  const double *dt;
+  const int *done;
+};
+
+template <class P> __global__ void __launch_bounds__(256) cooling_kernel(const CoolArgs<P> A) {
+  if (A.done && *A.done) return;
+  const Geom &g = A.g;
+  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = g.ks + blockIdx.z;
+  if (i > g.ie || j > g.je || k > g.ke) return;
+  const long vs = g.vstride, l = g.idx(k, j, i);
+  const double dt = *A.dt;
+  const double d = (double)A.w[IDN * vs + l], p = (double)A.w[IPR * vs + l];
+  const double t0 = p / d;
+  const double cc = A.gm1 * d * A.lambda0;
+  double t1;
+  if (fabs(A.alpha - 1.0) < 1e-12) {
+    t1 = t0 * exp(-cc * dt);
+  } else {
+    const double e = 1.0 - A.alpha;
+    const double base = pow(t0, e) + (A.alpha - 1.0) * cc * dt;
+    t1 = (base > 0.0) ? pow(base, 1.0 / e) : A.tfloor;
+  }
+  t1 = fmax(t1, A.tfloor);
+  A.u[IEN * vs + l] += d * (t1 - t0) / A.gm1;
+}
 
 // ---------------------------------------------------------------------------------------
 // FOFC flag of the tentative state (src/fofc.hpp:17-43): rho <= dfloor or p <= pfloor,

@@ -196,6 +196,22 @@ struct chq_mesh {
   // set while the mesh is a member of a batch: the batch's end-of-cycles event, which every
   // operation on the mesh's own stream waits for (not owned by the mesh)
   cudaEvent_t batch_evt = nullptr;
+  // output snapshot (chq_snapshot): device copy area, its stream and events, pending items
+  struct SnapItem {
+    double *host;
+    long n;
+    int ncomp, face;
+    size_t es;
+    int isint;
+    char *copy;
+    std::vector<unsigned char> tmp;   // host staging when the device element is not double
+  };
+  char *snap = nullptr;
+  size_t snap_bytes = 0;
+  cudaStream_t snap_stream = nullptr;
+  cudaEvent_t snap_taken = nullptr, snap_landed = nullptr;
+  std::vector<SnapItem> snap_items;
+  bool snap_pending = false;
   // timing
   cudaEvent_t slots[8] = {};
   bool prof = false;
@@ -402,6 +418,11 @@ UpdateArgs<P> update_args(chq_mesh *m, int out, double g0, double g1, double bdt
   a.idx1 = 1.0 / g.dx1; a.idx2 = 1.0 / g.dx2; a.idx3 = 1.0 / g.dx3;
   a.done = done;
   a.need = need;
+  const chq_config &c = m->cfg;
+  a.grav = GravityP{(c.gravity_uniform || c.gravity_point) ? 1 : 0, c.gravity_point ? 1 : 0,
+                    c.gravity_uniform ? c.g1 : 0.0, c.gravity_uniform ? c.g2 : 0.0, c.gravity_uniform ? c.g3 : 0.0,
+                    c.gm, c.gx0, c.gy0, c.gz0, c.rsoft};
+  a.w = as<P>(m->w);
   return a;
 }
 
@@ -676,6 +697,27 @@ int do_res_emf(chq_mesh *m, const double *b1, const double *b2, const double *b3
   const dim3 grid((unsigned)((g.ie + 2 - g.is + 31) / 32), (unsigned)((a.ju - g.js + 1 + 7) / 8), (unsigned)(a.ku - g.ks + 1));
   m->nlaunch += 1;
   resistive_emf_kernel<P><<<grid, dim3(32, 8), 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+// cooling of the step's end state u0 over this cycle's dt (srcterms::ApplyCooling)
+template <class P>
+int do_cooling(chq_mesh *m, const int *done, cudaStream_t s) {
+  const Geom &g = m->g;
+  CoolArgs<P> a{};
+  a.g = g;
+  a.gm1 = m->cfg.gamma - 1.0;
+  a.lambda0 = m->cfg.lambda0;
+  a.alpha = m->cfg.cool_alpha;
+  a.tfloor = m->cfg.tfloor;
+  a.u = m->u[0];
+  a.w = as<P>(m->w);
+  a.dt = &m->ctl->dt;
+  a.done = done;
+  const dim3 grid((unsigned)((g.nx1 + 31) / 32), (unsigned)((g.je - g.js + 1 + 7) / 8), (unsigned)(g.ke - g.ks + 1));
+  m->nlaunch += 1;
+  cooling_kernel<P><<<grid, dim3(32, 8), 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
@@ -1233,6 +1275,7 @@ void chq_config_defaults(chq_config *c) {
   c->precision = CHQ_FP64;
   c->tlim = 1.0;
   c->nlim = -1;
+  c->cool_alpha = 1.0;
 }
 
 int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
@@ -1381,6 +1424,13 @@ int chq_mesh_destroy(chq_mesh *m) {
   if (!m) return CHQ_OK;
   if (m->batch_evt) cudaEventSynchronize(m->batch_evt);
   if (m->stream) cudaStreamSynchronize(m->stream);
+  if (m->snap_stream) {
+    cudaStreamSynchronize(m->snap_stream);
+    cudaStreamDestroy(m->snap_stream);
+  }
+  if (m->snap_taken) cudaEventDestroy(m->snap_taken);
+  if (m->snap_landed) cudaEventDestroy(m->snap_landed);
+  if (m->snap) cudaFree(m->snap);
   for (auto &p : m->pending) { m->pool.push_back(p.b); m->pool.push_back(p.e); }
   for (cudaEvent_t e : m->pool) cudaEventDestroy(e);
   for (cudaEvent_t e : m->slots) if (e) cudaEventDestroy(e);
@@ -1466,6 +1516,80 @@ int chq_upload(chq_mesh *m, const char *name, const double *host, long n, void *
 int chq_download(chq_mesh *m, const char *name, double *host, long n, void *stream) {
   if (!m || !name || !host) return fail(CHQ_ERR_ARG, "null argument");
   return transfer(m, name, host, n, false, S(m, stream));
+}
+
+int chq_snapshot_wait(chq_mesh *m) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  if (!m->snap_pending) return CHQ_OK;
+  m->snap_pending = false;
+  CHQ_CUDA(cudaEventSynchronize(m->snap_landed));
+  for (auto &it : m->snap_items) {
+    if (it.tmp.empty()) continue;
+    for (long q = 0; q < it.n; ++q)
+      it.host[q] = it.isint ? (double)reinterpret_cast<int *>(it.tmp.data())[q]
+                            : (double)reinterpret_cast<float *>(it.tmp.data())[q];
+  }
+  m->snap_items.clear();
+  return CHQ_OK;
+}
+
+int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *const *host, const long *n) {
+  if (!m || nfields < 1 || !names || !host || !n) return fail(CHQ_ERR_ARG, "bad argument");
+  int rc = chq_snapshot_wait(m);
+  if (rc) return rc;
+  const Geom &g = m->g;
+  std::vector<FieldRef> fr(nfields);
+  size_t need = 0;
+  for (int q = 0; q < nfields; ++q) {
+    if (!names[q] || !host[q] || !field_by_name(m, names[q], fr[q]))
+      return fail(CHQ_ERR_ARG, std::string("unknown field: ") + (names[q] ? names[q] : "(null)"));
+    if (field_size(m, fr[q]) != n[q]) return fail(CHQ_ERR_ARG, std::string("size mismatch for field ") + names[q]);
+    need += align_up((size_t)fr[q].ncomp * g.vstride * field_esize(m, fr[q]), 256);
+  }
+  if (!m->snap_stream) {
+    CHQ_CUDA(cudaStreamCreateWithFlags(&m->snap_stream, cudaStreamNonBlocking));
+    CHQ_CUDA(cudaEventCreateWithFlags(&m->snap_taken, cudaEventDisableTiming));
+    CHQ_CUDA(cudaEventCreateWithFlags(&m->snap_landed, cudaEventDisableTiming));
+  }
+  if (need > m->snap_bytes) {
+    if (m->snap) CHQ_CUDA(cudaFree(m->snap));
+    m->snap = nullptr;
+    m->snap_bytes = 0;
+    const cudaError_t e = cudaMalloc(&m->snap, need);
+    if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("snapshot area: ") + cudaGetErrorString(e));
+    m->snap_bytes = need;
+  }
+  cudaStream_t s = S(m, nullptr);
+  char *p = m->snap;
+  m->snap_items.clear();
+  for (int q = 0; q < nfields; ++q) {
+    const FieldRef &f = fr[q];
+    const size_t es = field_esize(m, f), bytes = (size_t)f.ncomp * g.vstride * es;
+    CHQ_CUDA(cudaMemcpyAsync(p, f.base, bytes, cudaMemcpyDeviceToDevice, s));
+    chq_mesh::SnapItem it{host[q], n[q], f.ncomp, f.face, es, f.isint, p, {}};
+    if (es != sizeof(double) || f.isint) it.tmp.resize((size_t)n[q] * es);
+    m->snap_items.push_back(std::move(it));
+    p += align_up(bytes, 256);
+  }
+  CHQ_CUDA(cudaEventRecord(m->snap_taken, s));
+  CHQ_CUDA(cudaStreamWaitEvent(m->snap_stream, m->snap_taken, 0));
+  for (auto &it : m->snap_items) {
+    const int nx = it.face ? g.ni + 1 : g.ni, ny = it.face ? g.nj + 1 : g.nj, nz = it.face ? g.nk + 1 : g.nk;
+    void *hbase = it.tmp.empty() ? (void *)it.host : (void *)it.tmp.data();
+    for (int c = 0; c < it.ncomp; ++c) {
+      cudaMemcpy3DParms cp{};
+      char *dev = it.copy + (size_t)c * g.vstride * it.es;
+      char *hst = static_cast<char *>(hbase) + (size_t)c * nx * ny * nz * it.es;
+      cp.srcPtr = make_cudaPitchedPtr(dev, (size_t)g.sj * it.es, (size_t)nx * it.es, (size_t)(g.nj + 1));
+      cp.dstPtr = make_cudaPitchedPtr(hst, (size_t)nx * it.es, (size_t)nx * it.es, (size_t)ny);
+      cp.extent = make_cudaExtent((size_t)nx * it.es, (size_t)ny, (size_t)nz);
+      cp.kind = cudaMemcpyDeviceToHost;
+      CHQ_CUDA(cudaMemcpy3DAsync(&cp, m->snap_stream));
+    }
+  }
+  CHQ_CUDA(cudaEventRecord(m->snap_landed, m->snap_stream));
+  m->snap_pending = true;
+  return CHQ_OK;
 }
 
 int chq_fluxes(chq_mesh *m, int dir, int cur, void *stream) {
@@ -1574,6 +1698,10 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
   cudaStream_t s = S(m, stream);
   const int *done = &m->ctl->done;
   const bool sts = m->cfg.sts && m->diff;
+  const bool cool = m->cfg.cooling != 0;
+  // operator-split pieces after the hyperbolic step (src/main.cpp:272-290): RKL2 and
+  // cooling; with either, the last stage's con2prim takes no dt and a final one does
+  const bool split = sts || cool;
   for (int c = 0; c < n; ++c) {
     {
       Prof p(m, PK_CTL, s);
@@ -1581,27 +1709,26 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
       m->nlaunch += 1;
     }
     CHQ_CUDA(cudaGetLastError());
+    int rc;
     for (int st = 1; st <= m->nstage; ++st) {
       double g0, g1, beta;
       int cur, out;
       stage_table(m->nstage, st, g0, g1, beta, cur, out);
-      int rc = run_stage(m, cur, out, g0, g1, 0.0, &m->ctl->beta_dt[st - 1], done, s);
+      rc = run_stage(m, cur, out, g0, g1, 0.0, &m->ctl->beta_dt[st - 1], done, s);
       if (rc) return rc;
       const bool last = (st == m->nstage);
       {
         Prof p(m, PK_C2P, s);
-        // with RKL2 the last stage's con2prim takes no dt: the split step comes first
-        rc = DISPATCH_P(m, do_c2p)(m, out, (last && !sts) ? 1 : 0, &m->ctl->mdt_bits, m->ctl, done, s);
+        rc = DISPATCH_P(m, do_c2p)(m, out, (last && !split) ? 1 : 0, &m->ctl->mdt_bits, m->ctl, done, s);
       }
       if (rc) return rc;
-      if (last && m->diff) {
+      if (last && m->diff && (!split || sts)) {
         Prof p(m, PK_DIFF, s);
         if ((rc = DISPATCH_P(m, do_rho_min)(m, done, s))) return rc;
       }
     }
     if (sts) {
-      // operator-split RKL2 over this cycle's dt (src/main.cpp:282-290): the stage count is
-      // a host decision, so the host reads dt and the density minimum here
+      // the RKL2 stage count is a host decision: read dt and the density minimum here
       StepCtl h;
       CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
       CHQ_CUDA(cudaStreamSynchronize(s));
@@ -1609,7 +1736,7 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
       double rho_min;
       std::memcpy(&rho_min, &h.rho_bits, sizeof(rho_min));
       const double dt_par = host_parabolic_dt(m, rho_min);
-      int nst = 0, rc;
+      int nst = 0;
       {
         Prof p(m, PK_STS, s);
         rc = DISPATCH_P(m, sts_advance)(m, h.dt, dt_par, s, nst);
@@ -1617,9 +1744,21 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
       }
       if (rc) return rc;
       m->sts_stages += nst;
+    }
+    if (cool) {
+      Prof p(m, PK_C2P, s);
+      if ((rc = DISPATCH_P(m, do_c2p)(m, 0, 0, &m->ctl->mdt_bits, m->ctl, done, s))) return rc;
+      if ((rc = DISPATCH_P(m, do_cooling)(m, done, s))) return rc;
+      if ((rc = do_bc(m, 0, done, s))) return rc;
+    }
+    if (split) {
       {
         Prof p(m, PK_C2P, s);
         if ((rc = DISPATCH_P(m, do_c2p)(m, 0, 1, &m->ctl->mdt_bits, m->ctl, done, s))) return rc;
+      }
+      if (m->diff && !sts) {
+        Prof p(m, PK_DIFF, s);
+        if ((rc = DISPATCH_P(m, do_rho_min)(m, done, s))) return rc;
       }
     }
     {
@@ -1744,8 +1883,10 @@ int chq_event_elapsed(chq_mesh *m, int a, int b, float *ms) {
 int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   if (!meshes || n < 1 || !out) return fail(CHQ_ERR_ARG, "bad argument");
   for (int q = 0; q < n; ++q)
-    if (meshes[q] && meshes[q]->diff)
-      return fail(CHQ_ERR_ARG, "batched stepping covers the ideal-MHD stage; step diffusive meshes one by one");
+    if (meshes[q] && (meshes[q]->diff || meshes[q]->cfg.cooling || meshes[q]->cfg.gravity_uniform ||
+                      meshes[q]->cfg.gravity_point))
+      return fail(CHQ_ERR_ARG, "batched stepping covers the ideal-MHD stage; step meshes with diffusion or "
+                               "source terms one by one");
   *out = nullptr;
   const chq_mesh *a = meshes[0];
   for (int j = 0; j < n; ++j) {

@@ -212,8 +212,9 @@ int chq_server_submit(chq_server *S, const chq_config *cfg, int problem, const d
   const long long bytes = chq_config_bytes(cfg);
   if (bytes <= 0) return err(CHQ_ERR_ARG, "invalid job configuration");
   if (bytes > S->budget) return err(CHQ_ERR_ARG, "job larger than the server's HBM budget");
-  if (cfg->nu > 0 || cfg->kappa > 0 || cfg->eta > 0)
-    return err(CHQ_ERR_ARG, "the server batches ideal-MHD jobs; run diffusive jobs on their own mesh");
+  if (cfg->nu > 0 || cfg->kappa > 0 || cfg->eta > 0 || cfg->cooling || cfg->gravity_uniform || cfg->gravity_point)
+    return err(CHQ_ERR_ARG, "the server batches ideal-MHD jobs; run jobs with diffusion or source terms on their "
+                            "own mesh");
   Job *j = new Job;
   j->id = S->next_id++;
   j->cfg = *cfg;

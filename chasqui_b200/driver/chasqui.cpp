@@ -7,8 +7,8 @@
 // the device through the C ABI (include/chq.h): whole cycles are queued with chq_cycles and
 // dt, the FOFC and limiter counts stay on the device. The host reads the clock once per
 // cycle only while outputs are scheduled, otherwise once per `time.ndiag` cycles (at most 256).
-// Gravity and cooling source terms (src/srcterms.hpp) are outside this path: enabling them
-// is an error. `mhd.precision = mixed` selects the mixed FP32/FP64 form. `--write-ic FILE`
+// Gravity and cooling source terms (src/srcterms.hpp) run on the device as well.
+// `mhd.precision = mixed` selects the mixed FP32/FP64 form. `--write-ic FILE`
 // writes the problem generator's initial state as a restart file and exits without a GPU.
 #include <algorithm>
 #include <chrono>
@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <iomanip>
 #include <iostream>
 #include <stdexcept>
@@ -103,10 +104,20 @@ int run(int argc, char **argv) {
   cfg.nu = pin.real("diffusion", "nu", 0.0);
   cfg.kappa = pin.real("diffusion", "kappa", 0.0);
   cfg.eta = pin.real("diffusion", "eta", 0.0);
-  const bool grav = pin.boolean("gravity", "uniform", false) || pin.boolean("gravity", "point_mass", false);
-  const bool cool = pin.boolean("cooling", "enabled", false);
-  if (grav || cool)
-    throw std::runtime_error("gravity and cooling source terms are not part of the device stage path");
+  cfg.gravity_uniform = pin.boolean("gravity", "uniform", false);
+  cfg.g1 = pin.real("gravity", "g1", 0.0);
+  cfg.g2 = pin.real("gravity", "g2", 0.0);
+  cfg.g3 = pin.real("gravity", "g3", 0.0);
+  cfg.gravity_point = pin.boolean("gravity", "point_mass", false);
+  cfg.gm = pin.real("gravity", "gm", 0.0);
+  cfg.gx0 = pin.real("gravity", "x0", 0.0);
+  cfg.gy0 = pin.real("gravity", "y0", 0.0);
+  cfg.gz0 = pin.real("gravity", "z0", 0.0);
+  cfg.rsoft = pin.real("gravity", "rsoft", 0.0);
+  cfg.cooling = pin.boolean("cooling", "enabled", false);
+  cfg.lambda0 = pin.real("cooling", "lambda0", 0.0);
+  cfg.cool_alpha = pin.real("cooling", "alpha", 1.0);
+  cfg.tfloor = pin.real("cooling", "tfloor", 0.0);
   const std::string prec = pin.str("mhd", "precision", "fp64");
   cfg.precision = (prec == "fp64") ? CHQ_FP64 : (prec == "mixed") ? CHQ_MIXED : -1;
   if (cfg.precision < 0) throw std::runtime_error("unknown precision: " + prec + " (fp64 or mixed)");
@@ -186,13 +197,72 @@ int run(int argc, char **argv) {
     hst.open(basename + ".hst", rstfile.empty() ? std::ios::out : std::ios::app);
     if (rstfile.empty()) hst << "# time dt mass mom1 mom2 mom3 etot ekin emag eint divB_max divB_L1\n";
   }
+  // VTK and restart dumps go through chq_snapshot: the state is copied on the device behind
+  // the queued work and downloaded while the next cycle runs; the files are written from the
+  // page-locked buffers once the copy has landed (flush), overlapping the device.
+  struct Pinned {
+    double *p = nullptr;
+    long n = 0;
+    ~Pinned() { if (p) chq_host_free(p); }
+  };
+  const char *snap_names[6] = {"w", "bcc", "u0", "b1f0", "b2f0", "b3f0"};
+  Pinned snap_buf[6];
+  std::vector<std::function<void()>> pending;
+  auto buf = [&](int q) -> Pinned & {
+    Pinned &b = snap_buf[q];
+    if (!b.p) {
+      b.n = chq_array_size(m, snap_names[q]);
+      void *p = nullptr;
+      check(chq_host_alloc(b.n * (long long)sizeof(double), &p), "host buffer");
+      b.p = static_cast<double *>(p);
+    }
+    return b;
+  };
+  auto as_vec = [](const Pinned &b) { return std::vector<double>(b.p, b.p + b.n); };
+  auto flush = [&]() {
+    if (pending.empty()) return;
+    check(chq_snapshot_wait(m), "snapshot");
+    for (auto &w : pending) w();
+    pending.clear();
+  };
   auto do_outputs = [&](double dt, bool force, bool final_dump) {
     const double eps = 1e-10 * (tlim > 0 ? tlim : 1.0);
-    if (dt_vtk > 0 && (t >= next_vtk - eps || force)) {
-      char fn[512];
-      std::snprintf(fn, sizeof(fn), "%s.%04d.vtk", basename.c_str(), nvtk++);
-      chqd::write_vtk(g, download(m, "w"), download(m, "bcc"), fn, t, cycle);
-      next_vtk += dt_vtk;
+    const bool vtk_now = dt_vtk > 0 && (t >= next_vtk - eps || force);
+    const bool rst_now = dt_rst > 0 && (t >= next_rst - eps || final_dump);
+    if (vtk_now || rst_now) {
+      flush();
+      std::vector<int> fields;
+      if (vtk_now) fields.insert(fields.end(), {0, 1});
+      if (rst_now) fields.insert(fields.end(), {2, 3, 4, 5});
+      std::vector<const char *> names;
+      std::vector<double *> ptrs;
+      std::vector<long> sizes;
+      for (int q : fields) {
+        Pinned &b = buf(q);
+        names.push_back(snap_names[q]);
+        ptrs.push_back(b.p);
+        sizes.push_back(b.n);
+      }
+      check(chq_snapshot(m, (int)fields.size(), names.data(), ptrs.data(), sizes.data()), "snapshot");
+      const double tw = t;
+      const int cw = cycle;
+      if (vtk_now) {
+        char fn[512];
+        std::snprintf(fn, sizeof(fn), "%s.%04d.vtk", basename.c_str(), nvtk++);
+        const std::string f = fn;
+        pending.push_back([&, f, tw, cw]() { chqd::write_vtk(g, as_vec(snap_buf[0]), as_vec(snap_buf[1]), f, tw, cw); });
+        next_vtk += dt_vtk;
+      }
+      if (rst_now) {
+        char fn[512];
+        std::snprintf(fn, sizeof(fn), "%s.%04d.rst", basename.c_str(), nrst++);
+        const std::string f = fn;
+        pending.push_back([&, f, tw, cw]() {
+          chqd::write_restart(g, f, tw, cw, as_vec(snap_buf[2]), as_vec(snap_buf[3]), as_vec(snap_buf[4]),
+                              as_vec(snap_buf[5]));
+        });
+        next_rst += dt_rst;
+      }
     }
     if (dt_hst > 0 && (t >= next_hst - eps || force)) {
       double hv[10];
@@ -203,15 +273,9 @@ int run(int argc, char **argv) {
       hst.flush();
       next_hst += dt_hst;
     }
-    if (dt_rst > 0 && (t >= next_rst - eps || final_dump)) {
-      char fn[512];
-      std::snprintf(fn, sizeof(fn), "%s.%04d.rst", basename.c_str(), nrst++);
-      chqd::write_restart(g, fn, t, cycle, download(m, "u0"), download(m, "b1f0"), download(m, "b2f0"),
-                          download(m, "b3f0"));
-      next_rst += dt_rst;
-    }
   };
   if (rstfile.empty()) do_outputs(0.0, true, false);
+  flush();
 
   // ---- time loop on the device ----
   const bool outputs_on = dt_vtk > 0 || dt_hst > 0 || dt_rst > 0;
@@ -229,6 +293,7 @@ int run(int argc, char **argv) {
       if (ndiag > 0) chunk = std::min(chunk, ndiag - (cycle % ndiag));
     }
     check(chq_cycles(m, chunk, nullptr), "cycles");
+    flush();   // files of the previous output, written while these cycles run
     double tdev = 0.0, dt = 0.0, mdt = 0.0;
     int cdev = 0;
     check(chq_clock(m, &tdev, &cdev, &dt, &mdt), "clock");
@@ -241,8 +306,10 @@ int run(int argc, char **argv) {
     do_outputs(dt, false, false);
     if (advanced < chunk) break;
   }
+  flush();
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (outputs_on) do_outputs(0.0, true, true);
+  flush();
 
   const double zones = (double)g.nx1 * g.nx2 * g.nx3;
   const int ncyc = cycle - cycle0;

@@ -144,6 +144,20 @@ def config_from_params(pin: Params) -> dict:
     c["nu"] = pin.get_or_add_real("diffusion", "nu", 0.0)
     c["kappa"] = pin.get_or_add_real("diffusion", "kappa", 0.0)
     c["eta"] = pin.get_or_add_real("diffusion", "eta", 0.0)
+    c["gravity_uniform"] = int(pin.get_or_add_bool("gravity", "uniform", False))
+    c["g1"] = pin.get_or_add_real("gravity", "g1", 0.0)
+    c["g2"] = pin.get_or_add_real("gravity", "g2", 0.0)
+    c["g3"] = pin.get_or_add_real("gravity", "g3", 0.0)
+    c["gravity_point"] = int(pin.get_or_add_bool("gravity", "point_mass", False))
+    c["gm"] = pin.get_or_add_real("gravity", "gm", 0.0)
+    c["gx0"] = pin.get_or_add_real("gravity", "x0", 0.0)
+    c["gy0"] = pin.get_or_add_real("gravity", "y0", 0.0)
+    c["gz0"] = pin.get_or_add_real("gravity", "z0", 0.0)
+    c["rsoft"] = pin.get_or_add_real("gravity", "rsoft", 0.0)
+    c["cooling"] = int(pin.get_or_add_bool("cooling", "enabled", False))
+    c["lambda0"] = pin.get_or_add_real("cooling", "lambda0", 0.0)
+    c["cool_alpha"] = pin.get_or_add_real("cooling", "alpha", 1.0)
+    c["tfloor"] = pin.get_or_add_real("cooling", "tfloor", 0.0)
     c["nx1"] = pin.get_int("mesh", "nx1")
     c["nx2"] = pin.get_or_add_int("mesh", "nx2", 1)
     c["nx3"] = pin.get_or_add_int("mesh", "nx3", 1)

@@ -59,6 +59,14 @@ typedef struct chq_config {
   int precision;          /* CHQ_FP64 or CHQ_MIXED */
   double tlim;            /* end time used by chq_cycles */
   int nlim;               /* < 0: no cycle limit; else stop after nlim cycles (time.nlim) */
+  /* gravity source (src/srcterms.hpp:10-41): uniform (g1, g2, g3) and/or a softened point
+   * mass gm at (gx0, gy0, gz0), applied after every Update with the stage's beta*dt */
+  int gravity_uniform, gravity_point;
+  double g1, g2, g3, gm, gx0, gy0, gz0, rsoft;
+  /* optically thin cooling Lambda = lambda0 T^alpha, integrated exactly over each step after
+   * the hyperbolic update (src/srcterms.hpp:43-71); cool_alpha defaults to 1 */
+  int cooling;
+  double lambda0, cool_alpha, tfloor;
 } chq_config;
 
 typedef struct chq_mesh chq_mesh;
@@ -84,6 +92,17 @@ CHQ_API const char *chq_last_error(void);
 CHQ_API long chq_array_size(const chq_mesh *m, const char *name);
 CHQ_API int chq_upload(chq_mesh *m, const char *name, const double *host, long n, void *stream);
 CHQ_API int chq_download(chq_mesh *m, const char *name, double *host, long n, void *stream);
+/* Output snapshot that does not stall the stepping (no reference counterpart: the reference
+ * writes outputs between cycles with a synchronous copy, src/output.hpp, src/restart.hpp).
+ * Copies the named fields (any chq_download name) device-to-device into a snapshot area
+ * behind the work queued on the mesh stream, then downloads them on a separate stream into
+ * host[q] (n[q] doubles each, the reference layout) while later cycles run. Host buffers
+ * from chq_host_alloc make the download asynchronous; pageable ones work but may block.
+ * The host buffers must stay untouched until chq_snapshot_wait returns. One snapshot per
+ * mesh is in flight; a new one waits for the previous. The snapshot area is allocated on
+ * first use and kept with the mesh. */
+CHQ_API int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *const *host, const long *n);
+CHQ_API int chq_snapshot_wait(chq_mesh *m);
 
 /* ---- stage seam (replaces src/main.cpp:46-93 call by call) ------------------------------ */
 /* kernels::FluxesDispatch<dir> (src/physics.hpp:505-514): fluxes and face EMFs of one
@@ -94,6 +113,8 @@ CHQ_API int chq_fluxes_all(chq_mesh *m, int cur, void *stream);
 /* kernels::CornerEMF (src/physics.hpp:242-297) */
 CHQ_API int chq_corner_emf(chq_mesh *m, void *stream);
 /* kernels::Update (src/physics.hpp:307-348): out = g0*(u0,b?f0) + g1*(u1,b?f1) - beta_dt*L */
+/* kernels::Update, followed by srcterms::ApplyGravity when gravity is configured (the
+ * reference always applies it right after Update, src/main.cpp:75-76) */
 CHQ_API int chq_update(chq_mesh *m, int out, double g0, double g1, double beta_dt, void *stream);
 /* kernels::Boundaries (src/physics.hpp:354-432) on buffer buf */
 CHQ_API int chq_boundaries(chq_mesh *m, int buf, void *stream);

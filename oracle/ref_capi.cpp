@@ -69,6 +69,21 @@ void Configure(RefSim &s) {
   ph.diff.nu = pin.GetOrAddReal("diffusion", "nu", 0.0);
   ph.diff.kappa = pin.GetOrAddReal("diffusion", "kappa", 0.0);
   ph.diff.eta = pin.GetOrAddReal("diffusion", "eta", 0.0);
+  // gravity and cooling: src/main.cpp:147-162
+  ph.grav.uniform = pin.GetOrAddBool("gravity", "uniform", false);
+  ph.grav.g1 = pin.GetOrAddReal("gravity", "g1", 0.0);
+  ph.grav.g2 = pin.GetOrAddReal("gravity", "g2", 0.0);
+  ph.grav.g3 = pin.GetOrAddReal("gravity", "g3", 0.0);
+  ph.grav.point = pin.GetOrAddBool("gravity", "point_mass", false);
+  ph.grav.gm = pin.GetOrAddReal("gravity", "gm", 0.0);
+  ph.grav.x0 = pin.GetOrAddReal("gravity", "x0", 0.0);
+  ph.grav.y0 = pin.GetOrAddReal("gravity", "y0", 0.0);
+  ph.grav.z0 = pin.GetOrAddReal("gravity", "z0", 0.0);
+  ph.grav.rsoft = pin.GetOrAddReal("gravity", "rsoft", 0.0);
+  ph.cool.enabled = pin.GetOrAddBool("cooling", "enabled", false);
+  ph.cool.lambda0 = pin.GetOrAddReal("cooling", "lambda0", 0.0);
+  ph.cool.alpha = pin.GetOrAddReal("cooling", "alpha", 1.0);
+  ph.cool.tfloor = pin.GetOrAddReal("cooling", "tfloor", 0.0);
   // src/main.cpp:165-178
   Mesh &m = s.m;
   m.nx1 = pin.GetInt("mesh", "nx1");
@@ -133,10 +148,19 @@ bool Cycle(RefSim &s) {
     const Real mdt = kernels::ConsToPrim(m, cfg, uo, b1o, b2o, b3o, last && !split_ops);
     if (last && !split_ops) s.min_dt = fmin(mdt, diffusion::TimeStep(m, cfg, ph.diff));
   }
+  // operator-split pieces on the end-of-step state: src/main.cpp:281-290
   if (ph.sts) {
     ph.sts_stages += sts::Advance(m, cfg, ph.diff, ph.sts_work, dt, diffusion::TimeStep(m, cfg, ph.diff));
     kernels::Boundaries(m, cfg, m.u0, m.b1f0, m.b2f0, m.b3f0);
+  }
+  if (ph.cool.enabled) {
+    kernels::ConsToPrim(m, cfg, m.u0, m.b1f0, m.b2f0, m.b3f0, false);
+    srcterms::ApplyCooling(m, cfg.eos, ph.cool, m.u0, dt);
+    kernels::Boundaries(m, cfg, m.u0, m.b1f0, m.b2f0, m.b3f0);
+  }
+  if (ph.sts || ph.cool.enabled) {
     s.min_dt = kernels::ConsToPrim(m, cfg, m.u0, m.b1f0, m.b2f0, m.b3f0, true);
+    if (!ph.sts) s.min_dt = fmin(s.min_dt, diffusion::TimeStep(m, cfg, ph.diff));
   }
   s.t += dt;
   ++s.cycle;

@@ -95,13 +95,13 @@ def read_restart(path):
 def test_usage_and_configuration_errors(tmp_path):
     r = _run(DRIVER, [], str(tmp_path))
     assert r.returncode == 1 and "usage" in r.stderr
-    inp = _write(tmp_path, "[mesh]\nnx1 = 8\n[problem]\nname = blast\n[cooling]\nenabled = true\n")
-    r = _run(DRIVER, ["-i", inp], str(tmp_path))
-    assert r.returncode == 1 and "cooling" in r.stderr
-    r = _run(DRIVER, ["-i", inp, "cooling.enabled=false", "mhd.reconstruct=ppm7", "--write-ic", "x.rst"], str(tmp_path))
+    inp = _write(tmp_path, "[mesh]\nnx1 = 8\n[problem]\nname = blast\n")
+    r = _run(DRIVER, ["-i", inp, "mhd.reconstruct=ppm7", "--write-ic", "x.rst"], str(tmp_path))
     assert r.returncode == 1 and "unknown reconstruct" in r.stderr
-    r = _run(DRIVER, ["-i", inp, "cooling.enabled=false", "problem.name=nothing", "--write-ic", "x.rst"], str(tmp_path))
+    r = _run(DRIVER, ["-i", inp, "problem.name=nothing", "--write-ic", "x.rst"], str(tmp_path))
     assert r.returncode == 1 and "unknown problem" in r.stderr
+    r = _run(DRIVER, ["-i", inp, "mesh.bc_x1=sticky", "--write-ic", "x.rst"], str(tmp_path))
+    assert r.returncode == 1 and "boundary" in r.stderr
 
 
 @pytest.mark.parametrize("name", sorted(PROBLEMS))
@@ -129,6 +129,8 @@ DRIVER_RUNS = {
                                                "output.hst_dt=0.001"]),
     "limiter_rk2": (cases.ot(24), ["time.integrator=rk2", "mhd.flux_limiter=true", "time.nlim=10",
                                    "output.rst_dt=100"]),
+    "gravity_cooling": (cases.ot(24), ["gravity.uniform=true", "gravity.g2=-0.3", "cooling.enabled=true",
+                                       "cooling.lambda0=0.2", "time.nlim=10", "output.hst_dt=0.005"]),
 }
 
 
