@@ -227,10 +227,16 @@ class Mesh:
         return pins
 
     def snapshot_wait(self) -> dict:
+        """Wait for the snapshot and return its fields as ordinary numpy arrays (copied out of
+        the page-locked buffers, which are released here)."""
         _check(load_library().chq_snapshot_wait(self._h))
         pins = getattr(self, "_snap", {})
         self._snap = {}
-        return {n: (p.array if p.array.shape[0] > 1 else p.array[0]) for n, p in pins.items()}
+        out = {}
+        for n, p in pins.items():
+            a = np.array(p.array, copy=True)
+            out[n] = a if a.shape[0] > 1 else a[0]
+        return out
 
     def get(self, name: str) -> np.ndarray:
         shp = self.shape(name)
@@ -483,6 +489,7 @@ class PinnedArray:
         _check(load_library().chq_host_alloc(8 * max(n, 1), C.byref(p)))
         self._p = p
         buf = (C.c_double * max(n, 1)).from_address(p.value)
+        buf._owner = self   # numpy views keep the buffer, the buffer keeps the allocation
         self.array = np.frombuffer(buf, dtype=np.float64, count=n).reshape(shape)
 
     def __del__(self):

@@ -143,7 +143,9 @@ template <class P> CHQ_D double new_b3(const UpdateArgs<P> &A, long l, double g0
   return g0 * A.b3a[l] + g1 * A.b3b[l] - bdt * curl;
 }
 
-template <class P> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by, int bz) {
+// GRAV: compile the gravity epilogue (a separate instantiation keeps the plain update's
+// register count, and with it its occupancy, unchanged)
+template <class P, bool GRAV = false> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
   if (A.need && *A.need == 0) return;
   const Geom &g = A.g;
@@ -166,7 +168,7 @@ template <class P> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by
       if (g.three_d) divf += ((double)ldg(A.f3 + ln + g.sk) - (double)ldg(A.f3 + ln)) * A.idx3;
       un[n] = g0 * A.ua[ln] + g1 * A.ub[ln] - bdt * divf;
     }
-    if (A.grav.on) {
+    if (GRAV && A.grav.on) {
       // ApplyGravity on the updated state with the stage primitives and beta*dt
       const GravityP &gr = A.grav;
       double a1 = gr.g1, a2 = gr.g2, a3 = gr.g3;
@@ -206,7 +208,9 @@ template <class P> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by
   }
 }
 
-template <class P> __global__ void __launch_bounds__(256) update_kernel(const UpdateArgs<P> A) { update_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+template <class P, bool GRAV> __global__ void __launch_bounds__(256) update_kernel(const UpdateArgs<P> A) {
+  update_body<P, GRAV>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // ---------------------------------------------------------------------------------------
 // Optically thin cooling after the step (src/srcterms.hpp:43-71): dT/dt = -(gamma-1) rho

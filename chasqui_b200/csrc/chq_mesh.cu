@@ -208,6 +208,7 @@ struct chq_mesh {
   };
   char *snap = nullptr;
   size_t snap_bytes = 0;
+  double *stage_buf = nullptr;   // upload staging (packed host layout), allocated on first upload
   cudaStream_t snap_stream = nullptr;
   cudaEvent_t snap_taken = nullptr, snap_landed = nullptr;
   std::vector<SnapItem> snap_items;
@@ -438,7 +439,8 @@ int do_update(chq_mesh *m, int out, double g0, double g1, double bdt, const doub
   const UpdateArgs<P> a = update_args<P>(m, out, g0, g1, bdt, bdt_dev, done, need);
   const Launch3 L = update_grid(m);
   m->nlaunch += 1;
-  update_kernel<P><<<L.grid, L.block, 0, s>>>(a);
+  if (a.grav.on) update_kernel<P, true><<<L.grid, L.block, 0, s>>>(a);
+  else update_kernel<P, false><<<L.grid, L.block, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
@@ -961,6 +963,46 @@ size_t field_esize(const chq_mesh *m, const FieldRef &f) {
   return sizeof(double);
 }
 
+// Packed host planes -> the device frame: nz planes of ny rows of nx doubles, starting at
+// plane k0 of one component (dst = component base). Host-to-device copies of contiguous
+// packed data run at the link's full rate (the row-pitched 3-D copy reached ~60 % of it on
+// a B200 host link), so uploads go through a device staging buffer and this kernel.
+__global__ void __launch_bounds__(256) unpack_planes_kernel(const double *src, double *dst, int nx, int ny, int nz,
+                                                            long sj, long sk, int k0) {
+  const long total = (long)nx * ny * nz;
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % nx);
+    const long r = q / nx;
+    const int j = (int)(r % ny);
+    const int k = (int)(r / ny) + k0;
+    dst[(long)k * sk + (long)j * sj + i] = src[q];
+  }
+}
+
+const size_t kStageBytes = 64ull << 20;   // planes per chunk: as many as fit in 64 MB
+
+// upload of one double component in plane chunks: copy (stream order) -> unpack -> next copy
+int upload_staged(chq_mesh *m, char *dev, const double *hst, int nx, int ny, int nz, cudaStream_t s) {
+  const Geom &g = m->g;
+  if (!m->stage_buf) {
+    const cudaError_t e = cudaMalloc(&m->stage_buf, kStageBytes);
+    if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("upload staging: ") + cudaGetErrorString(e));
+  }
+  const size_t plane = (size_t)nx * ny;   // plane * sizeof(double) <= kStageBytes (caller)
+  const int per = (int)(kStageBytes / (plane * sizeof(double)));
+  for (int k0 = 0; k0 < nz; k0 += per) {
+    const int nzc = std::min(per, nz - k0);
+    CHQ_CUDA(cudaMemcpyAsync(m->stage_buf, hst + (size_t)k0 * plane, (size_t)nzc * plane * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+    const long tot = (long)nzc * plane;
+    const unsigned blocks = (unsigned)std::min<long>((tot + 255) / 256, 148L * 16);
+    m->nlaunch += 1;
+    unpack_planes_kernel<<<blocks, 256, 0, s>>>(m->stage_buf, reinterpret_cast<double *>(dev), nx, ny, nzc, g.sj, g.sk, k0);
+    CHQ_CUDA(cudaGetLastError());
+  }
+  return CHQ_OK;
+}
+
 int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaStream_t s) {
   FieldRef f;
   if (!field_by_name(m, name, f)) return fail(CHQ_ERR_ARG, std::string("unknown field: ") + name);
@@ -985,6 +1027,12 @@ int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaS
     cudaMemcpy3DParms p{};
     char *dev = static_cast<char *>(f.base) + (size_t)c * g.vstride * es;
     char *hst = static_cast<char *>(hptr) + (size_t)c * nx * ny * nz * es;
+    // (a plane larger than the staging buffer takes the pitched copy below)
+    if (up && es == sizeof(double) && !f.isint && (size_t)nx * ny * sizeof(double) <= kStageBytes) {
+      const int rc = upload_staged(m, dev, reinterpret_cast<const double *>(hst), nx, ny, nz, s);
+      if (rc) return rc;
+      continue;
+    }
     cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)g.sj * es, (size_t)nx * es, (size_t)(g.nj + 1));
     cudaPitchedPtr hp = make_cudaPitchedPtr(hst, (size_t)nx * es, (size_t)nx * es, (size_t)ny);
     p.extent = make_cudaExtent((size_t)nx * es, (size_t)ny, (size_t)nz);
@@ -1431,6 +1479,7 @@ int chq_mesh_destroy(chq_mesh *m) {
   if (m->snap_taken) cudaEventDestroy(m->snap_taken);
   if (m->snap_landed) cudaEventDestroy(m->snap_landed);
   if (m->snap) cudaFree(m->snap);
+  if (m->stage_buf) cudaFree(m->stage_buf);
   for (auto &p : m->pending) { m->pool.push_back(p.b); m->pool.push_back(p.e); }
   for (cudaEvent_t e : m->pool) cudaEventDestroy(e);
   for (cudaEvent_t e : m->slots) if (e) cudaEventDestroy(e);
