@@ -407,7 +407,7 @@ template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) ==
 #define CHQ_FLUXYZ_MINB_D 4
 #endif
 #ifndef CHQ_FLUXYZ_MINB_F
-#define CHQ_FLUXYZ_MINB_F 9
+#define CHQ_FLUXYZ_MINB_F 8
 #endif
 template <class P> struct FluxYzMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUXYZ_MINB_D : CHQ_FLUXYZ_MINB_F; };
 

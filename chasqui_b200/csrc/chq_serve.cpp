@@ -240,7 +240,7 @@ int chq_server_step(chq_server *S) {
   if (rc) return rc;
   // Balanced chunks: the next step waits for every lane, so each lane gets about the same
   // work per step. The lane with the most cells runs cycles_per_step cycles, a lighter lane
-  // proportionally more (at most 16x); cycles past a job's end return at once on the device.
+  // proportionally more (at most 4x); cycles past a job's end return at once on the device.
   long long heaviest = 0;
   for (auto &kv : S->groups)
     if (kv.second.batch) heaviest = std::max(heaviest, kv.second.cells);
@@ -249,7 +249,7 @@ int chq_server_step(chq_server *S) {
     Group &g = kv.second;
     if (!g.batch) continue;
     long long n = S->cycles_per_step;
-    if (g.cells > 0) n = std::min<long long>(16LL * S->cycles_per_step, (S->cycles_per_step * heaviest + g.cells - 1) / g.cells);
+    if (g.cells > 0) n = std::min<long long>(4LL * S->cycles_per_step, (S->cycles_per_step * heaviest + g.cells - 1) / g.cells);
     rc = chq_batch_cycles(g.batch, (int)std::max(1LL, n), nullptr);
     if (rc) return rc;
     active += (int)g.members.size();
