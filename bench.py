@@ -179,6 +179,41 @@ def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, pro
                   "clocks": sampler.summary() if sampler else None, "fofc": fofc, "tune": tune}
 
 
+def config_rates(steps: int = 5, warmup: int = 3) -> dict:
+    """zone-updates/s of the other BASELINE configurations, timed like the headline (CUDA
+    events around whole device cycles, warm-up first): OT 2D 256^2 (config 1), CPAW 3D 256^3
+    along 2 pi (1,1,1) with WENO-Z (config 2), and the 512^3 blast with RKL2 diffusion
+    nu = eta = 1e-4 (config 3b; each cycle synchronises once for the RKL2 stage count)."""
+    from chasqui_b200 import Mesh, make_config
+    out = {}
+    runs = [
+        ("ot2d_256", dict(nx1=256, nx2=256, nx3=1, cfl=0.4, tlim=0.5), "orszag_tang", [-1.0], (0, 1)),
+        ("cpaw3d_256_wenoz", dict(nx1=256, nx2=256, nx3=256, recon=3, cfl=0.4, tlim=10.0), "cpaw",
+         [1, 1, 1, 1.0, 0.1, 1.0, 0.1], (0, 1)),
+        ("blast3d_512_rkl2", dict(nx1=512, nx2=512, nx3=512, x1min=-.5, x1max=.5, x2min=-.5, x2max=.5, x3min=-.5,
+                                  x3max=.5, cfl=0.3, tlim=0.2, nu=1e-4, eta=1e-4, sts=1), "blast", BLAST_PARAMS, (0,)),
+    ]
+    for name, kw, pg, prm, precs in runs:
+        for prec in precs:
+            m = Mesh(make_config(precision=prec, **kw))
+            m.init_problem(pg, prm)
+            m.prime(0.0)
+            m.autotune()
+            m.cycles(warmup)
+            m.clock()
+            m.record(0)
+            m.cycles(steps)
+            m.record(1)
+            ms = m.elapsed_ms(0, 1)
+            cells = kw["nx1"] * kw["nx2"] * kw["nx3"]
+            r = {"value": cells * steps / (ms / 1e3), "ms_per_step": ms / steps, "cells": cells}
+            if kw.get("sts"):
+                r["rkl2_stages_per_cycle"] = m.sts_stages() / (warmup + steps)
+            out[name + ("_mixed" if prec else "_fp64")] = r
+            m.close()
+    return out
+
+
 def tune_summary(tune):
     """autotuned vs default march length of the flux kernel (ms per launch per length)"""
     ms = tune["ms"]
@@ -396,6 +431,7 @@ def main(argv=None):
     ap.add_argument("--srv-rates", default="10,40")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     rank, local = env_int("RANK", 0), env_int("LOCAL_RANK", 0)
@@ -453,6 +489,10 @@ def main(argv=None):
         meshm.close()
         del meshm
 
+    cfgs = None
+    if rank == 0 and not args.no_configs and n == 512:
+        cfgs = config_rates()
+
     ens = None
     if not args.no_ensemble:
         ens = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 4)
@@ -489,6 +529,7 @@ def main(argv=None):
             "autotune": tune_summary(r64["tune"]),
             "e2e": e2e,
             "mixed": mixed,
+            "configs": cfgs,
             "ensemble": ens,
             "serving": srv,
             "cpu_baseline": cpu,

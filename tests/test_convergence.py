@@ -1,0 +1,70 @@
+"""CPAW convergence on the device (README.md:90-99): one wave period of
+the circularly polarised Alfven wave at N = 32, 64, 128, total L1 error against the initial
+state as the reference's compute_error (src/main.cpp:310-327). The device errors equal the
+reference's own (relative 1e-9: the runs are bitwise up to the entropy slot's pow), so the
+convergence orders match the published table (README.md:90-96) as the reference does."""
+import math
+
+import numpy as np
+import pytest
+
+from tests import cases
+from tests.parity import copy_state, make_pair
+from tests.test_oracle_pins import PUBLISHED, cpaw_l1
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u0", "b1f0", "b2f0", "b3f0")
+
+
+def device_l1(text, ov, n_cells, act):
+    ref, mesh = make_pair(text, ov)
+    copy_state(ref, mesh, FIELDS)
+    ref.close()
+    mesh.prime(0.0)
+    u0, b0 = mesh.get("u0").copy(), mesh.get("bcc").copy()
+    while mesh.clock()["t"] < 1.0 - 1e-12:
+        mesh.cycles(256)
+    assert abs(mesh.clock()["t"] - 1.0) < 1e-12
+    u1, b1 = mesh.get("u0"), mesh.get("bcc")
+    err = np.abs(u1[act] - u0[act]).sum(axis=(1, 2, 3)).tolist() + np.abs(b1[act] - b0[act]).sum(axis=(1, 2, 3)).tolist()
+    return sum(e / n_cells for e in err)
+
+
+@pytest.mark.parametrize("scheme", sorted(PUBLISHED))
+def test_cpaw1d_errors_and_orders(scheme):
+    ov = [f"mhd.reconstruct={scheme}", "time.tlim=1.0"]
+    dev = []
+    for n in (32, 64, 128):
+        ng = 3 if scheme in ("ppm", "ppmx", "wenoz") else 2
+        act = (slice(None), slice(0, 1), slice(0, 1), slice(ng, ng + n))
+        dev.append(device_l1(cases.cpaw1d(n), ov, n, act))
+    ref = [cpaw_l1(scheme, n) for n in (32, 64, 128)]
+    for d, r in zip(dev, ref):
+        assert d == pytest.approx(r, rel=1e-9), (scheme, dev, ref)
+    pub = PUBLISHED[scheme]
+    for q in range(2):
+        assert abs(math.log2(dev[q] / dev[q + 1]) - math.log2(pub[q] / pub[q + 1])) < 0.15, (scheme, dev, pub)
+
+
+def test_cpaw3d_second_order():
+    """3D CPAW along the diagonal of the (x, y) plane, extruded in z (WENO-Z + HLLD): second
+    order between 16 and 32 cells per wavelength, as README.md:98-99 states for 3D."""
+    from oracle.refsim import RefSim
+    errs = []
+    for n in (16, 32):
+        text = cases.cpaw3d_extruded(n, 8)
+        ov = ["mhd.reconstruct=wenoz", "time.tlim=1.0"]
+        act = (slice(None), slice(3, 3 + 8), slice(3, 3 + n), slice(3, 3 + n))
+        errs.append(device_l1(text, ov, n * n * 8, act))
+        s = RefSim(text, ov)
+        u0, b0 = s.get("u0").copy(), s.get("bcc").copy()
+        while s.cycles(100) > 0:
+            pass
+        u1, b1 = s.get("u0"), s.get("bcc")
+        ref = sum(np.abs(u1[act] - u0[act]).sum(axis=(1, 2, 3)).tolist()
+                  + np.abs(b1[act] - b0[act]).sum(axis=(1, 2, 3)).tolist()) / (n * n * 8)
+        s.close()
+        assert errs[-1] == pytest.approx(ref, rel=1e-9), (n, errs[-1], ref)
+    order = math.log2(errs[0] / errs[1])
+    assert 1.7 < order < 2.6, (errs, order)   # the reference: 2.08
