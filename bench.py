@@ -152,7 +152,9 @@ def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, pro
     mesh.prime(0.0)
     # flux-kernel march length picked by the library's autotuner on this state (the default
     # is 16; the per-length launch times are reported beside the choice)
+    default_len = mesh.seglen
     tune = mesh.autotune()
+    tune["default"] = default_len
     mesh.cycles(warmup)
     mesh.clock()
     l0 = mesh.kernel_launches()
@@ -217,9 +219,10 @@ def config_rates(steps: int = 5, warmup: int = 3) -> dict:
 def tune_summary(tune):
     """autotuned vs default march length of the flux kernel (ms per launch per length)"""
     ms = tune["ms"]
-    out = {"default_seglen": 16, "seglen": tune["seglen"], "flux_ms_per_launch": {str(k): v for k, v in ms.items()}}
-    if ms.get(16, -1) > 0 and ms.get(tune["seglen"], -1) > 0:
-        out["speedup_vs_default"] = ms[16] / ms[tune["seglen"]]
+    d = tune.get("default", 16)
+    out = {"default_seglen": d, "seglen": tune["seglen"], "flux_ms_per_launch": {str(k): v for k, v in ms.items()}}
+    if ms.get(d, -1) > 0 and ms.get(tune["seglen"], -1) > 0:
+        out["speedup_vs_default"] = ms[d] / ms[tune["seglen"]]
     return out
 
 

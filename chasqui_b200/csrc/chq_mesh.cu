@@ -209,6 +209,11 @@ struct chq_mesh {
   char *snap = nullptr;
   size_t snap_bytes = 0;
   double *stage_buf = nullptr;   // upload staging (packed host layout), allocated on first upload
+  // whole-cycle CUDA graph of chq_cycles on the mesh stream (built after one plain cycle)
+  cudaGraph_t cyc_graph = nullptr;
+  cudaGraphExec_t cyc_exec = nullptr;
+  long long cyc_launches = 0;   // kernels in one captured cycle
+  bool cyc_warm = false;        // a plain cycle has run (first-launch attribute set-up done)
   cudaStream_t snap_stream = nullptr;
   cudaEvent_t snap_taken = nullptr, snap_landed = nullptr;
   std::vector<SnapItem> snap_items;
@@ -226,7 +231,6 @@ struct chq_mesh {
 
 namespace {
 
-const int kSeglen = 16;
 const int kHstBlocks = 1184;   // 8 blocks per SM on 148 SMs
 
 // bytes of one mesh slab: 18 double fields (u0, u1, 6 face fields), 39 fields of the
@@ -1376,7 +1380,6 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   m->nstage = c.integrator;
   m->mixed = (c.precision == CHQ_MIXED);
   m->psize = m->mixed ? sizeof(float) : sizeof(double);
-  m->seglen = kSeglen;
 
   // flux face ranges (src/physics.hpp:85-88) and active face ranges (src/positivity.hpp:32-33)
   for (int d = 0; d < 3; ++d) {
@@ -1394,6 +1397,22 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   m->active[0] = 1;
   m->active[1] = g.two_d;
   m->active[2] = g.three_d;
+  // default march length: the longest of 16, 8, 4 that still gives the y/z sweeps a full
+  // device of threads (148 SMs x 1024), so that small meshes are not one long serial march
+  // per thread (chq_autotune measures instead)
+  {
+    const long lanes = (long)((g.ni + 1 + 31) / 32) * 32;
+    m->seglen = 4;
+    for (int L : {16, 8}) {
+      long threads = 0;
+      if (g.two_d) threads += lanes * (m->hi[1][0] - m->lo[1][0] + 1) * ((m->hi[1][1] - m->lo[1][1] + 1 + L - 1) / L);
+      if (g.three_d) threads += lanes * (m->hi[2][1] - m->lo[2][1] + 1) * ((m->hi[2][0] - m->lo[2][0] + 1 + L - 1) / L);
+      if (threads >= 148L * 1024) {
+        m->seglen = L;
+        break;
+      }
+    }
+  }
 
   // one slab: doubles (u0, u1: 6 each; 6 face fields), P fields (w 6, bcc 3, ecc 3,
   // fluxes 18, face EMFs 6, edge EMFs 3), the int flag array, control block and scratch
@@ -1480,6 +1499,8 @@ int chq_mesh_destroy(chq_mesh *m) {
   if (m->snap_landed) cudaEventDestroy(m->snap_landed);
   if (m->snap) cudaFree(m->snap);
   if (m->stage_buf) cudaFree(m->stage_buf);
+  if (m->cyc_exec) cudaGraphExecDestroy(m->cyc_exec);
+  if (m->cyc_graph) cudaGraphDestroy(m->cyc_graph);
   for (auto &p : m->pending) { m->pool.push_back(p.b); m->pool.push_back(p.e); }
   for (cudaEvent_t e : m->pool) cudaEventDestroy(e);
   for (cudaEvent_t e : m->slots) if (e) cudaEventDestroy(e);
@@ -1742,9 +1763,11 @@ int chq_prime(chq_mesh *m, double t, void *stream) {
   return CHQ_OK;
 }
 
-int chq_cycles(chq_mesh *m, int n, void *stream) {
-  if (!m || n < 0) return fail(CHQ_ERR_ARG, "bad argument");
-  cudaStream_t s = S(m, stream);
+}  // extern "C"
+
+namespace chq {
+// n cycles as individual launches (the body of chq_cycles)
+int plain_cycles(chq_mesh *m, int n, cudaStream_t s) {
   const int *done = &m->ctl->done;
   const bool sts = m->cfg.sts && m->diff;
   const bool cool = m->cfg.cooling != 0;
@@ -1817,6 +1840,55 @@ int chq_cycles(chq_mesh *m, int n, void *stream) {
     }
     CHQ_CUDA(cudaGetLastError());
   }
+  return CHQ_OK;
+}
+
+void drop_cycle_graph(chq_mesh *m) {
+  if (m->cyc_exec) cudaGraphExecDestroy(m->cyc_exec);
+  if (m->cyc_graph) cudaGraphDestroy(m->cyc_graph);
+  m->cyc_exec = nullptr;
+  m->cyc_graph = nullptr;
+}
+}  // namespace chq
+
+extern "C" {
+
+// Whole cycles. Without RKL2 (whose stage count the host decides each cycle) and without
+// per-kernel profiling, cycles on the mesh's own stream replay a CUDA graph of one cycle,
+// captured after a first plain cycle: a cycle is ~70 small launches, and on small meshes
+// their CPU cost exceeds the device time. The launch count of a replayed cycle is the
+// captured one's.
+int chq_cycles(chq_mesh *m, int n, void *stream) {
+  if (!m || n < 0) return fail(CHQ_ERR_ARG, "bad argument");
+  cudaStream_t s = S(m, stream);
+  const bool graphable = !(m->cfg.sts && m->diff) && !m->prof && (stream == nullptr || s == m->stream);
+  if (!graphable || n == 0) return plain_cycles(m, n, s);
+  int done_plain = 0;
+  if (!m->cyc_warm) {
+    const int rc = plain_cycles(m, 1, s);
+    if (rc) return rc;
+    m->cyc_warm = true;
+    done_plain = 1;
+  }
+  if (done_plain == n) return CHQ_OK;
+  if (!m->cyc_exec) {
+    const long long l0 = m->nlaunch;
+    CHQ_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int rc = plain_cycles(m, 1, s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CHQ_CUDA(e);
+    m->cyc_graph = g;
+    CHQ_CUDA(cudaGraphInstantiate(&m->cyc_exec, m->cyc_graph, 0));
+    m->cyc_launches = m->nlaunch - l0;   // the capture itself ran nothing
+    m->nlaunch = l0;
+  }
+  for (int c = done_plain; c < n; ++c) CHQ_CUDA(cudaGraphLaunch(m->cyc_exec, s));
+  m->nlaunch += m->cyc_launches * (n - done_plain);
   return CHQ_OK;
 }
 
@@ -2049,6 +2121,7 @@ long long chq_kernel_launches(const chq_mesh *m) { return m ? m->nlaunch : 0; }
 
 int chq_set_seglen(chq_mesh *m, int seglen) {
   if (!m || seglen < 1 || seglen > 1024) return fail(CHQ_ERR_ARG, "march length must be in [1, 1024]");
+  if (seglen != m->seglen) drop_cycle_graph(m);
   m->seglen = seglen;
   return CHQ_OK;
 }
@@ -2057,6 +2130,7 @@ int chq_get_seglen(const chq_mesh *m) { return m ? m->seglen : 0; }
 
 int chq_autotune(chq_mesh *m, int *seglen, double ms[CHQ_TUNE_NLEN]) {
   if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  drop_cycle_graph(m);   // the captured cycle holds the old march length
   static std::mutex mu;
   static std::map<std::vector<int>, int> cache;
   const std::vector<int> key = {m->mixed, m->cfg.recon, m->cfg.rsolver, m->cfg.characteristic,

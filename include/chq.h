@@ -187,7 +187,8 @@ CHQ_API int chq_profile(chq_mesh *m, int enable);
 /* ---- flux-kernel autotuning (no reference counterpart: the reference has one fixed
  * Kokkos range policy) ---------------------------------------------------------------------
  * March length = faces each thread of the y/z sweeps carries its cell states across. The
- * default is 16. chq_autotune times the flux kernel of this mesh's scheme on its current
+ * default is the longest of 16, 8, 4 that keeps a full device of y/z threads busy (16 from
+ * about 128^3 up, 4 for small meshes). chq_autotune times the flux kernel of this mesh's scheme on its current
  * state (call it after chq_prime) for every candidate in CHQ_TUNE_LENGTHS, keeps the fastest
  * on the mesh, and returns it with the per-candidate ms per launch (ms may be NULL). The
  * choice is cached for the process per (precision, reconstruction, Riemann solver,
