@@ -6,13 +6,15 @@
 // (E_t2 = -F(B_t1), E_t1 = +F(B_t2)). Same face ranges and outputs as the reference's
 // Fluxes<DIR,R,S> (src/physics.hpp:66-226); the left/right face states never leave the SM.
 //
-// Work decomposition (one launch covers all three directions):
-//   x-sweep : one warp = 32 consecutive cells of a row; lane l computes the (aL, aR) pair
-//             of its cell once and receives its left neighbour's aR by __shfl_up_sync, so a
-//             warp emits 31 faces and no cell parabola is evaluated twice.
-//   y/z-sweep: lanes run along i (fully coalesced rows); each thread marches `seglen` faces
-//             along the sweep direction, carrying the previous cell's aR in registers.
-// Warps for z come first, then y, then x, so that the short x warps fill the tail.
+// Work decomposition, two launches per stage:
+//   flux_x_kernel : one warp = 32 consecutive cells of a row; lane l computes the (aL, aR)
+//             pair of its cell once (stencil from L1) and receives its left neighbour's aR by
+//             __shfl_up_sync, so a warp emits 31 faces and no cell parabola is evaluated twice.
+//   flux_yz_kernel: lanes run along i (fully coalesced rows); each thread marches `seglen`
+//             faces along y or z with its stencil in a shared-memory window that cp.async
+//             refills one cell ahead, and parks the previous cell's aR in shared memory
+//             during the Riemann solve. z warps come first, then y.
+// The batched forms (flux_x_batched, flux_yz_batched) run the same sweeps for many meshes.
 #pragma once
 #include "chq_common.cuh"
 #include "chq_recon.cuh"

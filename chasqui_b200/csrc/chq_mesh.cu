@@ -1843,6 +1843,22 @@ int plain_cycles(chq_mesh *m, int n, cudaStream_t s) {
   return CHQ_OK;
 }
 
+// the mesh's own stream (the server records events behind a solo job's cycles on it)
+cudaStream_t mesh_stream(chq_mesh *m) { return m->stream; }
+
+// A copy of the step control queued behind the mesh's work, so that the server learns a solo
+// job's clock without synchronising the stream (which would also wait for the next chunk).
+size_t clock_bytes() { return sizeof(StepCtl); }
+int clock_enqueue(chq_mesh *m, void *pinned) {
+  CHQ_CUDA(cudaMemcpyAsync(pinned, m->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, m->stream));
+  return CHQ_OK;
+}
+void clock_decode(const void *pinned, double *t, int *cycle) {
+  const StepCtl *c = static_cast<const StepCtl *>(pinned);
+  *t = c->t;
+  *cycle = c->cycle;
+}
+
 void drop_cycle_graph(chq_mesh *m) {
   if (m->cyc_exec) cudaGraphExecDestroy(m->cyc_exec);
   if (m->cyc_graph) cudaGraphDestroy(m->cyc_graph);

@@ -12,6 +12,9 @@
 //      with the fewest cells; each lane has its own stream and replays a CUDA graph, so the
 //      flux kernel of one lane overlaps the memory-bound kernels of another. Batching alone
 //      serialises every job through the same kernel sequence.
+// Jobs of 2^21 cells or more are not batched: each runs "solo" on its own mesh stream,
+// replaying a CUDA graph of one cycle, and the server polls an event behind its chunk instead
+// of waiting for it, so a large job never holds up the lanes (or another large job).
 // Each job keeps its own dt and clock on the device, so its result is the same alone and in
 // any mix. Times are seconds on the server's steady clock.
 #include <chrono>
@@ -21,10 +24,15 @@
 #include <string>
 #include <tuple>
 #include <vector>
+#include <cuda_runtime.h>
 #include "chq.h"
 
 namespace chq {
 void set_last_error(const std::string &msg);
+cudaStream_t mesh_stream(chq_mesh *m);
+size_t clock_bytes();
+int clock_enqueue(chq_mesh *m, void *pinned);
+void clock_decode(const void *pinned, double *t, int *cycle);
 }
 
 namespace {
@@ -43,7 +51,23 @@ struct Job {
   int cycle = 0;
   long long cells = 0;
   double hist[10] = {};
+  // solo jobs (large meshes) run on their own stream with graph-replayed cycles, two chunks
+  // queued; behind each chunk a copy of the clock lands in pinned memory and an event is
+  // recorded, which the server polls, so a solo job never waits for the rest of the server
+  bool solo = false;
+  int head = 0, nfly = 0;             // oldest chunk in flight, chunks in flight
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  void *clk[2] = {nullptr, nullptr};  // pinned clock copies
 };
+
+void free_solo(Job *j) {
+  for (int q = 0; q < 2; ++q) {
+    if (j->ev[q]) cudaEventDestroy(j->ev[q]);
+    if (j->clk[q]) cudaFreeHost(j->clk[q]);
+    j->ev[q] = nullptr;
+    j->clk[q] = nullptr;
+  }
+}
 
 // (precision, reconstruction, Riemann solver, characteristic, integrator, FOFC, limiter, lane)
 using ClassKey = std::tuple<int, int, int, int, int, int, int, int>;
@@ -74,6 +98,7 @@ struct chq_server {
   std::map<long long, Job *> jobs;
   std::vector<Job *> queue;
   std::map<ClassKey, Group> groups;
+  std::vector<Job *> solo;   // running solo jobs
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   long long zone_updates = 0;
   double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
@@ -128,9 +153,100 @@ int retire_finished(chq_server *S) {
   return CHQ_OK;
 }
 
+// Jobs of at least this many cells run solo: one mesh stream each, cycles replayed as a CUDA
+// graph. Their launches fill the device on their own (a 128^3 flux launch is two waves of
+// resident blocks), and running them concurrently overlaps one job's flux kernel with
+// another's memory-bound kernels, which a batch (one kernel kind at a time for all members)
+// cannot. Smaller jobs fill the device only together, in a batched launch.
+const long long kSoloCells = 1LL << 21;
+
+// finished solo chunks: progress and retirement; with `block`, wait for a chunk when none
+// has finished
+int retire_solo(chq_server *S, bool block) {
+  bool any = false;
+  Job *oldest = nullptr;
+  auto finish = [&](Job *j) -> int {
+    // the chunk behind the final one (if queued) returns at once on the device; history
+    // runs after it on the mesh stream
+    int rc = chq_history(j->mesh, j->hist, nullptr);
+    if (rc) return rc;
+    bool finite = true;
+    for (double v : j->hist) finite = finite && (v == v) && (v - v == 0.0);
+    chq_mesh_destroy(j->mesh);
+    j->mesh = nullptr;
+    free_solo(j);
+    j->nfly = 0;
+    S->used -= j->bytes;
+    j->state = finite ? CHQ_JOB_DONE : CHQ_JOB_FAILED;
+    j->t_done = S->now();
+    return CHQ_OK;
+  };
+  auto poll = [&]() -> int {
+    for (Job *j : S->solo) {
+      while (j->state == CHQ_JOB_RUNNING && j->nfly > 0) {
+        const cudaError_t q = cudaEventQuery(j->ev[j->head]);
+        if (q == cudaErrorNotReady) {
+          if (!oldest) oldest = j;
+          break;
+        }
+        if (q != cudaSuccess) return err(CHQ_ERR_CUDA, std::string("solo job: ") + cudaGetErrorString(q));
+        double t = 0;
+        int cyc = 0;
+        chq::clock_decode(j->clk[j->head], &t, &cyc);
+        j->head ^= 1;
+        --j->nfly;
+        any = true;
+        S->zone_updates += (long long)(cyc - j->cycle) * j->cells;
+        j->t = t;
+        j->cycle = cyc;
+        if (!(t < j->cfg.tlim) || (j->cfg.nlim >= 0 && cyc >= j->cfg.nlim)) {
+          const int rc = finish(j);
+          if (rc) return rc;
+        }
+      }
+    }
+    return CHQ_OK;
+  };
+  int rc = poll();
+  if (rc) return rc;
+  if (block && !any && oldest) {
+    // no wait-for-any on events: wait for the first queued chunk, then take every chunk
+    // that has finished by then
+    const cudaError_t e = cudaEventSynchronize(oldest->ev[oldest->head]);
+    if (e != cudaSuccess) return err(CHQ_ERR_CUDA, std::string("solo job: ") + cudaGetErrorString(e));
+    if ((rc = poll())) return rc;
+  }
+  std::vector<Job *> keep;
+  for (Job *j : S->solo)
+    if (j->state == CHQ_JOB_RUNNING) keep.push_back(j);
+  S->solo.swap(keep);
+  return CHQ_OK;
+}
+
+// keep two chunks of cycles_per_step cycles queued on every solo job's stream
+int launch_solo(chq_server *S) {
+  for (Job *j : S->solo) {
+    while (j->nfly < 2) {
+      const int slot = (j->head + j->nfly) & 1;
+      if (!j->ev[slot]) {
+        cudaError_t e = cudaEventCreateWithFlags(&j->ev[slot], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaHostAlloc(&j->clk[slot], chq::clock_bytes(), cudaHostAllocDefault);
+        if (e != cudaSuccess) return err(CHQ_ERR_CUDA, std::string("solo job: ") + cudaGetErrorString(e));
+      }
+      int rc = chq_cycles(j->mesh, S->cycles_per_step, nullptr);
+      if (!rc) rc = chq::clock_enqueue(j->mesh, j->clk[slot]);
+      if (rc) return rc;
+      const cudaError_t e = cudaEventRecord(j->ev[slot], chq::mesh_stream(j->mesh));
+      if (e != cudaSuccess) return err(CHQ_ERR_CUDA, std::string("solo job: ") + cudaGetErrorString(e));
+      ++j->nfly;
+    }
+  }
+  return CHQ_OK;
+}
+
 void admit(chq_server *S) {
   std::vector<Job *> still;
-  int active = 0;
+  int active = (int)S->solo.size();
   for (auto &kv : S->groups) active += (int)kv.second.members.size();
   for (Job *j : S->queue) {
     if (active >= S->max_active || S->used + j->bytes > S->budget) {
@@ -153,6 +269,12 @@ void admit(chq_server *S) {
     S->used += j->bytes;
     j->state = CHQ_JOB_RUNNING;
     j->t_start = S->now();
+    if (j->cells >= kSoloCells) {
+      j->solo = true;
+      S->solo.push_back(j);
+      ++active;
+      continue;
+    }
     int lane = 0;
     long long least = -1;
     for (int q = 0; q < S->lanes; ++q) {
@@ -233,7 +355,12 @@ int chq_server_submit(chq_server *S, const chq_config *cfg, int problem, const d
 
 int chq_server_step(chq_server *S) {
   if (!S) return err(CHQ_ERR_ARG, "null server");
-  int rc = retire_finished(S);
+  bool lanes_busy = false;
+  for (auto &kv : S->groups) lanes_busy = lanes_busy || (kv.second.batch && !kv.second.members.empty());
+  // solo jobs first without waiting (block only when nothing else would make progress)
+  int rc = retire_solo(S, !lanes_busy);
+  if (rc) return rc;
+  rc = retire_finished(S);
   if (rc) return rc;
   admit(S);
   rc = rebuild(S);
@@ -244,7 +371,9 @@ int chq_server_step(chq_server *S) {
   long long heaviest = 0;
   for (auto &kv : S->groups)
     if (kv.second.batch) heaviest = std::max(heaviest, kv.second.cells);
-  int active = 0;
+  rc = launch_solo(S);
+  if (rc) return rc;
+  int active = (int)S->solo.size();
   for (auto &kv : S->groups) {
     Group &g = kv.second;
     if (!g.batch) continue;
@@ -284,7 +413,7 @@ chq_mesh *chq_server_job_mesh(chq_server *S, long long id) {
 int chq_server_stats(chq_server *S, long long *used_bytes, int *active, int *queued, long long *zone_updates,
                      double *clock) {
   if (!S) return err(CHQ_ERR_ARG, "null server");
-  int a = 0;
+  int a = (int)S->solo.size();
   for (auto &kv : S->groups) a += (int)kv.second.members.size();
   if (used_bytes) *used_bytes = S->used;
   if (active) *active = a;
@@ -307,7 +436,8 @@ int chq_server_destroy(chq_server *S) {
     for (chq_mesh *m : kv.second.retired) chq_mesh_destroy(m);
   }
   for (auto &kv : S->jobs) {
-    if (kv.second->mesh) chq_mesh_destroy(kv.second->mesh);
+    if (kv.second->mesh) chq_mesh_destroy(kv.second->mesh);   // synchronises its stream first
+    free_solo(kv.second);
     delete kv.second;
   }
   delete S;

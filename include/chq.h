@@ -232,6 +232,8 @@ CHQ_API void *chq_batch_stream(chq_batch *b);
  * launches cycles_per_step batched cycles of every class. Each class is split into up to
  * `lanes` batches (default 8) of balanced cell counts, each on its own stream as a replayed
  * CUDA graph, so that the memory-bound kernels of one lane overlap the flux kernel of another.
+ * Jobs of 2^21 cells or more run solo on their own mesh stream (a replayed graph of one
+ * cycle); the server polls an event behind each solo chunk instead of waiting for it.
  * A job whose final state is not finite is reported FAILED; kernels index only their own
  * job, so it never disturbs the others. Times are seconds on the server clock. */
 enum { CHQ_JOB_QUEUED = 0, CHQ_JOB_RUNNING = 1, CHQ_JOB_DONE = 2, CHQ_JOB_FAILED = 3 };

@@ -36,14 +36,18 @@ JOBS = [
 ]
 
 
+SOLO_CELLS = 1 << 21   # jobs this large run unbatched on their own stream
+
+
 def solo_history(cfg, problem, params):
     """The job run by itself: alone on its mesh in the FP64 form (batched FP64 stepping is
     bitwise equal to it), in a batch of its own in the mixed form (the batched FP32 flux
-    kernel may fuse multiply-adds differently from the single-mesh one)."""
+    kernel may fuse multiply-adds differently from the single-mesh one) unless the job is
+    large enough for the server to run it unbatched."""
     m = Mesh(cfg)
     m.init_problem(problem, params)
     m.prime(0.0)
-    if cfg.precision == 1:
+    if cfg.precision == 1 and cfg.nx1 * cfg.nx2 * cfg.nx3 < SOLO_CELLS:
         b = Batch([m], graph=True)
         while not b.status()[0]["done"] and b.status()[0]["cycle"] < cfg.nlim:
             b.cycles(4)
@@ -73,6 +77,32 @@ def test_results_equal_solo_runs_in_any_mix():
         assert st["cycle"] == cyc == f().nlim
         assert np.array_equal(np.array(st["history"]), h), (p, st["history"], h)
         assert st["t_done"] >= st["t_start"] >= st["t_submit"]
+
+
+def test_large_jobs_run_solo_beside_batched_lanes():
+    """Jobs of 2^21 cells or more run on their own streams (polled, never waited for) while
+    small jobs step in batched lanes; every result equals the job run alone."""
+    jobs = [
+        (lambda: ot_cfg(2048, 4), "orszag_tang", [-1.0]),
+        (lambda: blast_cfg(128, 5, precision=1), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 3.0]),
+        (lambda: blast_cfg(128, 3), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 4.0]),
+        (lambda: blast_cfg(64, 5), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 5.0]),
+        (lambda: ot_cfg(32, 12), "orszag_tang", [-1.0]),
+        (lambda: blast_cfg(16, 9, precision=1), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 7.0]),
+    ]
+    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=2)
+    ids = [srv.submit(f(), p, prm) for f, p, prm in jobs]
+    run_all(srv)
+    total = 0
+    for jid, (f, p, prm) in zip(ids, jobs):
+        st = srv.status(jid)
+        h, cyc = solo_history(f(), p, prm)
+        assert st["state"] == "done", st
+        assert st["cycle"] == cyc == f().nlim
+        assert np.array_equal(np.array(st["history"]), h), (p, st["history"], h)
+        total += f().nlim * f().nx1 * f().nx2 * f().nx3
+    s = srv.stats()
+    assert s["zone_updates"] == total and s["active"] == 0 and s["used_bytes"] == 0
 
 
 def test_admission_respects_budget_and_drains():
