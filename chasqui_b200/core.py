@@ -83,12 +83,15 @@ SIGNATURES = [
     ("chq_get_seglen", C.c_int, [_P]),
     ("chq_history", C.c_int, [_P, _D, _P]),
     ("chq_run_host", C.c_int, [_P, _D, _D, _D, _D, C.c_int, C.c_double, _P]),
+    ("chq_run_host_async", C.c_int, [_P, _D, _D, _D, _D, C.c_int, C.c_double]),
+    ("chq_run_host_wait", C.c_int, [_P, C.POINTER(C.c_int)]),
     ("chq_set_device", C.c_int, [C.c_int]),
     ("chq_device_count", C.c_int, [C.POINTER(C.c_int)]),
     ("chq_host_alloc", C.c_int, [C.c_longlong, C.POINTER(_P)]),
     ("chq_host_free", C.c_int, [_P]),
     ("chq_event_record", C.c_int, [_P, C.c_int]),
     ("chq_event_elapsed", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_float)]),
+    ("chq_event_elapsed_between", C.c_int, [_P, C.c_int, _P, C.c_int, C.POINTER(C.c_float)]),
     ("chq_profile", C.c_int, [_P, C.c_int]),
     ("chq_profile_read", C.c_int, [_P, _D, C.POINTER(C.c_longlong), C.c_int]),
     ("chq_kernel_launches", C.c_longlong, [_P]),
@@ -188,8 +191,9 @@ class Mesh:
 
     def close(self):
         if getattr(self, "_h", None):
-            load_library().chq_mesh_destroy(self._h)
+            load_library().chq_mesh_destroy(self._h)   # waits for queued work, host jobs included
             self._h = None
+        self._host_jobs = None
 
     def __del__(self):
         try:
@@ -344,6 +348,25 @@ class Mesh:
                 raise ChqError("run_host needs C-contiguous float64 arrays")
         return _check(load_library().chq_run_host(self._h, _dptr(u), _dptr(b1), _dptr(b2), _dptr(b3), ncycles, t0, None))
 
+    def run_host_async(self, u: np.ndarray, b1: np.ndarray, b2: np.ndarray, b3: np.ndarray, ncycles: int,
+                       t0: float = 0.0):
+        """Queue run_host's job without waiting (up to two per mesh); the arrays must be
+        page-locked (PinnedArray) and are held until the run_host_wait() that returns it."""
+        for a in (u, b1, b2, b3):
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ChqError("run_host_async needs C-contiguous float64 arrays")
+        _check(load_library().chq_run_host_async(self._h, _dptr(u), _dptr(b1), _dptr(b2), _dptr(b3), ncycles, t0))
+        if getattr(self, "_host_jobs", None) is None:
+            self._host_jobs = []
+        self._host_jobs.append((u, b1, b2, b3))
+
+    def run_host_wait(self) -> int:
+        """Wait for the oldest queued host job; its cycle count."""
+        c = C.c_int()
+        _check(load_library().chq_run_host_wait(self._h, C.byref(c)))
+        self._host_jobs.pop(0)
+        return int(c.value)
+
     # ---- timing ----
     def record(self, slot: int):
         _check(load_library().chq_event_record(self._h, slot))
@@ -351,6 +374,12 @@ class Mesh:
     def elapsed_ms(self, a: int, b: int) -> float:
         v = C.c_float()
         _check(load_library().chq_event_elapsed(self._h, a, b, C.byref(v)))
+        return float(v.value)
+
+    def elapsed_ms_to(self, a: int, other: "Mesh", b: int) -> float:
+        """device time from this mesh's slot a to the other mesh's slot b"""
+        v = C.c_float()
+        _check(load_library().chq_event_elapsed_between(self._h, a, other._h, b, C.byref(v)))
         return float(v.value)
 
     def kernel_launches(self) -> int:

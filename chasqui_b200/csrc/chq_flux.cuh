@@ -107,7 +107,6 @@ CHQ_D void cell_states_from(const FluxArgs<P> &A, const DirView<P> &V, int lc, P
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
       P q5[5];
-#pragma unroll
       ld(n, q5);
 #pragma unroll
       for (int m = RE + 1; m <= 2; ++m) { q5[2 + m] = q5[2 + RE]; q5[2 - m] = q5[2 - RE]; }
@@ -124,7 +123,6 @@ CHQ_D void cell_states_from(const FluxArgs<P> &A, const DirView<P> &V, int lc, P
     P q[7][5];
 #pragma unroll
     for (int n = 0; n < 7; ++n) {
-#pragma unroll
       ld(n, q[n]);
 #pragma unroll
       for (int m = RE + 1; m <= 2; ++m) { q[n][2 + m] = q[n][2 + RE]; q[n][2 - m] = q[n][2 - RE]; }
@@ -164,7 +162,6 @@ CHQ_D void cell_states_from(const FluxArgs<P> &A, const DirView<P> &V, int lc, P
     }
     // entropy scalar, always primitive
     P q5[5];
-#pragma unroll
     ld(7, q5);
 #pragma unroll
     for (int m = RE + 1; m <= 2; ++m) { q5[2 + m] = q5[2 + RE]; q5[2 - m] = q5[2 - RE]; }

@@ -251,7 +251,9 @@ template <class P> __global__ void __launch_bounds__(256) cooling_kernel(const C
 
 // ---------------------------------------------------------------------------------------
 // FOFC flag of the tentative state (src/fofc.hpp:17-43): rho <= dfloor or p <= pfloor,
-// written for every active cell, with a warp-aggregated count into *nbad.
+// written for every active cell, with a warp-aggregated count into *nbad. The flagged cells'
+// linear indices are also appended to `list` (the first `cap` of them), so that the repair
+// visits only their faces.
 struct FlagArgs {
   Geom g;
   EOSp eos;
@@ -259,6 +261,8 @@ struct FlagArgs {
   int *flag;
   int *nbad;
   const int *done;
+  int *list;
+  int cap;
 };
 
 CHQ_D void fofc_flag_body(const FlagArgs &A, int bx, int by, int bz) {
@@ -287,15 +291,26 @@ CHQ_D void fofc_flag_body(const FlagArgs &A, int bx, int by, int bz) {
     bad = b ? 1 : 0;
     A.flag[l] = bad;
   }
+  // blockDim.x == 32: the lane is threadIdx.x
   const unsigned m = __ballot_sync(0xffffffffu, bad != 0);
-  if (m && (threadIdx.x & 31) == 0) atomicAdd(A.nbad, __popc(m));
+  if (m) {
+    int base = 0;
+    if (threadIdx.x == 0) base = atomicAdd(A.nbad, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (bad && A.list) {
+      const int pos = base + __popc(m & ((1u << threadIdx.x) - 1u));
+      if (pos < A.cap) A.list[pos] = g.idx32(k, j, i);
+    }
+  }
 }
 
 __global__ void __launch_bounds__(256) fofc_flag_kernel(const FlagArgs A) { fofc_flag_body(A, blockIdx.x, blockIdx.y, blockIdx.z); }
 
 // ---------------------------------------------------------------------------------------
 // FOFC repair: first-order (donor cell) HLLE fluxes on faces touching a flagged cell,
-// from the stage-start primitives (src/fofc.hpp:46-95). One launch, all directions.
+// from the stage-start primitives (src/fofc.hpp:46-95). One launch, all directions. With
+// the flag kernel's cell list (count *need <= cap) the launch visits the six faces of each
+// listed cell only; otherwise it scans every face, as the reference's loop does.
 template <class P> struct RepairArgs {
   Geom g;
   EOSp eos;
@@ -309,6 +324,8 @@ template <class P> struct RepairArgs {
   const int *need;
   int has_diff;             // re-add the diffusive fluxes on repaired active faces
   DiffArgs<P> diff;
+  const int *list;          // flagged cells (linear indices) of this stage, or null
+  int cap;                  // list capacity
 };
 
 template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k, int j, int i) {
@@ -349,28 +366,60 @@ template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k
   }
 }
 
-template <class P> CHQ_D void fofc_repair_body(const RepairArgs<P> &A, int bx) {
+template <class P> CHQ_D void repair_in_range(const RepairArgs<P> &A, int d, int k, int j, int i) {
+  if (k < A.lo[d][0] || k > A.hi[d][0] || j < A.lo[d][1] || j > A.hi[d][1] || i < A.lo[d][2] || i > A.hi[d][2]) return;
+  if (d == 0) repair_face<0, P>(A, k, j, i);
+  else if (d == 1) repair_face<1, P>(A, k, j, i);
+  else repair_face<2, P>(A, k, j, i);
+}
+
+// block bx of nbx blocks (grid-stride over the work)
+template <class P> CHQ_D void fofc_repair_body(const RepairArgs<P> &A, int bx, int nbx) {
   if (A.done && *A.done) return;
-  if (A.need && *A.need == 0) return;
-  int t = bx * (int)blockDim.x + (int)threadIdx.x;
-#pragma unroll
+  const int nb = A.need ? *A.need : -1;
+  if (nb == 0) return;
+  const int tid = bx * (int)blockDim.x + (int)threadIdx.x, nth = nbx * (int)blockDim.x;
+  const Geom &g = A.g;
+  if (A.list && nb > 0 && nb <= A.cap) {
+    // item = 6 * cell + 2 * direction + side. A face between two flagged cells belongs to the
+    // upper cell's low side only, so every face is written once (the diffusive flux is added
+    // to the repaired one, which must not happen twice).
+    const int sj = (int)g.sj, sk = (int)g.sk;
+    for (int it = tid; it < 6 * nb; it += nth) {
+      const int q = it / 6, f = it - 6 * q, d = f >> 1;
+      if (A.nface[d] == 0) continue;
+      const int c = A.list[q];
+      int k = c / sk;
+      const int r = c - k * sk;
+      int j = r / sj;
+      int i = r - j * sj;
+      if (f & 1) {
+        const int kn = k + (d == 2), jn = j + (d == 1), in = i + (d == 0);
+        if (in <= g.ie && jn <= g.je && kn <= g.ke && A.flag[g.idx32(kn, jn, in)]) continue;
+        k = kn;
+        j = jn;
+        i = in;
+      }
+      repair_in_range<P>(A, d, k, j, i);
+    }
+    return;
+  }
+#pragma unroll 1
   for (int d = 0; d < 3; ++d) {
-    if (t < A.nface[d]) {
-      const int ni = A.hi[d][2] - A.lo[d][2] + 1, nj = A.hi[d][1] - A.lo[d][1] + 1;
+    const int ni = A.hi[d][2] - A.lo[d][2] + 1, nj = A.hi[d][1] - A.lo[d][1] + 1;
+    for (long t = tid; t < A.nface[d]; t += nth) {
       const int i = A.lo[d][2] + (int)(t % ni);
-      const int r = t / ni;
+      const long r = t / ni;
       const int j = A.lo[d][1] + (int)(r % nj);
       const int k = A.lo[d][0] + (int)(r / nj);
-      if (d == 0) repair_face<0, P>(A, k, j, i);
-      else if (d == 1) repair_face<1, P>(A, k, j, i);
-      else repair_face<2, P>(A, k, j, i);
-      return;
+      repair_in_range<P>(A, d, k, j, i);
     }
-    t -= (int)A.nface[d];
   }
 }
 
-template <class P> __global__ void __launch_bounds__(256) fofc_repair_kernel(const RepairArgs<P> A) { fofc_repair_body<P>(A, blockIdx.x); }
+template <class P> __global__ void __launch_bounds__(256) fofc_repair_kernel(const RepairArgs<P> A) {
+  fofc_repair_body<P>(A, blockIdx.x, gridDim.x);
+}
 
 // ---------------------------------------------------------------------------------------
 // Positivity flux limiter (Hu, Adams & Shu 2013) on the active faces of each direction.
@@ -703,7 +752,7 @@ template <class P> __global__ void __launch_bounds__(256) fofc_repair_batched(co
   const int j = batch_job(slots, n, blockIdx.x);
   __shared__ __align__(16) unsigned char sa[sizeof(RepairArgs<P>)];
   const RepairArgs<P> &A = stage_args(args, j, sa);
-  fofc_repair_body<P>(A, (int)(blockIdx.x - slots[j].off));
+  fofc_repair_body<P>(A, (int)(blockIdx.x - slots[j].off), slots[j].gx);
 }
 template <class P> __global__ void __launch_bounds__(256) limit_batched(const LimitArgs<P> *args, const BatchSlot *slots, int n) {
   const int j = batch_job(slots, n, blockIdx.x);

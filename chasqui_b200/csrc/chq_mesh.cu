@@ -181,6 +181,14 @@ struct chq_mesh {
   double *bf[2][3];
   void *w, *bcc, *ecc, *flx[3], *et2[3], *et1[3], *e[3];
   int *flag;
+  // chq_run_host_async jobs: uploads on up_stream, at most two in flight (oldest = hj_head)
+  int device = 0;                          // the device the mesh was created on
+  cudaStream_t up_stream = nullptr, down_stream = nullptr;   // the device's shared copy lanes
+  cudaEvent_t up_ready = nullptr, prev_done = nullptr, hj_evt[2] = {nullptr, nullptr};
+  void *hj_clk[2] = {nullptr, nullptr};   // pinned copies of the clock after each job's cycles
+  int hj_head = 0, hj_count = 0;
+  int *bad_list;   // this stage's flagged cells (first bad_cap), filled by the flag kernel
+  int bad_cap;     // kBadCap; CHQ_FOFC_LIST_CAP in the environment lowers it (0: always scan)
   StepCtl *ctl;            // device
   double *hst_part, *hst_out;
   int hst_blocks;
@@ -208,7 +216,10 @@ struct chq_mesh {
   };
   char *snap = nullptr;
   size_t snap_bytes = 0;
-  double *stage_buf = nullptr;   // upload staging (packed host layout), allocated on first upload
+  double *stage_buf = nullptr;   // four upload staging slots (packed host layout), allocated on first upload
+  cudaEvent_t stage_copied[4] = {}, stage_unpacked[4] = {};
+  unsigned long long stage_seq = 0;   // chunks staged so far (slot = seq % 4)
+  cudaStream_t unpack_stream = nullptr;   // the device's shared unpack lane (host jobs)
   // whole-cycle CUDA graph of chq_cycles on the mesh stream (built after one plain cycle)
   cudaGraph_t cyc_graph = nullptr;
   cudaGraphExec_t cyc_exec = nullptr;
@@ -232,6 +243,9 @@ struct chq_mesh {
 namespace {
 
 const int kHstBlocks = 1184;   // 8 blocks per SM on 148 SMs
+const size_t kBadCap = 1 << 16;            // flagged cells listed per stage
+const long kRepairBlocks = 1184;           // repair grid of one mesh
+const long kRepairBlocksBatched = 148;     // repair blocks per mesh of a batch
 
 // bytes of one mesh slab: 18 double fields (u0, u1, 6 face fields), 39 fields of the
 // primitive type, the int flags, the control block and the history scratch
@@ -239,8 +253,8 @@ size_t slab_size(size_t nel, size_t psize, bool sts) {
   auto up = [](size_t x) { return (x + 255) / 256 * 256; };
   // RKL2: 5 cell arrays of 6 components and 5 x 3 face fields, all double
   const size_t sts_fields = sts ? 45 : 0;
-  return nel * sizeof(double) * (18 + sts_fields) + nel * psize * 39 + up(nel * sizeof(int)) + up(sizeof(StepCtl)) +
-         up((size_t)(kHstBlocks * 10 + 16) * sizeof(double));
+  return nel * sizeof(double) * (18 + sts_fields) + nel * psize * 39 + up(nel * sizeof(int)) +
+         up(kBadCap * sizeof(int)) + up(sizeof(StepCtl)) + up((size_t)(kHstBlocks * 10 + 16) * sizeof(double));
 }
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -459,6 +473,8 @@ FlagArgs flag_args(chq_mesh *m, int buf, int *nbad_dev, const int *done) {
   a.flag = m->flag;
   a.nbad = nbad_dev;
   a.done = done;
+  a.list = m->bad_list;
+  a.cap = m->bad_cap;
   return a;
 }
 
@@ -497,7 +513,15 @@ RepairArgs<P> repair_args(chq_mesh *m, int cur, unsigned dirmask, const int *don
   a.flag = m->flag;
   a.done = done;
   a.need = need;
+  a.list = m->bad_list;
+  a.cap = m->bad_cap;
   return a;
+}
+
+// repair grid: grid-stride, at most kRepairBlocks blocks of 256 (a listed repair touches a
+// few faces; the full scan is the rare fallback)
+Launch3 repair_grid(long faces, long max_blocks) {
+  return {dim3((unsigned)std::max(1L, std::min((faces + 255) / 256, max_blocks))), dim3(256)};
 }
 
 template <class P>
@@ -506,7 +530,7 @@ int do_repair(chq_mesh *m, int cur, unsigned dirmask, const int *done, const int
   const RepairArgs<P> a = repair_args<P>(m, cur, dirmask, done, need, tot);
   if (tot == 0) return CHQ_OK;
   m->nlaunch += 1;
-  fofc_repair_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
+  fofc_repair_kernel<P><<<repair_grid(tot, kRepairBlocks).grid, 256, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
@@ -753,7 +777,7 @@ int do_repair_d(chq_mesh *m, int cur, bool with_diff, const int *done, const int
     a.diff = diff_args<P>(m, m->bf[cur][0], m->bf[cur][1], m->bf[cur][2], done, nd);
   }
   m->nlaunch += 1;
-  fofc_repair_kernel<P><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a);
+  fofc_repair_kernel<P><<<repair_grid(tot, kRepairBlocks).grid, 256, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
@@ -983,31 +1007,79 @@ __global__ void __launch_bounds__(256) unpack_planes_kernel(const double *src, d
   }
 }
 
-const size_t kStageBytes = 64ull << 20;   // planes per chunk: as many as fit in 64 MB
+// The device frame -> packed host planes of ncomp components (the inverse of the unpack):
+// downloads of contiguous packed data run at the link's full rate.
+template <class T>
+__global__ void __launch_bounds__(256) pack_planes_kernel(const T *src, T *dst, int ncomp, int nx, int ny, int nz,
+                                                          long sj, long sk, long vstride) {
+  const long plane3 = (long)nx * ny * nz, total = plane3 * ncomp;
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(q / plane3);
+    const long r0 = q - c * plane3;
+    const int i = (int)(r0 % nx);
+    const long r = r0 / nx;
+    const int j = (int)(r % ny);
+    const int k = (int)(r / ny);
+    dst[q] = src[c * vstride + (long)k * sk + (long)j * sj + i];
+  }
+}
 
-// upload of one double component in plane chunks: copy (stream order) -> unpack -> next copy
+const size_t kStageBytes = 64ull << 20;   // per staging slot; planes per chunk: as many as fit
+const int kStageSlots = 4;
+
+// make s wait until every staging slot's last unpack (and so its copy) is done
+int stage_fence(chq_mesh *m, cudaStream_t s) {
+  for (int q = 0; q < kStageSlots; ++q)
+    if (m->stage_unpacked[q]) CHQ_CUDA(cudaStreamWaitEvent(s, m->stage_unpacked[q], 0));
+  return CHQ_OK;
+}
+
+
+// Upload of one double component in plane chunks through kStageSlots staging slots: copy
+// chunk c into slot c % kStageSlots, unpack it, and copy the next chunks into the other slots
+// meanwhile. On the host-job upload lane the copies run on s and the unpacks on the unpack
+// lane, so the link does not wait while an unpack kernel waits for SMs that a running cycle
+// holds; on any other stream both run on s.
 int upload_staged(chq_mesh *m, char *dev, const double *hst, int nx, int ny, int nz, cudaStream_t s) {
   const Geom &g = m->g;
   if (!m->stage_buf) {
-    const cudaError_t e = cudaMalloc(&m->stage_buf, kStageBytes);
+    cudaError_t e = cudaMalloc(&m->stage_buf, kStageSlots * kStageBytes);
     if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("upload staging: ") + cudaGetErrorString(e));
+    for (int q = 0; q < kStageSlots && e == cudaSuccess; ++q) {
+      e = cudaEventCreateWithFlags(&m->stage_copied[q], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->stage_unpacked[q], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "upload staging events");
+  }
+  const bool lane = m->up_stream && s == m->up_stream;
+  cudaStream_t us = lane ? m->unpack_stream : s;
+  if (!lane) {
+    const int rc = stage_fence(m, s);   // a queued host job may still be uploading through the slots
+    if (rc) return rc;
   }
   const size_t plane = (size_t)nx * ny;   // plane * sizeof(double) <= kStageBytes (caller)
   const int per = (int)(kStageBytes / (plane * sizeof(double)));
   for (int k0 = 0; k0 < nz; k0 += per) {
     const int nzc = std::min(per, nz - k0);
-    CHQ_CUDA(cudaMemcpyAsync(m->stage_buf, hst + (size_t)k0 * plane, (size_t)nzc * plane * sizeof(double),
+    const int slot = (int)(m->stage_seq++ % kStageSlots);
+    double *buf = m->stage_buf + (size_t)slot * (kStageBytes / sizeof(double));
+    CHQ_CUDA(cudaStreamWaitEvent(s, m->stage_unpacked[slot], 0));   // the slot's last unpack is done
+    CHQ_CUDA(cudaMemcpyAsync(buf, hst + (size_t)k0 * plane, (size_t)nzc * plane * sizeof(double),
                              cudaMemcpyHostToDevice, s));
+    CHQ_CUDA(cudaEventRecord(m->stage_copied[slot], s));
+    CHQ_CUDA(cudaStreamWaitEvent(us, m->stage_copied[slot], 0));
     const long tot = (long)nzc * plane;
     const unsigned blocks = (unsigned)std::min<long>((tot + 255) / 256, 148L * 16);
     m->nlaunch += 1;
-    unpack_planes_kernel<<<blocks, 256, 0, s>>>(m->stage_buf, reinterpret_cast<double *>(dev), nx, ny, nzc, g.sj, g.sk, k0);
+    unpack_planes_kernel<<<blocks, 256, 0, us>>>(buf, reinterpret_cast<double *>(dev), nx, ny, nzc, g.sj, g.sk, k0);
     CHQ_CUDA(cudaGetLastError());
+    CHQ_CUDA(cudaEventRecord(m->stage_unpacked[slot], us));
   }
   return CHQ_OK;
 }
 
-int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaStream_t s) {
+// sync = false: leave the copies queued on s (double fields only; no host conversion)
+int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaStream_t s, bool sync = true) {
   FieldRef f;
   if (!field_by_name(m, name, f)) return fail(CHQ_ERR_ARG, std::string("unknown field: ") + name);
   if (field_size(m, f) != n) return fail(CHQ_ERR_ARG, std::string("size mismatch for field ") + name);
@@ -1017,6 +1089,8 @@ int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaS
   // stage through a host buffer of the device element type when it is not double
   std::vector<unsigned char> tmp;
   void *hptr = host;
+  if (!sync && (es != sizeof(double) || f.isint))
+    return fail(CHQ_ERR_ARG, std::string("field ") + name + " needs a host conversion; it cannot be queued");
   if (es != sizeof(double) || f.isint) {
     tmp.resize((size_t)n * es);
     hptr = tmp.data();
@@ -1044,6 +1118,7 @@ int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaS
     else { p.srcPtr = dp; p.dstPtr = hp; p.kind = cudaMemcpyDeviceToHost; }
     CHQ_CUDA(cudaMemcpy3DAsync(&p, s));
   }
+  if (!sync) return CHQ_OK;
   CHQ_CUDA(cudaStreamSynchronize(s));
   if (!up && hptr != host) {
     for (long q = 0; q < n; ++q) {
@@ -1137,7 +1212,7 @@ int batch_build(chq_batch *B) {
   o_repair_s = slots_of(h, J, [](chq_mesh *m) {
     long tot = 0;
     repair_args<P>(m, 0, 7u, nullptr, nullptr, tot);
-    return linear(tot, 256);
+    return repair_grid(tot, kRepairBlocksBatched);
   }, B->k_repair.nblocks);
   o_limit_s = slots_of(h, J, [](chq_mesh *m) {
     long tot = 0;
@@ -1350,6 +1425,7 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   if (c.nu < 0 || c.kappa < 0 || c.eta < 0) return fail(CHQ_ERR_ARG, "diffusion coefficients must be >= 0");
 
   chq_mesh *m = new chq_mesh;
+  cudaGetDevice(&m->device);
   m->cfg = c;
   m->cfg.nghost = ng;
   Geom &g = m->g;
@@ -1438,6 +1514,9 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   for (int d = 0; d < 3; ++d) { m->et2[d] = p; p += pbytes; m->et1[d] = p; p += pbytes; }
   for (int d = 0; d < 3; ++d) { m->e[d] = p; p += pbytes; }
   m->flag = (int *)p; p += ibytes;
+  m->bad_list = (int *)p; p += align_up(kBadCap * sizeof(int), 256);
+  m->bad_cap = (int)kBadCap;
+  if (const char *cap = std::getenv("CHQ_FOFC_LIST_CAP")) m->bad_cap = std::max(0, std::min(std::atoi(cap), (int)kBadCap));
   m->ctl = (StepCtl *)p; p += ctl_bytes;
   m->hst_part = (double *)p;
   m->hst_out = m->hst_part + (size_t)m->hst_blocks * 10;
@@ -1491,6 +1570,18 @@ int chq_mesh_destroy(chq_mesh *m) {
   if (!m) return CHQ_OK;
   if (m->batch_evt) cudaEventSynchronize(m->batch_evt);
   if (m->stream) cudaStreamSynchronize(m->stream);
+  // (the copy lanes are shared by the device's meshes and stay; wait for this mesh's copies)
+  if (m->up_stream) cudaStreamSynchronize(m->up_stream);
+  if (m->unpack_stream) cudaStreamSynchronize(m->unpack_stream);
+  if (m->down_stream) cudaStreamSynchronize(m->down_stream);
+  for (int q = 0; q < 4; ++q) {
+    if (m->stage_copied[q]) cudaEventDestroy(m->stage_copied[q]);
+    if (m->stage_unpacked[q]) cudaEventDestroy(m->stage_unpacked[q]);
+  }
+  for (cudaEvent_t e : {m->up_ready, m->prev_done, m->hj_evt[0], m->hj_evt[1]})
+    if (e) cudaEventDestroy(e);
+  for (void *p : m->hj_clk)
+    if (p) cudaFreeHost(p);
   if (m->snap_stream) {
     cudaStreamSynchronize(m->snap_stream);
     cudaStreamDestroy(m->snap_stream);
@@ -1603,10 +1694,13 @@ int chq_snapshot_wait(chq_mesh *m) {
   return CHQ_OK;
 }
 
-int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *const *host, const long *n) {
-  if (!m || nfields < 1 || !names || !host || !n) return fail(CHQ_ERR_ARG, "bad argument");
-  int rc = chq_snapshot_wait(m);
-  if (rc) return rc;
+namespace {
+// Packs the named fields into the snapshot area in the host layout (a device-side copy
+// behind the work queued on the mesh stream, once the previous snapshot's download has left
+// the area), then downloads each with one linear copy on `down` (the snapshot stream when
+// null); `items` describes the copies.
+int snapshot_enqueue(chq_mesh *m, int nfields, const char *const *names, double *const *host, const long *n,
+                     std::vector<chq_mesh::SnapItem> &items, cudaStream_t down) {
   const Geom &g = m->g;
   std::vector<FieldRef> fr(nfields);
   size_t need = 0;
@@ -1614,7 +1708,9 @@ int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *con
     if (!names[q] || !host[q] || !field_by_name(m, names[q], fr[q]))
       return fail(CHQ_ERR_ARG, std::string("unknown field: ") + (names[q] ? names[q] : "(null)"));
     if (field_size(m, fr[q]) != n[q]) return fail(CHQ_ERR_ARG, std::string("size mismatch for field ") + names[q]);
-    need += align_up((size_t)fr[q].ncomp * g.vstride * field_esize(m, fr[q]), 256);
+    const FieldRef &f = fr[q];
+    const size_t nx = f.face ? g.ni + 1 : g.ni, ny = f.face ? g.nj + 1 : g.nj, nz = f.face ? g.nk + 1 : g.nk;
+    need += align_up((size_t)f.ncomp * nx * ny * nz * field_esize(m, f), 256);
   }
   if (!m->snap_stream) {
     CHQ_CUDA(cudaStreamCreateWithFlags(&m->snap_stream, cudaStreamNonBlocking));
@@ -1622,6 +1718,7 @@ int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *con
     CHQ_CUDA(cudaEventCreateWithFlags(&m->snap_landed, cudaEventDisableTiming));
   }
   if (need > m->snap_bytes) {
+    // (cudaFree waits for the device, so no download still reads the old area)
     if (m->snap) CHQ_CUDA(cudaFree(m->snap));
     m->snap = nullptr;
     m->snap_bytes = 0;
@@ -1630,34 +1727,46 @@ int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *con
     m->snap_bytes = need;
   }
   cudaStream_t s = S(m, nullptr);
+  CHQ_CUDA(cudaStreamWaitEvent(s, m->snap_landed, 0));   // the previous download has left the area
   char *p = m->snap;
-  m->snap_items.clear();
+  items.clear();
   for (int q = 0; q < nfields; ++q) {
+    // packed into the snapshot area in the host layout
     const FieldRef &f = fr[q];
-    const size_t es = field_esize(m, f), bytes = (size_t)f.ncomp * g.vstride * es;
-    CHQ_CUDA(cudaMemcpyAsync(p, f.base, bytes, cudaMemcpyDeviceToDevice, s));
+    const int nx = f.face ? g.ni + 1 : g.ni, ny = f.face ? g.nj + 1 : g.nj, nz = f.face ? g.nk + 1 : g.nk;
+    const size_t es = field_esize(m, f), bytes = (size_t)f.ncomp * nx * ny * nz * es;
+    const long tot = (long)f.ncomp * nx * ny * nz;
+    const unsigned blocks = (unsigned)std::max(1L, std::min<long>((tot + 255) / 256, 148L * 16));
+    m->nlaunch += 1;
+    if (es == 8)
+      pack_planes_kernel<unsigned long long><<<blocks, 256, 0, s>>>(static_cast<const unsigned long long *>(f.base),
+          reinterpret_cast<unsigned long long *>(p), f.ncomp, nx, ny, nz, g.sj, g.sk, g.vstride);
+    else
+      pack_planes_kernel<unsigned><<<blocks, 256, 0, s>>>(static_cast<const unsigned *>(f.base),
+          reinterpret_cast<unsigned *>(p), f.ncomp, nx, ny, nz, g.sj, g.sk, g.vstride);
+    CHQ_CUDA(cudaGetLastError());
     chq_mesh::SnapItem it{host[q], n[q], f.ncomp, f.face, es, f.isint, p, {}};
     if (es != sizeof(double) || f.isint) it.tmp.resize((size_t)n[q] * es);
-    m->snap_items.push_back(std::move(it));
+    items.push_back(std::move(it));
     p += align_up(bytes, 256);
   }
+  if (!down) down = m->snap_stream;
   CHQ_CUDA(cudaEventRecord(m->snap_taken, s));
-  CHQ_CUDA(cudaStreamWaitEvent(m->snap_stream, m->snap_taken, 0));
-  for (auto &it : m->snap_items) {
-    const int nx = it.face ? g.ni + 1 : g.ni, ny = it.face ? g.nj + 1 : g.nj, nz = it.face ? g.nk + 1 : g.nk;
+  CHQ_CUDA(cudaStreamWaitEvent(down, m->snap_taken, 0));
+  for (auto &it : items) {
     void *hbase = it.tmp.empty() ? (void *)it.host : (void *)it.tmp.data();
-    for (int c = 0; c < it.ncomp; ++c) {
-      cudaMemcpy3DParms cp{};
-      char *dev = it.copy + (size_t)c * g.vstride * it.es;
-      char *hst = static_cast<char *>(hbase) + (size_t)c * nx * ny * nz * it.es;
-      cp.srcPtr = make_cudaPitchedPtr(dev, (size_t)g.sj * it.es, (size_t)nx * it.es, (size_t)(g.nj + 1));
-      cp.dstPtr = make_cudaPitchedPtr(hst, (size_t)nx * it.es, (size_t)nx * it.es, (size_t)ny);
-      cp.extent = make_cudaExtent((size_t)nx * it.es, (size_t)ny, (size_t)nz);
-      cp.kind = cudaMemcpyDeviceToHost;
-      CHQ_CUDA(cudaMemcpy3DAsync(&cp, m->snap_stream));
-    }
+    CHQ_CUDA(cudaMemcpyAsync(hbase, it.copy, (size_t)it.n * it.es, cudaMemcpyDeviceToHost, down));
   }
-  CHQ_CUDA(cudaEventRecord(m->snap_landed, m->snap_stream));
+  CHQ_CUDA(cudaEventRecord(m->snap_landed, down));
+  return CHQ_OK;
+}
+}  // namespace
+
+int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *const *host, const long *n) {
+  if (!m || nfields < 1 || !names || !host || !n) return fail(CHQ_ERR_ARG, "bad argument");
+  int rc = chq_snapshot_wait(m);
+  if (rc) return rc;
+  if ((rc = snapshot_enqueue(m, nfields, names, host, n, m->snap_items, nullptr))) return rc;
   m->snap_pending = true;
   return CHQ_OK;
 }
@@ -1979,6 +2088,113 @@ int chq_run_host(chq_mesh *m, double *u, double *b1, double *b2, double *b3, int
   return done_cycles;
 }
 
+namespace {
+// Host jobs of all meshes on a device take turns, in submission order, on three lanes: one
+// upload stream, the SMs (a job's cycles start after the previous job's cycles ended) and
+// one download stream. Jobs on several meshes then never upload, compute or download all at
+// once (which leaves the SMs idle while everything uploads), and one job's copies overlap
+// another's cycles. The upload stream has the highest priority: its unpack kernels get SMs
+// as soon as blocks of a running cycle retire. Lanes live as long as the process.
+struct CopyLanes {
+  cudaStream_t up = nullptr, unpack = nullptr, down = nullptr;
+  cudaEvent_t computed = nullptr;   // recorded after the last queued host job's cycles
+};
+std::mutex g_lanes_mu;
+CopyLanes g_lanes[64];
+
+int copy_lanes(int device, CopyLanes &out) {
+  if (device < 0 || device >= 64) return fail(CHQ_ERR_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_lanes_mu);
+  CopyLanes &l = g_lanes[device];
+  if (!l.up) {
+    int least = 0, greatest = 0;
+    CHQ_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CHQ_CUDA(cudaStreamCreateWithPriority(&l.up, cudaStreamNonBlocking, greatest));
+    CHQ_CUDA(cudaStreamCreateWithPriority(&l.unpack, cudaStreamNonBlocking, greatest));
+    CHQ_CUDA(cudaStreamCreateWithFlags(&l.down, cudaStreamNonBlocking));
+    CHQ_CUDA(cudaEventCreateWithFlags(&l.computed, cudaEventDisableTiming));
+  }
+  out = l;
+  return CHQ_OK;
+}
+
+// page-locked (cudaHostAlloc / cudaHostRegister) host memory: copies from it are asynchronous
+bool page_locked(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+}  // namespace
+
+int chq_run_host_async(chq_mesh *m, double *u, double *b1, double *b2, double *b3, int ncycles, double t0) {
+  if (!m || !u || !b1 || !b2 || !b3 || ncycles < 0) return fail(CHQ_ERR_ARG, "bad argument");
+  if (m->hj_count == 2) return fail(CHQ_ERR_STATE, "two host jobs in flight on this mesh: call chq_run_host_wait first");
+  for (const double *p : {u, b1, b2, b3})
+    if (!page_locked(p)) return fail(CHQ_ERR_ARG, "chq_run_host_async needs page-locked host arrays (chq_host_alloc)");
+  if (!m->up_stream) {
+    CopyLanes l;
+    const int rc0 = copy_lanes(m->device, l);
+    if (rc0) return rc0;
+    m->up_stream = l.up;
+    m->unpack_stream = l.unpack;
+    m->down_stream = l.down;
+    CHQ_CUDA(cudaEventCreateWithFlags(&m->up_ready, cudaEventDisableTiming));
+    CHQ_CUDA(cudaEventCreateWithFlags(&m->prev_done, cudaEventDisableTiming));
+    for (int q = 0; q < 2; ++q) {
+      CHQ_CUDA(cudaEventCreateWithFlags(&m->hj_evt[q], cudaEventDisableTiming));
+      CHQ_CUDA(cudaHostAlloc(&m->hj_clk[q], sizeof(StepCtl), cudaHostAllocDefault));
+    }
+  }
+  cudaStream_t s = m->stream;
+  int rc;
+  double *const arr[4] = {u, b1, b2, b3};
+  const char *const names[4] = {"u0", "b1f0", "b2f0", "b3f0"};
+  long sizes[4];
+  for (int q = 0; q < 4; ++q) sizes[q] = chq_array_size(m, names[q]);
+  // the upload waits for everything queued before it on the mesh stream (the previous job's
+  // cycles and its copy into the snapshot area), not for that job's download
+  CHQ_CUDA(cudaEventRecord(m->prev_done, s));
+  CHQ_CUDA(cudaStreamWaitEvent(m->up_stream, m->prev_done, 0));
+  for (int q = 0; q < 4; ++q)
+    if ((rc = transfer(m, names[q], arr[q], sizes[q], true, m->up_stream, false))) return rc;
+  if ((rc = stage_fence(m, m->up_stream))) return rc;   // up_ready then covers the unpacks
+  CHQ_CUDA(cudaEventRecord(m->up_ready, m->up_stream));
+  CHQ_CUDA(cudaStreamWaitEvent(s, m->up_ready, 0));
+  CopyLanes l;
+  if ((rc = copy_lanes(m->device, l))) return rc;
+  {
+    // the SM lane: after the previous host job's cycles (on any mesh of the device)
+    std::lock_guard<std::mutex> lock(g_lanes_mu);
+    CHQ_CUDA(cudaStreamWaitEvent(s, l.computed, 0));
+    if ((rc = chq_prime(m, t0, s))) return rc;
+    if ((rc = chq_cycles(m, ncycles, s))) return rc;
+    CHQ_CUDA(cudaEventRecord(l.computed, s));
+  }
+  const int slot = (m->hj_head + m->hj_count) & 1;
+  CHQ_CUDA(cudaMemcpyAsync(m->hj_clk[slot], m->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s));
+  std::vector<chq_mesh::SnapItem> items;
+  if ((rc = snapshot_enqueue(m, 4, names, arr, sizes, items, m->down_stream))) return rc;
+  CHQ_CUDA(cudaEventRecord(m->hj_evt[slot], m->down_stream));
+  ++m->hj_count;
+  return CHQ_OK;
+}
+
+int chq_run_host_wait(chq_mesh *m, int *cycles) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  if (m->hj_count == 0) return fail(CHQ_ERR_STATE, "no host job in flight on this mesh");
+  const int slot = m->hj_head;
+  m->hj_head ^= 1;
+  --m->hj_count;
+  // the clock copy precedes the job's snapshot copy on the mesh stream, which precedes its
+  // download on the snapshot stream
+  CHQ_CUDA(cudaEventSynchronize(m->hj_evt[slot]));
+  if (cycles) *cycles = static_cast<const StepCtl *>(m->hj_clk[slot])->cycle;
+  return CHQ_OK;
+}
+
 int chq_set_device(int device) {
   CHQ_CUDA(cudaSetDevice(device));
   return CHQ_OK;
@@ -2006,6 +2222,14 @@ int chq_event_record(chq_mesh *m, int slot) {
   if (!m || slot < 0 || slot >= 8) return fail(CHQ_ERR_ARG, "bad argument");
   if (!m->slots[slot]) CHQ_CUDA(cudaEventCreate(&m->slots[slot]));
   CHQ_CUDA(cudaEventRecord(m->slots[slot], S(m, nullptr)));
+  return CHQ_OK;
+}
+
+int chq_event_elapsed_between(chq_mesh *ma, int a, chq_mesh *mb, int b, float *ms) {
+  if (!ma || !mb || !ms || a < 0 || a >= 8 || b < 0 || b >= 8 || !ma->slots[a] || !mb->slots[b])
+    return fail(CHQ_ERR_ARG, "bad argument");
+  CHQ_CUDA(cudaEventSynchronize(mb->slots[b]));
+  CHQ_CUDA(cudaEventElapsedTime(ms, ma->slots[a], mb->slots[b]));
   return CHQ_OK;
 }
 

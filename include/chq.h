@@ -94,8 +94,9 @@ CHQ_API int chq_upload(chq_mesh *m, const char *name, const double *host, long n
 CHQ_API int chq_download(chq_mesh *m, const char *name, double *host, long n, void *stream);
 /* Output snapshot that does not stall the stepping (no reference counterpart: the reference
  * writes outputs between cycles with a synchronous copy, src/output.hpp, src/restart.hpp).
- * Copies the named fields (any chq_download name) device-to-device into a snapshot area
- * behind the work queued on the mesh stream, then downloads them on a separate stream into
+ * Packs the named fields (any chq_download name) on the device into a snapshot area in the
+ * reference layout behind the work queued on the mesh stream, then downloads them on a
+ * separate stream into
  * host[q] (n[q] doubles each, the reference layout) while later cycles run. Host buffers
  * from chq_host_alloc make the download asynchronous; pageable ones work but may block.
  * The host buffers must stay untouched until chq_snapshot_wait returns. One snapshot per
@@ -163,6 +164,15 @@ CHQ_API int chq_history(chq_mesh *m, double out[10], void *stream);
  * and download the result state into the same host arrays. Returns the cycles done. */
 CHQ_API int chq_run_host(chq_mesh *m, double *u, double *b1, double *b2, double *b3, int ncycles, double t0,
                  void *stream);
+/* The same job queued without waiting: returns once the upload, priming, cycles and download
+ * are queued. The host arrays must be page-locked (chq_host_alloc) and stay untouched until
+ * the chq_run_host_wait() that returns this job. Up to two host jobs per mesh are in flight:
+ * the result leaves through the snapshot area (chq_snapshot), so the next job's upload
+ * overlaps the previous job's download, and jobs on two meshes overlap one job's copies with
+ * the other's cycles. */
+CHQ_API int chq_run_host_async(chq_mesh *m, double *u, double *b1, double *b2, double *b3, int ncycles, double t0);
+/* Waits for the mesh's oldest host job; *cycles (may be NULL) = its cycle count. */
+CHQ_API int chq_run_host_wait(chq_mesh *m, int *cycles);
 
 /* ---- device, host memory and timing utilities (no reference counterpart) ----------------- */
 /* Make `device` current for this host thread's subsequent chq calls and meshes. */
@@ -175,6 +185,8 @@ CHQ_API int chq_host_free(void *ptr);
  * (synchronises on the later one). */
 CHQ_API int chq_event_record(chq_mesh *m, int slot);
 CHQ_API int chq_event_elapsed(chq_mesh *m, int from_slot, int to_slot, float *ms);
+/* elapsed device time from slot a of mesh ma to slot b of mesh mb (events of two streams) */
+CHQ_API int chq_event_elapsed_between(chq_mesh *ma, int a, chq_mesh *mb, int b, float *ms);
 /* Per-kernel CUDA-event timing inside the stage sequence (off by default). Kinds:
  * 0 fluxes (K1), 1 corner EMF (K2), 2 update (K3), 3 FOFC flag, 4 FOFC repair + re-run,
  * 5 boundaries (K4), 6 con2prim + dt (K5), 7 positivity limiter, 8 step control,

@@ -53,6 +53,25 @@ def test_strong_blast_exercises_fofc():
     assert ref.fofc_count > 0, "the case no longer triggers first-order flux corrections"
 
 
+@pytest.mark.parametrize("cap", ["0", "7"])
+def test_fofc_repair_scan_fallback_is_bitwise_equal(monkeypatch, cap):
+    """The repair visits only the faces of the cells the flag kernel listed; when a stage
+    flags more cells than the list holds (here 7, or no list at all) it scans every face as
+    the reference's loop does. Both paths give the same state, bit for bit."""
+    text, ov = CYCLE_CASES["blast3d_strong_fofc"]
+    ref, listed = make_pair(text, ov)
+    monkeypatch.setenv("CHQ_FOFC_LIST_CAP", cap)
+    _, scanned = make_pair(text, ov)
+    for m in (listed, scanned):
+        copy_state(ref, m, FIELDS)
+        m.prime(0.0)
+        m.cycles(10)
+    for f in FIELDS:
+        assert np.array_equal(listed.get(f), scanned.get(f)), f
+    assert listed.counters() == scanned.counters()
+    assert listed.counters()[0] > 7
+
+
 def test_history_matches_reference():
     ref, mesh = make_pair(cases.blast(16), [])
     ref.cycles(5)
@@ -114,6 +133,51 @@ def test_run_host_round_trip():
     ref.cycles(7)
     assert l1_rel(u, ref.get("u0")) <= 1e-12
     assert l1_rel(b1, ref.get("b1f0")) <= 1e-12
+
+
+def test_run_host_async_pipelined_over_two_meshes():
+    """The queued host-buffer call: jobs alternating over two meshes, two in flight on each
+    (a job's upload overlaps the previous one's download), give the blocking call's results
+    bit for bit; a third job on a mesh, pageable arrays and a wait without a job are
+    refused. A snapshot taken between host jobs sees the right state."""
+    from chasqui_b200 import ChqError, Mesh, PinnedArray
+    ref, mesh = make_pair(cases.ot(32), [])
+    other = Mesh(mesh.cfg)
+    names = ("u0", "b1f0", "b2f0", "b3f0")
+    start = [np.ascontiguousarray(ref.get(f)) for f in names]
+    expect = [a.copy() for a in start]
+    assert mesh.run_host(*expect, 5) == 5
+    pins = []
+    for _ in range(8):
+        ps = [PinnedArray(a.shape) for a in start]
+        for p, a in zip(ps, start):
+            p.array[...] = a
+        pins.append([p.array for p in ps])
+    ms = [mesh, other]
+    for q in range(4):
+        ms[q % 2].run_host_async(*pins[q], 5)
+    with pytest.raises(ChqError):
+        mesh.run_host_async(*pins[4], 5)     # two jobs per mesh in flight at most
+    for q in range(4, 8):
+        assert ms[q % 2].run_host_wait() == 5
+        ms[q % 2].run_host_async(*pins[q], 5)
+    for m in ms:
+        assert m.run_host_wait() == 5
+        assert m.run_host_wait() == 5
+    for arrs in pins:
+        for got, want in zip(arrs, expect):
+            assert np.array_equal(got, want)
+    with pytest.raises(ChqError):
+        mesh.run_host_wait()
+    with pytest.raises(ChqError):
+        mesh.run_host_async(*[a.copy() for a in start], 5)   # pageable memory
+    # a public snapshot after queued host jobs: the state of the last job
+    mesh.run_host_async(*pins[0], 2)
+    mesh.snapshot(["u0"])
+    snap = mesh.snapshot_wait()["u0"]
+    assert mesh.run_host_wait() == 2
+    assert np.array_equal(snap, pins[0][0])
+    other.close()
 
 
 @pytest.mark.parametrize("name,tol", [("ot2d_64_ppm_hlld", 1e-4), ("cpaw3d_wenoz_hlld", 1e-4),
