@@ -146,6 +146,13 @@ template <class P> CHQ_D void diff_flux_body(const DiffArgs<P> &A, int bx) {
 
 template <class P> __global__ void __launch_bounds__(256) diff_flux_kernel(const DiffArgs<P> A) { diff_flux_body<P>(A, blockIdx.x); }
 
+template <class P> __global__ void __launch_bounds__(256) diff_flux_batched(const DiffArgs<P> *args, const BatchSlot *slots, int n) {
+  const int j = batch_job(slots, n, blockIdx.x);
+  __shared__ __align__(16) unsigned char sa[sizeof(DiffArgs<P>)];
+  const DiffArgs<P> &A = stage_args(args, j, sa);
+  diff_flux_body<P>(A, (int)(blockIdx.x - slots[j].off));
+}
+
 // eta J added to the edge EMFs (ResistiveEMF); threads over k in [ks, ku], j in [js, ju],
 // i in [is, ie+1] with ku = ke+1 (3D) or ks+1, ju = je+1 (2D) or js+1
 template <class P> struct ResEmfArgs {
@@ -158,13 +165,13 @@ template <class P> struct ResEmfArgs {
   const int *need;   // when set: run only if *need != 0 (the FOFC re-run)
 };
 
-template <class P> __global__ void __launch_bounds__(256) resistive_emf_kernel(const ResEmfArgs<P> A) {
+template <class P> CHQ_D void resistive_emf_body(const ResEmfArgs<P> &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
   if (A.need && *A.need == 0) return;
   const Geom &g = A.g;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   if (i > g.ie + 1 || j > A.ju || k > A.ku) return;
   const long l = g.idx(k, j, i);
   if (i <= g.ie) A.e1[l] = (P)((double)A.e1[l] + A.eta * A.J.J1(l));
@@ -172,18 +179,53 @@ template <class P> __global__ void __launch_bounds__(256) resistive_emf_kernel(c
   if (k <= g.ke || !g.three_d) A.e3[l] = (P)((double)A.e3[l] + A.eta * A.J.J3(l));
 }
 
+template <class P> __global__ void __launch_bounds__(256) resistive_emf_kernel(const ResEmfArgs<P> A) {
+  resistive_emf_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class P> __global__ void __launch_bounds__(256) resistive_emf_batched(const ResEmfArgs<P> *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  __shared__ __align__(16) unsigned char sa[sizeof(ResEmfArgs<P>)];
+  const ResEmfArgs<P> &A = stage_args(args, j, sa);
+  resistive_emf_body<P>(A, bx, by, bz);
+}
+
 // minimum density over the active cells into *bits (atomic min of positive doubles)
-template <class P> __global__ void __launch_bounds__(256) rho_min_kernel(Geom g, const P *w, unsigned long long *bits,
-                                                                          const int *done) {
-  if (done && *done) return;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+template <class P> struct RhoMinArgs {
+  Geom g;
+  const P *w;
+  unsigned long long *bits;
+  const int *done;
+};
+
+template <class P> CHQ_D void rho_min_body(const RhoMinArgs<P> &A, int bx, int by, int bz) {
+  const Geom &g = A.g;
+  const P *w = A.w;
+  unsigned long long *bits = A.bits;
+  if (A.done && *A.done) return;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   double v = __longlong_as_double(0x7ff0000000000000LL);
   if (i <= g.ie && j <= g.je) v = (double)w[g.idx(k, j, i)];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) atomic_min_pos(bits, v);
+}
+
+template <class P> __global__ void __launch_bounds__(256) rho_min_kernel(const RhoMinArgs<P> A) {
+  rho_min_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class P> __global__ void __launch_bounds__(256) rho_min_batched(const RhoMinArgs<P> *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  __shared__ __align__(16) unsigned char sa[sizeof(RhoMinArgs<P>)];
+  const RhoMinArgs<P> &A = stage_args(args, j, sa);
+  rho_min_body<P>(A, bx, by, bz);
 }
 
 // M(U) = -div F and M(B) = -curl E over the update ranges (sts_div)

@@ -225,12 +225,12 @@ template <class P> struct CoolArgs {
   const int *done;
 };
 
-template <class P> __global__ void __launch_bounds__(256) cooling_kernel(const CoolArgs<P> A) {
+template <class P> CHQ_D void cooling_body(const CoolArgs<P> &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
   const Geom &g = A.g;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   if (i > g.ie || j > g.je || k > g.ke) return;
   const long vs = g.vstride, l = g.idx(k, j, i);
   const double dt = *A.dt;
@@ -247,6 +247,10 @@ template <class P> __global__ void __launch_bounds__(256) cooling_kernel(const C
   }
   t1 = fmax(t1, A.tfloor);
   A.u[IEN * vs + l] += d * (t1 - t0) / A.gm1;
+}
+
+template <class P> __global__ void __launch_bounds__(256) cooling_kernel(const CoolArgs<P> A) {
+  cooling_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -732,13 +736,13 @@ template <class P> __global__ void __launch_bounds__(256) corner_emf_batched(con
   const EmfArgs<P> &A = stage_args(args, j, sa);
   corner_emf_body<P>(A, bx, by, bz);
 }
-template <class P> __global__ void __launch_bounds__(256) update_batched(const UpdateArgs<P> *args, const BatchSlot *slots, int n) {
+template <class P, bool GRAV> __global__ void __launch_bounds__(256) update_batched(const UpdateArgs<P> *args, const BatchSlot *slots, int n) {
   int bx, by, bz;
   const int j = batch_job(slots, n, blockIdx.x);
   batch_block(slots[j], blockIdx.x, bx, by, bz);
   __shared__ __align__(16) unsigned char sa[sizeof(UpdateArgs<P>)];
   const UpdateArgs<P> &A = stage_args(args, j, sa);
-  update_body<P>(A, bx, by, bz);
+  update_body<P, GRAV>(A, bx, by, bz);
 }
 __global__ void __launch_bounds__(256) fofc_flag_batched(const FlagArgs *args, const BatchSlot *slots, int n) {
   int bx, by, bz;
@@ -773,6 +777,14 @@ template <class P> __global__ void __launch_bounds__(256) c2p_batched(const C2pA
   __shared__ __align__(16) unsigned char sa[sizeof(C2pArgs<P>)];
   const C2pArgs<P> &A = stage_args(args, j, sa);
   c2p_body<P>(A, bx, by, bz);
+}
+template <class P> __global__ void __launch_bounds__(256) cooling_batched(const CoolArgs<P> *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  __shared__ __align__(16) unsigned char sa[sizeof(CoolArgs<P>)];
+  const CoolArgs<P> &A = stage_args(args, j, sa);
+  cooling_body<P>(A, bx, by, bz);
 }
 
 }  // namespace chq

@@ -697,6 +697,16 @@ DiffArgs<P> diff_args(chq_mesh *m, const double *b1, const double *b2, const dou
   return a;
 }
 
+template <class P> RhoMinArgs<P> rho_min_args(chq_mesh *m, const int *done) {
+  return RhoMinArgs<P>{m->g, as<P>(m->w), &m->ctl->rho_bits, done};
+}
+
+// grid of the kernels over the active cells (rho_min, cooling)
+Launch3 active_grid(const chq_mesh *m) {
+  const Geom &g = m->g;
+  return {dim3((unsigned)((g.nx1 + 31) / 32), (unsigned)((g.je - g.js + 1 + 7) / 8), (unsigned)(g.ke - g.ks + 1)), dim3(32, 8)};
+}
+
 // diffusive fluxes of every active direction in one launch (diffusion::Fluxes<0..2>)
 template <class P>
 int do_diff(chq_mesh *m, const double *b1, const double *b2, const double *b3, const int *done, cudaStream_t s) {
@@ -709,11 +719,9 @@ int do_diff(chq_mesh *m, const double *b1, const double *b2, const double *b3, c
   return CHQ_OK;
 }
 
-// eta J added to the edge EMFs (diffusion::ResistiveEMF); a no-op without resistivity
 template <class P>
-int do_res_emf(chq_mesh *m, const double *b1, const double *b2, const double *b3, const int *done, const int *need,
-               cudaStream_t s) {
-  if (!(m->cfg.eta > 0.0)) return CHQ_OK;
+ResEmfArgs<P> res_emf_args(chq_mesh *m, const double *b1, const double *b2, const double *b3, const int *done,
+                           const int *need) {
   const Geom &g = m->g;
   ResEmfArgs<P> a{};
   a.g = g;
@@ -724,14 +732,45 @@ int do_res_emf(chq_mesh *m, const double *b1, const double *b2, const double *b3
   a.ju = g.two_d ? g.je + 1 : g.js + 1;
   a.done = done;
   a.need = need;
-  const dim3 grid((unsigned)((g.ie + 2 - g.is + 31) / 32), (unsigned)((a.ju - g.js + 1 + 7) / 8), (unsigned)(a.ku - g.ks + 1));
+  return a;
+}
+
+// the resistive EMF grid; empty without resistivity
+Launch3 res_emf_grid(const chq_mesh *m) {
+  const Geom &g = m->g;
+  if (!(m->cfg.eta > 0.0)) return {dim3(0, 1, 1), dim3(32, 8)};
+  const int ku = g.three_d ? g.ke + 1 : g.ks + 1, ju = g.two_d ? g.je + 1 : g.js + 1;
+  return {dim3((unsigned)((g.ie + 2 - g.is + 31) / 32), (unsigned)((ju - g.js + 1 + 7) / 8), (unsigned)(ku - g.ks + 1)),
+          dim3(32, 8)};
+}
+
+// eta J added to the edge EMFs (diffusion::ResistiveEMF); a no-op without resistivity
+template <class P>
+int do_res_emf(chq_mesh *m, const double *b1, const double *b2, const double *b3, const int *done, const int *need,
+               cudaStream_t s) {
+  if (!(m->cfg.eta > 0.0)) return CHQ_OK;
+  const ResEmfArgs<P> a = res_emf_args<P>(m, b1, b2, b3, done, need);
   m->nlaunch += 1;
-  resistive_emf_kernel<P><<<grid, dim3(32, 8), 0, s>>>(a);
+  resistive_emf_kernel<P><<<res_emf_grid(m).grid, dim3(32, 8), 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
 
 // cooling of the step's end state u0 over this cycle's dt (srcterms::ApplyCooling)
+template <class P> CoolArgs<P> cool_args(chq_mesh *m, const int *done) {
+  CoolArgs<P> a{};
+  a.g = m->g;
+  a.gm1 = m->cfg.gamma - 1.0;
+  a.lambda0 = m->cfg.lambda0;
+  a.alpha = m->cfg.cool_alpha;
+  a.tfloor = m->cfg.tfloor;
+  a.u = m->u[0];
+  a.w = as<P>(m->w);
+  a.dt = &m->ctl->dt;
+  a.done = done;
+  return a;
+}
+
 template <class P>
 int do_cooling(chq_mesh *m, const int *done, cudaStream_t s) {
   const Geom &g = m->g;
@@ -758,7 +797,7 @@ int do_rho_min(chq_mesh *m, const int *done, cudaStream_t s) {
   const Geom &g = m->g;
   const dim3 grid((unsigned)((g.nx1 + 31) / 32), (unsigned)((g.je - g.js + 1 + 7) / 8), (unsigned)(g.ke - g.ks + 1));
   m->nlaunch += 1;
-  rho_min_kernel<P><<<grid, dim3(32, 8), 0, s>>>(g, as<P>(m->w), &m->ctl->rho_bits, done);
+  rho_min_kernel<P><<<grid, dim3(32, 8), 0, s>>>(rho_min_args<P>(m, done));
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
@@ -1147,6 +1186,13 @@ struct chq_batch {
     long nblocks = 0;
   };
   Kind k_flux, k_flux_yz, k_corner, k_update, k_flag, k_repair, k_limit, k_bc[3], k_c2p;
+  // source terms and explicit diffusion (every member or none): the stage adds the diffusive
+  // fluxes after K1 and eta J after the corner EMFs; gravity runs in the update epilogue;
+  // cooling is split after the step
+  int diff = 0, grav = 0, cool = 0;
+  Kind k_diff, k_res, k_rho, k_cool;
+  void *a_diff[4] = {}, *a_res[4] = {}, *a_res_need[4] = {};
+  void *a_rho = nullptr, *a_cool = nullptr, *a_c2p_split[2] = {}, *a_bc0[3] = {};
   void *a_flux[4] = {}, *a_update[4] = {}, *a_update_need[4] = {}, *a_repair[4] = {}, *a_limit[4] = {},
        *a_c2p[4] = {}, *a_flag[4] = {}, *a_bc[4][3] = {};
   void *a_corner = nullptr, *a_corner_need = nullptr;
@@ -1222,6 +1268,18 @@ int batch_build(chq_batch *B) {
   for (int d = 0; d < 3; ++d)
     o_bc_s[d] = slots_of(h, J, [d](chq_mesh *m) { return linear(bc_threads(m, d), 256); }, B->k_bc[d].nblocks);
   o_c2p_s = slots_of(h, J, [](chq_mesh *m) { return c2p_grid(m); }, B->k_c2p.nblocks);
+  const size_t o_diff_s = slots_of(h, J, [](chq_mesh *m) {
+    long tot = 0;
+    if (m->diff) diff_args<P>(m, m->bf[0][0], m->bf[0][1], m->bf[0][2], nullptr, tot);
+    return linear(tot, 256);
+  }, B->k_diff.nblocks);
+  const size_t o_res_s = slots_of(h, J, [](chq_mesh *m) { return res_emf_grid(m); }, B->k_res.nblocks);
+  const size_t o_rho_s = slots_of(h, J, [](chq_mesh *m) {
+    return m->diff ? active_grid(m) : Launch3{dim3(0, 1, 1), dim3(32, 8)};
+  }, B->k_rho.nblocks);
+  const size_t o_cool_s = slots_of(h, J, [](chq_mesh *m) {
+    return m->cfg.cooling ? active_grid(m) : Launch3{dim3(0, 1, 1), dim3(32, 8)};
+  }, B->k_cool.nblocks);
 
   std::vector<EmfArgs<P>> corner(n), corner_need(n);
   std::vector<StepCtl *> ctls(n);
@@ -1233,6 +1291,25 @@ int batch_build(chq_batch *B) {
   }
   const size_t o_corner = push_vec(h, corner), o_corner_need = push_vec(h, corner_need), o_ctls = push_vec(h, ctls);
   size_t o_flux[4], o_update[4], o_update_need[4], o_flag[4], o_repair[4], o_limit[4], o_bc[4][3], o_c2p[4];
+  size_t o_diff[4] = {}, o_res[4] = {}, o_res_need[4] = {};
+  // the cooling split: con2prim of u0 without and with the dt, cooling, boundaries of u0
+  std::vector<RhoMinArgs<P>> rho(n);
+  std::vector<CoolArgs<P>> cool(n);
+  std::vector<C2pArgs<P>> split0(n), split1(n);
+  std::vector<BcArgs> bc0[3] = {std::vector<BcArgs>(n), std::vector<BcArgs>(n), std::vector<BcArgs>(n)};
+  for (int j = 0; j < n; ++j) {
+    chq_mesh *m = J[j];
+    StepCtl *c = m->ctl;
+    rho[j] = rho_min_args<P>(m, &c->done);
+    cool[j] = cool_args<P>(m, &c->done);
+    split0[j] = c2p_args<P>(m, 0, 0, &c->mdt_bits, c, &c->done);
+    split1[j] = c2p_args<P>(m, 0, 1, &c->mdt_bits, c, &c->done);
+    for (int d = 0; d < 3; ++d) bc0[d][j] = bc_args(m, 0, &c->done, d);
+  }
+  const size_t o_rho = push_vec(h, rho), o_cool = push_vec(h, cool), o_split0 = push_vec(h, split0),
+               o_split1 = push_vec(h, split1);
+  size_t o_bc0[3];
+  for (int d = 0; d < 3; ++d) o_bc0[d] = push_vec(h, bc0[d]);
   for (int st = 1; st <= B->nstage; ++st) {
     double g0, g1, beta;
     int cur, out;
@@ -1245,9 +1322,16 @@ int batch_build(chq_batch *B) {
     std::vector<LimitArgs<P>> la(n);
     std::vector<BcArgs> bc[3] = {std::vector<BcArgs>(n), std::vector<BcArgs>(n), std::vector<BcArgs>(n)};
     std::vector<C2pArgs<P>> ca(n);
+    std::vector<DiffArgs<P>> da(n);
+    std::vector<ResEmfArgs<P>> ea(n), ean(n);
     for (int j = 0; j < n; ++j) {
       chq_mesh *m = J[j];
       StepCtl *c = m->ctl;
+      const double *bc1 = m->bf[cur][0], *bc2 = m->bf[cur][1], *bc3 = m->bf[cur][2];
+      long nd = 0;
+      da[j] = diff_args<P>(m, bc1, bc2, bc3, &c->done, nd);
+      ea[j] = res_emf_args<P>(m, bc1, bc2, bc3, &c->done, nullptr);
+      ean[j] = res_emf_args<P>(m, bc1, bc2, bc3, &c->done, &c->nbad);
       fa[j] = flux_args<P>(m, cur, 7u);
       fa[j].skip = &c->done;
       ua[j] = update_args<P>(m, out, g0, g1, 0.0, &c->beta_dt[st - 1], &c->done, nullptr);
@@ -1255,10 +1339,17 @@ int batch_build(chq_batch *B) {
       fl[j] = flag_args(m, out, &c->nbad, &c->done);
       long tot = 0;
       ra[j] = repair_args<P>(m, cur, 7u, &c->done, &c->nbad, tot);
+      if (m->diff) {
+        ra[j].has_diff = 1;
+        ra[j].diff = da[j];
+      }
       la[j] = limit_args<P>(m, 7u, 0.0, &c->beta_dt[st - 1], &c->limiter_count, &c->done, tot);
       for (int d = 0; d < 3; ++d) bc[d][j] = bc_args(m, out, &c->done, d);
-      ca[j] = c2p_args<P>(m, out, last ? 1 : 0, &c->mdt_bits, c, &c->done);
+      ca[j] = c2p_args<P>(m, out, (last && !m->cfg.cooling) ? 1 : 0, &c->mdt_bits, c, &c->done);
     }
+    o_diff[st - 1] = push_vec(h, da);
+    o_res[st - 1] = push_vec(h, ea);
+    o_res_need[st - 1] = push_vec(h, ean);
     o_flux[st - 1] = push_vec(h, fa);
     o_update[st - 1] = push_vec(h, ua);
     o_update_need[st - 1] = push_vec(h, uan);
@@ -1287,7 +1378,19 @@ int batch_build(chq_batch *B) {
   B->a_corner_need = d + o_corner_need;
   B->ctls = (StepCtl **)(d + o_ctls);
   B->status = (double *)(d + o_status);
+  B->k_diff.slots = (BatchSlot *)(d + o_diff_s);
+  B->k_res.slots = (BatchSlot *)(d + o_res_s);
+  B->k_rho.slots = (BatchSlot *)(d + o_rho_s);
+  B->k_cool.slots = (BatchSlot *)(d + o_cool_s);
+  B->a_rho = d + o_rho;
+  B->a_cool = d + o_cool;
+  B->a_c2p_split[0] = d + o_split0;
+  B->a_c2p_split[1] = d + o_split1;
+  for (int q = 0; q < 3; ++q) B->a_bc0[q] = d + o_bc0[q];
   for (int st = 0; st < B->nstage; ++st) {
+    B->a_diff[st] = d + o_diff[st];
+    B->a_res[st] = d + o_res[st];
+    B->a_res_need[st] = d + o_res_need[st];
     B->a_flux[st] = d + o_flux[st];
     B->a_update[st] = d + o_update[st];
     B->a_update_need[st] = d + o_update_need[st];
@@ -1326,19 +1429,37 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
   for (int st = 0; st < B->nstage; ++st) {
     CHQ_CUDA(batch_flux<P>(B, (const FluxArgs<P> *)B->a_flux[st], s));
     ++L;
+    if (B->diff && B->k_diff.nblocks) {
+      diff_flux_batched<P><<<(unsigned)B->k_diff.nblocks, 256, 0, s>>>((const DiffArgs<P> *)B->a_diff[st], B->k_diff.slots, n);
+      ++L;
+    }
     if (B->limiter && B->k_limit.nblocks) {
       limit_batched<P><<<(unsigned)B->k_limit.nblocks, 256, 0, s>>>((const LimitArgs<P> *)B->a_limit[st], B->k_limit.slots, n);
       ++L;
     }
+    auto update = [&](const void *args) {
+      if (B->grav)
+        update_batched<P, true><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)args, B->k_update.slots, n);
+      else
+        update_batched<P, false><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)args, B->k_update.slots, n);
+      ++L;
+    };
+    auto res_emf = [&](const void *args) {
+      if (!B->diff || !B->k_res.nblocks) return;
+      resistive_emf_batched<P><<<(unsigned)B->k_res.nblocks, b2, 0, s>>>((const ResEmfArgs<P> *)args, B->k_res.slots, n);
+      ++L;
+    };
     corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner, B->k_corner.slots, n);
-    update_batched<P><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)B->a_update[st], B->k_update.slots, n);
-    L += 2;
+    ++L;
+    res_emf(B->a_res[st]);
+    update(B->a_update[st]);
     if (B->fofc) {
       fofc_flag_batched<<<(unsigned)B->k_flag.nblocks, b2, 0, s>>>((const FlagArgs *)B->a_flag[st], B->k_flag.slots, n);
       fofc_repair_batched<P><<<(unsigned)B->k_repair.nblocks, 256, 0, s>>>((const RepairArgs<P> *)B->a_repair[st], B->k_repair.slots, n);
       corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner_need, B->k_corner.slots, n);
-      update_batched<P><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)B->a_update_need[st], B->k_update.slots, n);
-      L += 4;
+      L += 3;
+      res_emf(B->a_res_need[st]);
+      update(B->a_update_need[st]);
     }
     bc_batched<0><<<(unsigned)B->k_bc[0].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc[st][0], B->k_bc[0].slots, n);
     ++L;
@@ -1352,6 +1473,29 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
     }
     c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p[st], B->k_c2p.slots, n);
     ++L;
+    if (st == B->nstage - 1 && B->diff && !B->cool) {
+      rho_min_batched<P><<<(unsigned)B->k_rho.nblocks, b2, 0, s>>>((const RhoMinArgs<P> *)B->a_rho, B->k_rho.slots, n);
+      ++L;
+    }
+  }
+  if (B->cool) {
+    // operator-split cooling of u0 after the step (src/main.cpp:272-290)
+    c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p_split[0], B->k_c2p.slots, n);
+    cooling_batched<P><<<(unsigned)B->k_cool.nblocks, b2, 0, s>>>((const CoolArgs<P> *)B->a_cool, B->k_cool.slots, n);
+    L += 2;
+    for (int q = 0; q < 3; ++q) {
+      if (!B->k_bc[q].nblocks) continue;
+      if (q == 0) bc_batched<0><<<(unsigned)B->k_bc[0].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[0], B->k_bc[0].slots, n);
+      if (q == 1) bc_batched<1><<<(unsigned)B->k_bc[1].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[1], B->k_bc[1].slots, n);
+      if (q == 2) bc_batched<2><<<(unsigned)B->k_bc[2].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[2], B->k_bc[2].slots, n);
+      ++L;
+    }
+    c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p_split[1], B->k_c2p.slots, n);
+    ++L;
+    if (B->diff) {
+      rho_min_batched<P><<<(unsigned)B->k_rho.nblocks, b2, 0, s>>>((const RhoMinArgs<P> *)B->a_rho, B->k_rho.slots, n);
+      ++L;
+    }
   }
   ctl_end_batched<<<(n + 127) / 128, 128, 0, s>>>(B->ctls, n);
   ++L;
@@ -2241,13 +2385,14 @@ int chq_event_elapsed(chq_mesh *m, int a, int b, float *ms) {
   return CHQ_OK;
 }
 
+bool grav_on(const chq_mesh *m) { return m->cfg.gravity_uniform || m->cfg.gravity_point; }
+
 int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   if (!meshes || n < 1 || !out) return fail(CHQ_ERR_ARG, "bad argument");
   for (int q = 0; q < n; ++q)
-    if (meshes[q] && (meshes[q]->diff || meshes[q]->cfg.cooling || meshes[q]->cfg.gravity_uniform ||
-                      meshes[q]->cfg.gravity_point))
-      return fail(CHQ_ERR_ARG, "batched stepping covers the ideal-MHD stage; step meshes with diffusion or "
-                               "source terms one by one");
+    if (meshes[q] && meshes[q]->diff && meshes[q]->cfg.sts)
+      return fail(CHQ_ERR_ARG, "batched stepping covers explicit diffusion only; step meshes with RKL2 "
+                               "super-time-stepping (diffusion.sts) one by one");
   *out = nullptr;
   const chq_mesh *a = meshes[0];
   for (int j = 0; j < n; ++j) {
@@ -2258,6 +2403,9 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
         m->cfg.flux_limiter != a->cfg.flux_limiter)
       return fail(CHQ_ERR_ARG, "batch members must share precision, reconstruction, Riemann solver, "
                                "characteristic flag, integrator, FOFC and limiter switches");
+    if (m->diff != a->diff || (m->cfg.cooling != 0) != (a->cfg.cooling != 0) || grav_on(m) != grav_on(a))
+      return fail(CHQ_ERR_ARG, "batch members must agree on explicit diffusion, cooling and gravity (on or "
+                               "off; their coefficients may differ)");
     for (int q = 0; q < j; ++q)
       if (meshes[q] == m) return fail(CHQ_ERR_ARG, "a mesh appears twice in the batch");
   }
@@ -2270,6 +2418,9 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   B->nstage = a->nstage;
   B->fofc = a->cfg.fofc;
   B->limiter = a->cfg.flux_limiter;
+  B->diff = a->diff ? 1 : 0;
+  B->cool = a->cfg.cooling ? 1 : 0;
+  B->grav = grav_on(a) ? 1 : 0;
   int rc = B->mixed ? batch_build<float>(B) : batch_build<double>(B);
   if (rc == CHQ_OK) {
     cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);

@@ -12,9 +12,11 @@
 //      with the fewest cells; each lane has its own stream and replays a CUDA graph, so the
 //      flux kernel of one lane overlaps the memory-bound kernels of another. Batching alone
 //      serialises every job through the same kernel sequence.
-// Jobs of 2^21 cells or more are not batched: each runs "solo" on its own mesh stream,
-// replaying a CUDA graph of one cycle, and the server polls an event behind its chunk instead
-// of waiting for it, so a large job never holds up the lanes (or another large job).
+// Jobs of 2^21 cells or more, and jobs with RKL2 super-time-stepping, are not batched: each
+// runs "solo" on its own mesh stream (large ones replaying a CUDA graph of one cycle) and the
+// server polls an event behind its chunk instead of waiting for it, so a large job never holds
+// up the lanes (or another large job). Explicit diffusion, cooling and gravity batch with
+// jobs that have the same terms switched on.
 // Each job keeps its own dt and clock on the device, so its result is the same alone and in
 // any mix. Times are seconds on the server's steady clock.
 #include <chrono>
@@ -69,11 +71,19 @@ void free_solo(Job *j) {
   }
 }
 
-// (precision, reconstruction, Riemann solver, characteristic, integrator, FOFC, limiter, lane)
-using ClassKey = std::tuple<int, int, int, int, int, int, int, int>;
+// (precision, reconstruction, Riemann solver, characteristic, integrator, FOFC, limiter,
+//  explicit diffusion | cooling << 1 | gravity << 2, lane)
+using ClassKey = std::tuple<int, int, int, int, int, int, int, int, int>;
+
+bool has_diffusion(const chq_config &c) { return c.nu > 0 || c.kappa > 0 || c.eta > 0; }
+
+int features(const chq_config &c) {
+  return (has_diffusion(c) ? 1 : 0) | (c.cooling ? 2 : 0) | ((c.gravity_uniform || c.gravity_point) ? 4 : 0);
+}
 
 ClassKey key_of(const chq_config &c, int lane) {
-  return ClassKey{c.precision, c.recon, c.rsolver, c.characteristic, c.integrator, c.fofc, c.flux_limiter, lane};
+  return ClassKey{c.precision, c.recon, c.rsolver, c.characteristic, c.integrator, c.fofc, c.flux_limiter,
+                  features(c), lane};
 }
 
 struct Group {
@@ -269,7 +279,8 @@ void admit(chq_server *S) {
     S->used += j->bytes;
     j->state = CHQ_JOB_RUNNING;
     j->t_start = S->now();
-    if (j->cells >= kSoloCells) {
+    // RKL2 super-time-stepping takes a host decision every cycle: such jobs never batch
+    if (j->cells >= kSoloCells || (has_diffusion(j->cfg) && j->cfg.sts)) {
       j->solo = true;
       S->solo.push_back(j);
       ++active;
@@ -335,9 +346,6 @@ int chq_server_submit(chq_server *S, const chq_config *cfg, int problem, const d
   const long long bytes = chq_config_bytes(cfg);
   if (bytes <= 0) return err(CHQ_ERR_ARG, "invalid job configuration");
   if (bytes > S->budget) return err(CHQ_ERR_ARG, "job larger than the server's HBM budget");
-  if (cfg->nu > 0 || cfg->kappa > 0 || cfg->eta > 0 || cfg->cooling || cfg->gravity_uniform || cfg->gravity_point)
-    return err(CHQ_ERR_ARG, "the server batches ideal-MHD jobs; run jobs with diffusion or source terms on their "
-                            "own mesh");
   Job *j = new Job;
   j->id = S->next_id++;
   j->cfg = *cfg;

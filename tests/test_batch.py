@@ -42,6 +42,29 @@ SETS = {
 }
 
 
+GRAV_U = ("gravity.uniform=true", "gravity.g1=0.5", "gravity.g2=-0.25", "gravity.g3=1.0")
+GRAV_P = ("gravity.point_mass=true", "gravity.gm=0.05", "gravity.x0=0.05", "gravity.y0=-0.1", "gravity.z0=0.02",
+          "gravity.rsoft=0.05")
+STRONG = ("problem.pres_in=1e4", "problem.pres_out=1e-3", "time.cfl=0.5")
+
+# explicit diffusion, gravity and cooling: every member has the terms on, with its own
+# coefficients; the strong blasts add FOFC re-runs (diffusive fluxes re-added on repaired faces)
+SETS.update({
+    "diffusion_fp64": [(cases.ot(32), ("diffusion.nu=2e-3", "diffusion.kappa=2e-3", "diffusion.eta=1e-3")),
+                       (cases.blast(16), STRONG + ("diffusion.eta=2e-3",)),
+                       (cases.diffusion("b", 1, 32, 8), ("diffusion.eta=0.01", "mhd.reconstruct=ppm"))],
+    "gravity_fp64": [(cases.blast(16), STRONG + GRAV_P), (cases.ot(32), GRAV_P + GRAV_U),
+                     (cases.cpaw3d_extruded(16, 8), ("mhd.reconstruct=ppm",) + GRAV_U)],
+    "cooling_fp64": [(cases.ot(32), ("cooling.enabled=true", "cooling.lambda0=0.5")),
+                     (cases.blast(16), ("cooling.enabled=true", "cooling.lambda0=5.0", "cooling.alpha=2.0",
+                                        "cooling.tfloor=0.05"))],
+    "all_terms_fp64": [(cases.ot(32), GRAV_U + ("cooling.enabled=true", "cooling.lambda0=0.2", "diffusion.nu=2e-3",
+                                                "diffusion.kappa=2e-3")),
+                       (cases.blast(16), STRONG + GRAV_P + ("cooling.enabled=true", "cooling.lambda0=1.0",
+                                                            "diffusion.eta=1e-3"))],
+})
+
+
 @pytest.mark.parametrize("graph", [False, True], ids=["launches", "graph"])
 @pytest.mark.parametrize("name", sorted(SETS))
 def test_batched_members_equal_solo(name, graph):
@@ -112,3 +135,9 @@ def test_batch_rejects_mixed_classes():
         Batch([a, c])
     with pytest.raises(ChqError):
         Batch([a, a])
+    # source terms and diffusion on in every member or in none; no RKL2 members
+    for ov in (GRAV_U, ("cooling.enabled=true", "cooling.lambda0=0.5"), ("diffusion.nu=1e-3",)):
+        with pytest.raises(ChqError):
+            Batch([a, _mesh(cases.ot(16), ov)])
+    with pytest.raises(ChqError):
+        Batch([_mesh(cases.ot(16), ("diffusion.eta=1e-3", "diffusion.sts=true"))])

@@ -109,13 +109,17 @@ def test_decay_rate_matches_exact_solution():
     assert ratio == pytest.approx(np.exp(-0.02 * k * k * t), rel=2e-3)
 
 
-def test_batch_and_server_refuse_diffusive_jobs():
-    from chasqui_b200 import Batch, Server, ChqError
-    from chasqui_b200.core import make_config
+def test_batch_refuses_rkl2_and_mixed_diffusion():
+    """Explicit diffusion batches (tests/test_batch.py); RKL2 meshes do not, since their
+    stage count is a host decision every cycle, and a batch has diffusion in every member or
+    in none. The server runs RKL2 jobs unbatched (tests/test_server.py)."""
+    from chasqui_b200 import Batch, ChqError
     text, ov = CASES["ot2d_all"]
     _, mesh = make_pair(text, ov)
+    Batch([mesh]).close()
+    _, plain = make_pair(text, [])
     with pytest.raises(ChqError):
-        Batch([mesh])
-    srv = Server(1 << 30, 4, 1)
+        Batch([mesh, plain])
+    _, sts = make_pair(text, list(ov) + ["diffusion.sts=true"])
     with pytest.raises(ChqError):
-        srv.submit(make_config(nx1=32, nx2=32, nx3=1, eta=1e-3), "orszag_tang", [1.0])
+        Batch([sts])

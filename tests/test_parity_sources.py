@@ -101,12 +101,14 @@ def test_cooling_temperature_is_exact():
     assert T == pytest.approx((math.sqrt(0.5) - 0.5 * c) ** 2, rel=1e-6)
 
 
-def test_batch_and_server_refuse_source_terms():
-    from chasqui_b200 import Batch, ChqError, Server
-    from chasqui_b200.core import make_config
-    _, mesh = make_pair(UNIFORM, GRAV_U)
-    with pytest.raises(ChqError):
-        Batch([mesh])
-    srv = Server(1 << 30, 4, 1)
-    with pytest.raises(ChqError):
-        srv.submit(make_config(nx1=32, nx2=32, nx3=1, cooling=1, lambda0=0.1), "orszag_tang", [1.0])
+def test_batch_groups_source_terms_by_switch():
+    """A batch takes meshes with gravity (or cooling) only together with meshes that have it
+    too; their coefficients may differ (tests/test_batch.py checks the results)."""
+    from chasqui_b200 import Batch, ChqError
+    _, grav = make_pair(UNIFORM, GRAV_U)
+    _, plain = make_pair(UNIFORM, [])
+    _, cool = make_pair(UNIFORM, ["cooling.enabled=true", "cooling.lambda0=0.1"])
+    Batch([grav]).close()
+    for pair in ([grav, plain], [grav, cool], [cool, plain]):
+        with pytest.raises(ChqError):
+            Batch(pair)

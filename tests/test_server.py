@@ -105,6 +105,30 @@ def test_large_jobs_run_solo_beside_batched_lanes():
     assert s["zone_updates"] == total and s["active"] == 0 and s["used_bytes"] == 0
 
 
+def test_jobs_with_diffusion_and_source_terms():
+    """Explicit diffusion, cooling and gravity batch with jobs that have the same terms (their
+    own coefficients); RKL2 jobs run unbatched. Every result equals the job run alone."""
+    jobs = [
+        (lambda: ot_cfg(32, 8, nu=2e-3, kappa=2e-3, eta=1e-3), "orszag_tang", [-1.0]),
+        (lambda: ot_cfg(24, 9, nu=1e-3), "orszag_tang", [0.5]),
+        (lambda: blast_cfg(16, 6, gravity_uniform=1, g1=0.5, g3=-0.25), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 2.0]),
+        (lambda: blast_cfg(12, 7, gravity_point=1, gm=0.05, rsoft=0.05), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 3.0]),
+        (lambda: ot_cfg(32, 8, cooling=1, lambda0=0.5), "orszag_tang", [-1.0]),
+        (lambda: ot_cfg(32, 6, cooling=1, lambda0=0.2, nu=2e-3, gravity_uniform=1, g1=0.3), "orszag_tang", [-1.0]),
+        (lambda: ot_cfg(32, 5, eta=0.02, sts=1), "orszag_tang", [-1.0]),
+        (lambda: ot_cfg(32, 10), "orszag_tang", [-1.0]),
+    ]
+    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=3)
+    ids = [srv.submit(f(), p, prm) for f, p, prm in jobs]
+    run_all(srv)
+    for jid, (f, p, prm) in zip(ids, jobs):
+        st = srv.status(jid)
+        h, cyc = solo_history(f(), p, prm)
+        assert st["state"] == "done", st
+        assert st["cycle"] == cyc == f().nlim
+        assert np.array_equal(np.array(st["history"]), h), (p, st["history"], h)
+
+
 def test_admission_respects_budget_and_drains():
     one = load_library().chq_config_bytes(blast_cfg(16, 6))
     srv = Server(hbm_budget_bytes=int(2.5 * one), cycles_per_step=2)
