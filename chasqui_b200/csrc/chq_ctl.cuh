@@ -44,4 +44,22 @@ CHQ_D void atomic_min_pos(unsigned long long *bits, double v) {
   atomicMin(bits, (unsigned long long)__double_as_longlong(v));
 }
 
+// Minimum of v over the block into *bits with one atomic per block: warp shuffles, then the
+// warps' minima through shared memory. Every thread of the block must call it (it holds a
+// barrier); blocks of at most 32 warps. The result is the same as one atomic per thread.
+CHQ_D void block_min_pos(unsigned long long *bits, double v) {
+  __shared__ double wmin[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int tid = (int)(threadIdx.z * blockDim.y + threadIdx.y) * (int)blockDim.x + (int)threadIdx.x;
+  const int nw = (int)((blockDim.x * blockDim.y * blockDim.z + 31) / 32);
+  if ((tid & 31) == 0) wmin[tid >> 5] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double m = wmin[0];
+    for (int w = 1; w < nw; ++w) m = fmin(m, wmin[w]);
+    atomic_min_pos(bits, m);
+  }
+}
+
 }  // namespace chq

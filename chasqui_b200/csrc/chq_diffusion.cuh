@@ -210,9 +210,7 @@ template <class P> CHQ_D void rho_min_body(const RhoMinArgs<P> &A, int bx, int b
   const int k = g.ks + bz;
   double v = __longlong_as_double(0x7ff0000000000000LL);
   if (i <= g.ie && j <= g.je) v = (double)w[g.idx(k, j, i)];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0) atomic_min_pos(bits, v);
+  block_min_pos(bits, v);   // one atomic per block (the whole block is here)
 }
 
 template <class P> __global__ void __launch_bounds__(256) rho_min_kernel(const RhoMinArgs<P> A) {

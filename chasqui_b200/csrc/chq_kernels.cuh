@@ -717,11 +717,7 @@ template <class P> CHQ_D void c2p_body(const C2pArgs<P> &A, int bx, int by, int 
       mdt = dt;
     }
   }
-  if (A.compute_dt) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mdt = fmin(mdt, __shfl_xor_sync(0xffffffffu, mdt, o));
-    if ((threadIdx.x & 31) == 0) atomic_min_pos(A.mdt_bits, mdt);
-  }
+  if (A.compute_dt) block_min_pos(A.mdt_bits, mdt);   // one atomic per block (the whole block is here)
 }
 
 template <class P> __global__ void __launch_bounds__(256) c2p_kernel(const C2pArgs<P> A) { c2p_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
