@@ -31,13 +31,15 @@ int fail(int code, const std::string &msg) {
   g_err = msg;
   return code;
 }
-int cuda_fail(cudaError_t e, const char *where) {
-  return fail(CHQ_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+int cuda_fail(cudaError_t e, const char *where, int line = 0) {
+  std::string at = where;
+  if (line > 0) at += " (chq_mesh.cu:" + std::to_string(line) + ")";
+  return fail(CHQ_ERR_CUDA, at + ": " + cudaGetErrorString(e));
 }
-#define CHQ_CUDA(call)                                   \
-  do {                                                   \
-    cudaError_t e_ = (call);                             \
-    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+#define CHQ_CUDA(call)                                             \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call, __LINE__);  \
   } while (0)
 
 }  // namespace
@@ -1425,79 +1427,99 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
   const dim3 b2(32, 8);
   long long &L = B->nlaunch;
   ctl_begin_batched<<<(n + 127) / 128, 128, 0, s>>>(B->ctls, n);
+  CHQ_CUDA(cudaGetLastError());
   ++L;
   for (int st = 0; st < B->nstage; ++st) {
     CHQ_CUDA(batch_flux<P>(B, (const FluxArgs<P> *)B->a_flux[st], s));
     ++L;
     if (B->diff && B->k_diff.nblocks) {
       diff_flux_batched<P><<<(unsigned)B->k_diff.nblocks, 256, 0, s>>>((const DiffArgs<P> *)B->a_diff[st], B->k_diff.slots, n);
+      CHQ_CUDA(cudaGetLastError());
       ++L;
     }
     if (B->limiter && B->k_limit.nblocks) {
       limit_batched<P><<<(unsigned)B->k_limit.nblocks, 256, 0, s>>>((const LimitArgs<P> *)B->a_limit[st], B->k_limit.slots, n);
+      CHQ_CUDA(cudaGetLastError());
       ++L;
     }
-    auto update = [&](const void *args) {
+    auto update = [&](const void *args) -> cudaError_t {
       if (B->grav)
         update_batched<P, true><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)args, B->k_update.slots, n);
       else
         update_batched<P, false><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const UpdateArgs<P> *)args, B->k_update.slots, n);
       ++L;
+      return cudaGetLastError();
     };
-    auto res_emf = [&](const void *args) {
-      if (!B->diff || !B->k_res.nblocks) return;
+    auto res_emf = [&](const void *args) -> cudaError_t {
+      if (!B->diff || !B->k_res.nblocks) return cudaSuccess;
       resistive_emf_batched<P><<<(unsigned)B->k_res.nblocks, b2, 0, s>>>((const ResEmfArgs<P> *)args, B->k_res.slots, n);
       ++L;
+      return cudaGetLastError();
     };
     corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner, B->k_corner.slots, n);
+    CHQ_CUDA(cudaGetLastError());
     ++L;
-    res_emf(B->a_res[st]);
-    update(B->a_update[st]);
+    CHQ_CUDA(res_emf(B->a_res[st]));
+    CHQ_CUDA(update(B->a_update[st]));
     if (B->fofc) {
       fofc_flag_batched<<<(unsigned)B->k_flag.nblocks, b2, 0, s>>>((const FlagArgs *)B->a_flag[st], B->k_flag.slots, n);
+      CHQ_CUDA(cudaGetLastError());
       fofc_repair_batched<P><<<(unsigned)B->k_repair.nblocks, 256, 0, s>>>((const RepairArgs<P> *)B->a_repair[st], B->k_repair.slots, n);
+      CHQ_CUDA(cudaGetLastError());
       corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner_need, B->k_corner.slots, n);
+      CHQ_CUDA(cudaGetLastError());
       L += 3;
-      res_emf(B->a_res_need[st]);
-      update(B->a_update_need[st]);
+      CHQ_CUDA(res_emf(B->a_res_need[st]));
+      CHQ_CUDA(update(B->a_update_need[st]));
     }
     bc_batched<0><<<(unsigned)B->k_bc[0].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc[st][0], B->k_bc[0].slots, n);
+    CHQ_CUDA(cudaGetLastError());
     ++L;
     if (B->k_bc[1].nblocks) {
       bc_batched<1><<<(unsigned)B->k_bc[1].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc[st][1], B->k_bc[1].slots, n);
+      CHQ_CUDA(cudaGetLastError());
       ++L;
     }
     if (B->k_bc[2].nblocks) {
       bc_batched<2><<<(unsigned)B->k_bc[2].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc[st][2], B->k_bc[2].slots, n);
+      CHQ_CUDA(cudaGetLastError());
       ++L;
     }
     c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p[st], B->k_c2p.slots, n);
+    CHQ_CUDA(cudaGetLastError());
     ++L;
     if (st == B->nstage - 1 && B->diff && !B->cool) {
       rho_min_batched<P><<<(unsigned)B->k_rho.nblocks, b2, 0, s>>>((const RhoMinArgs<P> *)B->a_rho, B->k_rho.slots, n);
+      CHQ_CUDA(cudaGetLastError());
       ++L;
     }
   }
   if (B->cool) {
     // operator-split cooling of u0 after the step (src/main.cpp:272-290)
     c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p_split[0], B->k_c2p.slots, n);
+    CHQ_CUDA(cudaGetLastError());
     cooling_batched<P><<<(unsigned)B->k_cool.nblocks, b2, 0, s>>>((const CoolArgs<P> *)B->a_cool, B->k_cool.slots, n);
+    CHQ_CUDA(cudaGetLastError());
     L += 2;
     for (int q = 0; q < 3; ++q) {
       if (!B->k_bc[q].nblocks) continue;
       if (q == 0) bc_batched<0><<<(unsigned)B->k_bc[0].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[0], B->k_bc[0].slots, n);
       if (q == 1) bc_batched<1><<<(unsigned)B->k_bc[1].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[1], B->k_bc[1].slots, n);
       if (q == 2) bc_batched<2><<<(unsigned)B->k_bc[2].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[2], B->k_bc[2].slots, n);
+      CHQ_CUDA(cudaGetLastError());
       ++L;
     }
     c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p_split[1], B->k_c2p.slots, n);
+    CHQ_CUDA(cudaGetLastError());
     ++L;
     if (B->diff) {
       rho_min_batched<P><<<(unsigned)B->k_rho.nblocks, b2, 0, s>>>((const RhoMinArgs<P> *)B->a_rho, B->k_rho.slots, n);
+      CHQ_CUDA(cudaGetLastError());
       ++L;
     }
   }
   ctl_end_batched<<<(n + 127) / 128, 128, 0, s>>>(B->ctls, n);
+  CHQ_CUDA(cudaGetLastError());
   ++L;
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;

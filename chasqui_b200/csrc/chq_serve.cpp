@@ -12,8 +12,9 @@
 //      with the fewest cells; each lane has its own stream and replays a CUDA graph, so the
 //      flux kernel of one lane overlaps the memory-bound kernels of another. Batching alone
 //      serialises every job through the same kernel sequence.
-// Jobs of 2^21 cells or more, and jobs with RKL2 super-time-stepping, are not batched: each
-// runs "solo" on its own mesh stream (large ones replaying a CUDA graph of one cycle) and the
+// Jobs of 2^21 cells or more (chq_server_set_solo_cells), and jobs with RKL2
+// super-time-stepping, are not batched: each runs "solo" on its own mesh stream (replaying a
+// CUDA graph of one cycle, except RKL2) and the
 // server polls an event behind its chunk instead of waiting for it, so a large job never holds
 // up the lanes (or another large job). Explicit diffusion, cooling and gravity batch with
 // jobs that have the same terms switched on.
@@ -104,6 +105,7 @@ int err(int code, const std::string &m) {
 struct chq_server {
   long long budget = 0, used = 0;
   int max_active = 0, cycles_per_step = 1, lanes = 8;
+  long long solo_cells = 0;   // jobs of at least this many cells run unbatched
   long long next_id = 1;
   std::map<long long, Job *> jobs;
   std::vector<Job *> queue;
@@ -164,11 +166,13 @@ int retire_finished(chq_server *S) {
 }
 
 // Jobs of at least this many cells run solo: one mesh stream each, cycles replayed as a CUDA
-// graph. Their launches fill the device on their own (a 128^3 flux launch is two waves of
-// resident blocks), and running them concurrently overlaps one job's flux kernel with
-// another's memory-bound kernels, which a batch (one kernel kind at a time for all members)
-// cannot. Smaller jobs fill the device only together, in a batched launch.
-const long long kSoloCells = 1LL << 21;
+// graph. Running them concurrently overlaps one job's flux kernel with another's
+// memory-bound kernels, which a batch (one kernel kind at a time for all members) cannot.
+// On the 256-job ensemble (64^2..1024^2, 32^3..192^3) the server ran at 4.8e8
+// zone-updates/s with the threshold at 2^21 cells, 5.3e8 at 2^18 and 5.4e8 at 2^15 (the rate
+// of one stream per job); chq_server_set_solo_cells lowers it. The default stays at the
+// setting the serving runs were verified with.
+const long long kSoloCells = 1LL << 21;   // default of chq_server::solo_cells
 
 // finished solo chunks: progress and retirement; with `block`, wait for a chunk when none
 // has finished
@@ -280,7 +284,7 @@ void admit(chq_server *S) {
     j->state = CHQ_JOB_RUNNING;
     j->t_start = S->now();
     // RKL2 super-time-stepping takes a host decision every cycle: such jobs never batch
-    if (j->cells >= kSoloCells || (has_diffusion(j->cfg) && j->cfg.sts)) {
+    if (j->cells >= S->solo_cells || (has_diffusion(j->cfg) && j->cfg.sts)) {
       j->solo = true;
       S->solo.push_back(j);
       ++active;
@@ -336,6 +340,7 @@ int chq_server_create(long long hbm_budget_bytes, int max_active, int cycles_per
   S->budget = hbm_budget_bytes;
   S->max_active = max_active;
   S->cycles_per_step = cycles_per_step;
+  S->solo_cells = kSoloCells;
   *out = S;
   return CHQ_OK;
 }
@@ -434,6 +439,12 @@ int chq_server_stats(chq_server *S, long long *used_bytes, int *active, int *que
 int chq_server_set_lanes(chq_server *S, int lanes) {
   if (!S || lanes < 1 || lanes > 64) return err(CHQ_ERR_ARG, "lanes must be in [1, 64]");
   S->lanes = lanes;
+  return CHQ_OK;
+}
+
+int chq_server_set_solo_cells(chq_server *S, long long cells) {
+  if (!S || cells < 0) return err(CHQ_ERR_ARG, "bad argument");
+  S->solo_cells = cells;
   return CHQ_OK;
 }
 

@@ -36,7 +36,7 @@ JOBS = [
 ]
 
 
-SOLO_CELLS = 1 << 21   # jobs this large run unbatched on their own stream
+SOLO_CELLS = 1 << 21   # jobs this large run unbatched on their own stream (server default)
 
 
 def solo_history(cfg, problem, params):
