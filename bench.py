@@ -182,10 +182,10 @@ def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, pro
 
 
 def config_rates(steps: int = 5, warmup: int = 3) -> dict:
-    """zone-updates/s of the other BASELINE configurations, timed like the headline (CUDA
-    events around whole device cycles, warm-up first): OT 2D 256^2 (config 1), CPAW 3D 256^3
-    along 2 pi (1,1,1) with WENO-Z (config 2), and the 512^3 blast with RKL2 diffusion
-    nu = eta = 1e-4 (config 3b; each cycle synchronises once for the RKL2 stage count)."""
+    """zone-updates/s of the other benchmark configurations, timed like the headline (CUDA
+    events around whole device cycles, warm-up first): OT 2D 256^2, CPAW 3D 256^3 along
+    2 pi (1,1,1) with WENO-Z, and the 512^3 blast with RKL2 diffusion nu = eta = 1e-4 (each
+    cycle synchronises once for the RKL2 stage count)."""
     from chasqui_b200 import Mesh, make_config
     out = {}
     runs = [
@@ -342,12 +342,14 @@ name = blast
     return times
 
 
-def ensemble(njobs: int, cycles: int, seed: int, cps: int) -> dict:
-    """njobs seeded jobs (OT 2D 64^2..1024^2, CPAW / blast 3D
-    32^3..192^3, PPM or WENO-Z, mixed precision), `cycles` cycles each: all submitted at
-    once to the batching server vs the same jobs as sequential one-job runs."""
+def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 192)) -> dict:
+    """The ensemble configuration: njobs seeded jobs (OT 2D sizes[0]^2..sizes[1]^2, CPAW /
+    blast 3D sizes[2]^3..sizes[3]^3, PPM or WENO-Z, mixed precision), `cycles` cycles each:
+    all submitted at once to the batching server vs the same jobs as sequential one-job runs
+    and vs every job on its own stream at once."""
     from chasqui_b200 import Mesh, Server, workloads
-    jobs = workloads.draw_jobs(njobs, seed=seed, precision=1, nlim=cycles)
+    jobs = workloads.draw_jobs(njobs, seed=seed, precision=1, nlim=cycles, nmin2=sizes[0], nmax2=sizes[1],
+                               nmin3=sizes[2], nmax3=sizes[3])
     zu = sum(j["cells"] for j in jobs) * cycles
     srv = Server(150 << 30, max_active=100000, cycles_per_step=cps)
     t0 = time.perf_counter()
@@ -382,7 +384,7 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int) -> dict:
     t_con = time.perf_counter() - t0
     for m in meshes:
         m.close()
-    return {"jobs": njobs, "cycles_each": cycles, "zone_updates": zu, "done": ok,
+    return {"jobs": njobs, "cycles_each": cycles, "zone_updates": zu, "done": ok, "sizes": list(sizes),
             "batched": {"seconds": t_batched, "value": zu / t_batched, "server_steps": steps},
             "sequential": {"seconds": t_seq, "value": zu / t_seq},
             "concurrent_streams": {"seconds": t_con, "value": zu / t_con},
@@ -392,7 +394,7 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int) -> dict:
 
 def serving(njobs: int, rate: float, precision: int, seed: int, t_end=(0.005, 0.05), nmax2=512, nmax3=96,
             cps=4) -> dict:
-    """BASELINE config 5, scaled: njobs requests with Poisson arrivals at `rate` jobs/s,
+    """The serving configuration, scaled: njobs requests with Poisson arrivals at `rate` jobs/s,
     kinds and sizes from the ensemble distribution (capped at nmax2^2 / nmax3^3), end time
     U[t_end]; submitted to the server as they arrive; time-to-solution per job."""
     from chasqui_b200 import Server, workloads
@@ -541,6 +543,9 @@ def main(argv=None):
     ens = None
     if not args.no_ensemble:
         ens = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 4)
+        # the same draw restricted to small meshes (32^2..128^2, 16^3..32^3), where one job
+        # alone cannot fill the device and batching is what keeps it busy
+        ens["small_jobs"] = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 16, sizes=(32, 128, 16, 32))
     srv = None
     if not args.no_serving:
         srv = [serving(args.srv_jobs, float(r), prec, 77 + rank)

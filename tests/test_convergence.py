@@ -1,4 +1,4 @@
-"""CPAW convergence on the device (README.md:90-99): one wave period of
+"""CPAW convergence on the device (the reference's table, README.md:90-99): one wave period of
 the circularly polarised Alfven wave at N = 32, 64, 128, total L1 error against the initial
 state as the reference's compute_error (src/main.cpp:310-327). The device errors equal the
 reference's own (relative 1e-9: the runs are bitwise up to the entropy slot's pow), so the
