@@ -1188,10 +1188,11 @@ struct chq_batch {
     long nblocks = 0;
   };
   Kind k_flux, k_flux_yz, k_corner, k_update, k_flag, k_repair, k_limit, k_bc[3], k_c2p;
-  // source terms and explicit diffusion (every member or none): the stage adds the diffusive
-  // fluxes after K1 and eta J after the corner EMFs; gravity runs in the update epilogue;
-  // cooling is split after the step
+  // source terms and diffusion (every member or none): with explicit diffusion (diff) the
+  // stage adds the diffusive fluxes after K1 and eta J after the corner EMFs; gravity runs in
+  // the update epilogue; cooling is split after the step
   int diff = 0, grav = 0, cool = 0;
+  int sts = 0;   // RKL2 members: their super-time-stepping stages run per member after the batched stages
   Kind k_diff, k_res, k_rho, k_cool;
   void *a_diff[4] = {}, *a_res[4] = {}, *a_res_need[4] = {};
   void *a_rho = nullptr, *a_cool = nullptr, *a_c2p_split[2] = {}, *a_bc0[3] = {};
@@ -1341,13 +1342,14 @@ int batch_build(chq_batch *B) {
       fl[j] = flag_args(m, out, &c->nbad, &c->done);
       long tot = 0;
       ra[j] = repair_args<P>(m, cur, 7u, &c->done, &c->nbad, tot);
-      if (m->diff) {
+      if (m->diff && !m->cfg.sts) {
         ra[j].has_diff = 1;
         ra[j].diff = da[j];
       }
       la[j] = limit_args<P>(m, 7u, 0.0, &c->beta_dt[st - 1], &c->limiter_count, &c->done, tot);
       for (int d = 0; d < 3; ++d) bc[d][j] = bc_args(m, out, &c->done, d);
-      ca[j] = c2p_args<P>(m, out, (last && !m->cfg.cooling) ? 1 : 0, &c->mdt_bits, c, &c->done);
+      const bool split = m->cfg.cooling || (m->diff && m->cfg.sts);
+      ca[j] = c2p_args<P>(m, out, (last && !split) ? 1 : 0, &c->mdt_bits, c, &c->done);
     }
     o_diff[st - 1] = push_vec(h, da);
     o_res[st - 1] = push_vec(h, ea);
@@ -1420,6 +1422,35 @@ cudaError_t batch_flux(const chq_batch *B, const FluxArgs<P> *args, cudaStream_t
   }
 }
 
+// The RKL2 part of a batched cycle (src/main.cpp:274-281): the stage count of each member is a
+// host decision on its dt and density minimum, so the batch stream is synchronised once, and
+// every member that is not done advances its diffusive terms with its own launches on the
+// batch stream, exactly as chq_cycles does for a single mesh.
+template <class P>
+int batch_sts(chq_batch *B, cudaStream_t s) {
+  const int n = (int)B->jobs.size();
+  std::vector<StepCtl> h(n);
+  for (int j = 0; j < n; ++j)
+    CHQ_CUDA(cudaMemcpyAsync(&h[j], B->jobs[j]->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  for (int j = 0; j < n; ++j) {
+    if (h[j].done) continue;
+    chq_mesh *m = B->jobs[j];
+    double rho_min;
+    std::memcpy(&rho_min, &h[j].rho_bits, sizeof(rho_min));
+    const double dt_par = host_parabolic_dt(m, rho_min);
+    int nst = 0;
+    const long long l0 = m->nlaunch;
+    int rc = sts_advance<P>(m, h[j].dt, dt_par, s, nst);
+    if (!rc) rc = do_bc(m, 0, nullptr, s);
+    if (rc) return rc;
+    m->sts_stages += nst;
+    B->nlaunch += m->nlaunch - l0;
+    m->nlaunch = l0;
+  }
+  return CHQ_OK;
+}
+
 // one cycle of every member: the launch sequence of chq_cycles, batched
 template <class P>
 int batch_cycle(chq_batch *B, cudaStream_t s) {
@@ -1488,11 +1519,15 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
     c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p[st], B->k_c2p.slots, n);
     CHQ_CUDA(cudaGetLastError());
     ++L;
-    if (st == B->nstage - 1 && B->diff && !B->cool) {
+    if (st == B->nstage - 1 && ((B->diff && !B->cool) || B->sts)) {
       rho_min_batched<P><<<(unsigned)B->k_rho.nblocks, b2, 0, s>>>((const RhoMinArgs<P> *)B->a_rho, B->k_rho.slots, n);
       CHQ_CUDA(cudaGetLastError());
       ++L;
     }
+  }
+  if (B->sts) {
+    const int rc = batch_sts<P>(B, s);
+    if (rc) return rc;
   }
   if (B->cool) {
     // operator-split cooling of u0 after the step (src/main.cpp:272-290)
@@ -1509,6 +1544,8 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
       CHQ_CUDA(cudaGetLastError());
       ++L;
     }
+  }
+  if (B->cool || B->sts) {
     c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_c2p_split[1], B->k_c2p.slots, n);
     CHQ_CUDA(cudaGetLastError());
     ++L;
@@ -2408,13 +2445,10 @@ int chq_event_elapsed(chq_mesh *m, int a, int b, float *ms) {
 }
 
 bool grav_on(const chq_mesh *m) { return m->cfg.gravity_uniform || m->cfg.gravity_point; }
+bool sts_on(const chq_mesh *m) { return m->diff && m->cfg.sts; }
 
 int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   if (!meshes || n < 1 || !out) return fail(CHQ_ERR_ARG, "bad argument");
-  for (int q = 0; q < n; ++q)
-    if (meshes[q] && meshes[q]->diff && meshes[q]->cfg.sts)
-      return fail(CHQ_ERR_ARG, "batched stepping covers explicit diffusion only; step meshes with RKL2 "
-                               "super-time-stepping (diffusion.sts) one by one");
   *out = nullptr;
   const chq_mesh *a = meshes[0];
   for (int j = 0; j < n; ++j) {
@@ -2425,9 +2459,10 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
         m->cfg.flux_limiter != a->cfg.flux_limiter)
       return fail(CHQ_ERR_ARG, "batch members must share precision, reconstruction, Riemann solver, "
                                "characteristic flag, integrator, FOFC and limiter switches");
-    if (m->diff != a->diff || (m->cfg.cooling != 0) != (a->cfg.cooling != 0) || grav_on(m) != grav_on(a))
-      return fail(CHQ_ERR_ARG, "batch members must agree on explicit diffusion, cooling and gravity (on or "
-                               "off; their coefficients may differ)");
+    if (m->diff != a->diff || (m->cfg.cooling != 0) != (a->cfg.cooling != 0) || grav_on(m) != grav_on(a) ||
+        sts_on(m) != sts_on(a))
+      return fail(CHQ_ERR_ARG, "batch members must agree on diffusion, RKL2 super-time-stepping, cooling and "
+                               "gravity (on or off; their coefficients may differ)");
     for (int q = 0; q < j; ++q)
       if (meshes[q] == m) return fail(CHQ_ERR_ARG, "a mesh appears twice in the batch");
   }
@@ -2440,9 +2475,10 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   B->nstage = a->nstage;
   B->fofc = a->cfg.fofc;
   B->limiter = a->cfg.flux_limiter;
-  B->diff = a->diff ? 1 : 0;
+  B->diff = (a->diff && !a->cfg.sts) ? 1 : 0;   // explicit diffusion inside the stages
   B->cool = a->cfg.cooling ? 1 : 0;
   B->grav = grav_on(a) ? 1 : 0;
+  B->sts = sts_on(a) ? 1 : 0;
   int rc = B->mixed ? batch_build<float>(B) : batch_build<double>(B);
   if (rc == CHQ_OK) {
     cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
@@ -2478,7 +2514,7 @@ int chq_batch_cycles(chq_batch *B, int n, void *stream) {
   // members' own streams may still hold work (uploads, prime): order after them
   for (chq_mesh *m : B->jobs) CHQ_CUDA(cudaStreamSynchronize(m->stream));
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : B->stream;
-  if (!B->use_graph) {
+  if (!B->use_graph || B->sts) {   // RKL2 batches take host decisions every cycle: no graph
     for (int c = 0; c < n; ++c) {
       const int rc = B->mixed ? batch_cycle<float>(B, s) : batch_cycle<double>(B, s);
       if (rc) return rc;

@@ -12,12 +12,11 @@
 //      with the fewest cells; each lane has its own stream and replays a CUDA graph, so the
 //      flux kernel of one lane overlaps the memory-bound kernels of another. Batching alone
 //      serialises every job through the same kernel sequence.
-// Jobs of 2^21 cells or more (chq_server_set_solo_cells), and jobs with RKL2
-// super-time-stepping, are not batched: each runs "solo" on its own mesh stream (replaying a
-// CUDA graph of one cycle, except RKL2) and the
+// Jobs of 2^21 cells or more (chq_server_set_solo_cells) are not batched: each runs "solo" on
+// its own mesh stream (replaying a CUDA graph of one cycle, except with RKL2) and the
 // server polls an event behind its chunk instead of waiting for it, so a large job never holds
-// up the lanes (or another large job). Explicit diffusion, cooling and gravity batch with
-// jobs that have the same terms switched on.
+// up the lanes (or another large job). Diffusion (explicit or RKL2), cooling and gravity
+// batch with jobs that have the same terms switched on.
 // Each job keeps its own dt and clock on the device, so its result is the same alone and in
 // any mix. Times are seconds on the server's steady clock.
 #include <chrono>
@@ -73,13 +72,14 @@ void free_solo(Job *j) {
 }
 
 // (precision, reconstruction, Riemann solver, characteristic, integrator, FOFC, limiter,
-//  explicit diffusion | cooling << 1 | gravity << 2, lane)
+//  diffusion | cooling << 1 | gravity << 2 | RKL2 << 3, lane)
 using ClassKey = std::tuple<int, int, int, int, int, int, int, int, int>;
 
 bool has_diffusion(const chq_config &c) { return c.nu > 0 || c.kappa > 0 || c.eta > 0; }
 
 int features(const chq_config &c) {
-  return (has_diffusion(c) ? 1 : 0) | (c.cooling ? 2 : 0) | ((c.gravity_uniform || c.gravity_point) ? 4 : 0);
+  return (has_diffusion(c) ? 1 : 0) | (c.cooling ? 2 : 0) | ((c.gravity_uniform || c.gravity_point) ? 4 : 0) |
+         ((has_diffusion(c) && c.sts) ? 8 : 0);
 }
 
 ClassKey key_of(const chq_config &c, int lane) {
@@ -283,8 +283,7 @@ void admit(chq_server *S) {
     S->used += j->bytes;
     j->state = CHQ_JOB_RUNNING;
     j->t_start = S->now();
-    // RKL2 super-time-stepping takes a host decision every cycle: such jobs never batch
-    if (j->cells >= S->solo_cells || (has_diffusion(j->cfg) && j->cfg.sts)) {
+    if (j->cells >= S->solo_cells) {
       j->solo = true;
       S->solo.push_back(j);
       ++active;

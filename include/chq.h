@@ -218,13 +218,15 @@ CHQ_API int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launch
 /* ---- batched stepping of many meshes (no reference counterpart: the reference steps one
  * mesh at a time) ---------------------------------------------------------------------------
  * A batch groups primed meshes of one class (same precision, reconstruction, Riemann solver,
- * characteristic flag, integrator, FOFC and limiter switches, and explicit diffusion,
- * cooling and gravity either on in every member or off in every member; coefficients may
- * differ) of any sizes and dimensions and advances all of them with one launch per kernel
- * kind per stage, the blocks of every member in the same grid. Each member keeps its own dt
- * (the parabolic limit included), clock, boundaries and FOFC decisions, and stops at its own
- * tlim, so its results are identical to stepping it alone. Meshes with RKL2
- * super-time-stepping are refused (their stage count is a host decision every cycle).
+ * characteristic flag, integrator, FOFC and limiter switches, and diffusion, RKL2
+ * super-time-stepping, cooling and gravity either on in every member or off in every
+ * member; coefficients may differ) of any sizes and dimensions and advances all of them with
+ * one launch per kernel kind per stage, the blocks of every member in the same grid. Each
+ * member keeps its own dt (the parabolic limit included), clock, boundaries and FOFC
+ * decisions, and stops at its own tlim, so its results are identical to stepping it alone.
+ * With RKL2 the stage count of every member is a host decision each cycle: the batch
+ * synchronises once per cycle and runs each member's super-time-stepping stages with its own
+ * launches (no graph replay for such batches).
  * Membership is fixed at creation; meshes must outlive the batch. */
 typedef struct chq_batch chq_batch;
 CHQ_API int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out);
@@ -247,9 +249,9 @@ CHQ_API void *chq_batch_stream(chq_batch *b);
  * launches cycles_per_step batched cycles of every class. Each class is split into up to
  * `lanes` batches (default 8) of balanced cell counts, each on its own stream as a replayed
  * CUDA graph, so that the memory-bound kernels of one lane overlap the flux kernel of another.
- * Jobs of 2^21 cells or more, and jobs with RKL2 super-time-stepping, run solo on their own
- * mesh stream; the server polls an event behind each solo chunk instead of waiting for it.
- * Jobs with explicit diffusion, cooling or gravity batch with jobs that have the same terms.
+ * Jobs of 2^21 cells or more run solo on their own mesh stream; the server polls an event
+ * behind each solo chunk instead of waiting for it. Jobs with diffusion (explicit or RKL2),
+ * cooling or gravity batch with jobs that have the same terms.
  * A job whose final state is not finite is reported FAILED; kernels index only their own
  * job, so it never disturbs the others. Times are seconds on the server clock. */
 enum { CHQ_JOB_QUEUED = 0, CHQ_JOB_RUNNING = 1, CHQ_JOB_DONE = 2, CHQ_JOB_FAILED = 3 };

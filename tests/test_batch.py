@@ -58,6 +58,15 @@ SETS.update({
     "cooling_fp64": [(cases.ot(32), ("cooling.enabled=true", "cooling.lambda0=0.5")),
                      (cases.blast(16), ("cooling.enabled=true", "cooling.lambda0=5.0", "cooling.alpha=2.0",
                                         "cooling.tfloor=0.05"))],
+    # RKL2: the batched stages, then each member's own super-time-stepping stages
+    "rkl2_fp64": [(cases.ot(32), ("diffusion.eta=0.02", "diffusion.sts=true")),
+                  (cases.diffusion("temp", 1, 32, 8), ("diffusion.kappa=0.02", "diffusion.sts=true",
+                                                      "mhd.reconstruct=ppm")),
+                  (cases.blast(16), STRONG + ("diffusion.nu=5e-3", "diffusion.eta=5e-3", "diffusion.sts=true"))],
+    "rkl2_cooling_fp64": [(cases.ot(32), ("diffusion.eta=0.02", "diffusion.sts=true", "cooling.enabled=true",
+                                          "cooling.lambda0=0.2")),
+                          (cases.blast(16), ("diffusion.nu=2e-3", "diffusion.sts=true", "cooling.enabled=true",
+                                             "cooling.lambda0=1.0"))],
     "all_terms_fp64": [(cases.ot(32), GRAV_U + ("cooling.enabled=true", "cooling.lambda0=0.2", "diffusion.nu=2e-3",
                                                 "diffusion.kappa=2e-3")),
                        (cases.blast(16), STRONG + GRAV_P + ("cooling.enabled=true", "cooling.lambda0=1.0",
@@ -135,9 +144,11 @@ def test_batch_rejects_mixed_classes():
         Batch([a, c])
     with pytest.raises(ChqError):
         Batch([a, a])
-    # source terms and diffusion on in every member or in none; no RKL2 members
-    for ov in (GRAV_U, ("cooling.enabled=true", "cooling.lambda0=0.5"), ("diffusion.nu=1e-3",)):
+    # source terms, diffusion and RKL2 on in every member or in none
+    sts = ("diffusion.eta=1e-3", "diffusion.sts=true")
+    for ov in (GRAV_U, ("cooling.enabled=true", "cooling.lambda0=0.5"), ("diffusion.nu=1e-3",), sts):
         with pytest.raises(ChqError):
             Batch([a, _mesh(cases.ot(16), ov)])
     with pytest.raises(ChqError):
-        Batch([_mesh(cases.ot(16), ("diffusion.eta=1e-3", "diffusion.sts=true"))])
+        Batch([_mesh(cases.ot(16), ("diffusion.eta=1e-3",)), _mesh(cases.ot(16), sts)])
+    Batch([_mesh(cases.ot(16), sts)]).close()

@@ -109,10 +109,9 @@ def test_decay_rate_matches_exact_solution():
     assert ratio == pytest.approx(np.exp(-0.02 * k * k * t), rel=2e-3)
 
 
-def test_batch_refuses_rkl2_and_mixed_diffusion():
-    """Explicit diffusion batches (tests/test_batch.py); RKL2 meshes do not, since their
-    stage count is a host decision every cycle, and a batch has diffusion in every member or
-    in none. The server runs RKL2 jobs unbatched (tests/test_server.py)."""
+def test_batch_groups_diffusion_by_switch():
+    """Explicit diffusion and RKL2 meshes batch (tests/test_batch.py checks the results), each
+    only with meshes that have the same switches."""
     from chasqui_b200 import Batch, ChqError
     text, ov = CASES["ot2d_all"]
     _, mesh = make_pair(text, ov)
@@ -121,5 +120,6 @@ def test_batch_refuses_rkl2_and_mixed_diffusion():
     with pytest.raises(ChqError):
         Batch([mesh, plain])
     _, sts = make_pair(text, list(ov) + ["diffusion.sts=true"])
+    Batch([sts]).close()
     with pytest.raises(ChqError):
-        Batch([sts])
+        Batch([mesh, sts])
