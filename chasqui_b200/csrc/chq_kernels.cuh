@@ -27,6 +27,8 @@ template <class P> struct EmfArgs {
   P *e1, *e2, *e3;
   const int *done;   // skip when nonzero
   const int *need;   // run only when *need != 0 (FOFC re-run); null = always
+  const int *list;   // FOFC re-run: the stage's flagged cells (count *need, first `cap` listed)
+  int cap;
 };
 
 template <class P> CHQ_D P upwind(P flux, P left, P right) {
@@ -34,13 +36,10 @@ template <class P> CHQ_D P upwind(P flux, P left, P right) {
   return (flux > tol) ? left : (flux < -tol) ? right : P(0.5) * (left + right);
 }
 
-template <class P> CHQ_D void corner_emf_body(const EmfArgs<P> &A, int bx, int by, int bz) {
-  if (A.done && *A.done) return;
-  if (A.need && *A.need == 0) return;
+// The edge EMFs stored at point (k, j, i): E1 at (k-1/2, j-1/2, i), E2 at (k-1/2, j, i-1/2),
+// E3 at (k, j-1/2, i-1/2), each where it is in range (src/physics.hpp:242-297).
+template <class P> CHQ_D void corner_point(const EmfArgs<P> &A, int k, int j, int i) {
   const Geom &g = A.g;
-  const int i = g.is + bx * blockDim.x + threadIdx.x;
-  const int j = g.js + by * blockDim.y + threadIdx.y;
-  const int k = g.ks + bz;
   const long vs = g.vstride;
   const long sj = g.sj, sk = g.sk;
   if (i > g.ie + 1) return;
@@ -92,7 +91,49 @@ template <class P> CHQ_D void corner_emf_body(const EmfArgs<P> &A, int bx, int b
   }
 }
 
+template <class P> CHQ_D void corner_emf_body(const EmfArgs<P> &A, int bx, int by, int bz) {
+  if (A.done && *A.done) return;
+  if (A.need && *A.need == 0) return;
+  const Geom &g = A.g;
+  corner_point<P>(A, g.ks + bz, g.js + by * (int)blockDim.y + (int)threadIdx.y, g.is + bx * (int)blockDim.x + (int)threadIdx.x);
+}
+
 template <class P> __global__ void __launch_bounds__(256) corner_emf_kernel(const EmfArgs<P> A) { corner_emf_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+
+// FOFC re-run of the corner EMFs (no explicit diffusion: the edges are overwritten, never
+// accumulated). A repaired face is a face of a listed cell and only the edges of the repaired
+// faces see new inputs, so recomputing the points of the listed cells' edges (k..k+1, j..j+1,
+// i..i+1; k..k only below 3D) gives every edge the value a full re-run gives it; the other
+// edges keep values equal to it. Without a usable list every point is recomputed.
+template <class P> CHQ_D void corner_rerun_body(const EmfArgs<P> &A, int bx, int nbx) {
+  if (A.done && *A.done) return;
+  const int nb = *A.need;
+  if (nb == 0) return;
+  const Geom &g = A.g;
+  const int tid = bx * (int)blockDim.x + (int)threadIdx.x, nth = nbx * (int)blockDim.x;
+  const int nzk = g.three_d ? 2 : 1;
+  if (A.list && nb > 0 && nb <= A.cap) {
+    const int per = 4 * nzk, sj = (int)g.sj, sk = (int)g.sk;
+    for (int it = tid; it < per * nb; it += nth) {
+      const int q = it / per, p = it - per * q;
+      const int c = A.list[q];
+      const int k = c / sk, r = c - k * sk, j = r / sj, i = r - j * sj;
+      corner_point<P>(A, k + (p >> 2), j + ((p >> 1) & 1), i + (p & 1));
+    }
+    return;
+  }
+  const int ni = g.ie + 2 - g.is, nj = g.je + 2 - g.js, nk = g.three_d ? g.ke + 2 - g.ks : 1;
+  const long tot = (long)ni * nj * nk;
+  for (long t = tid; t < tot; t += nth) {
+    const int i = g.is + (int)(t % ni);
+    const long r = t / ni;
+    corner_point<P>(A, g.ks + (int)(r / nj), g.js + (int)(r % nj), i);
+  }
+}
+
+template <class P> __global__ void __launch_bounds__(256) corner_rerun_kernel(const EmfArgs<P> A) {
+  corner_rerun_body<P>(A, blockIdx.x, gridDim.x);
+}
 
 // ---------------------------------------------------------------------------------------
 // K3. Each thread owns one (k, j, i) of the face/edge frame: the cell update when (k, j, i)
@@ -731,6 +772,12 @@ template <class P> __global__ void __launch_bounds__(256) corner_emf_batched(con
   __shared__ __align__(16) unsigned char sa[sizeof(EmfArgs<P>)];
   const EmfArgs<P> &A = stage_args(args, j, sa);
   corner_emf_body<P>(A, bx, by, bz);
+}
+template <class P> __global__ void __launch_bounds__(256) corner_rerun_batched(const EmfArgs<P> *args, const BatchSlot *slots, int n) {
+  const int j = batch_job(slots, n, blockIdx.x);
+  __shared__ __align__(16) unsigned char sa[sizeof(EmfArgs<P>)];
+  const EmfArgs<P> &A = stage_args(args, j, sa);
+  corner_rerun_body<P>(A, (int)(blockIdx.x - slots[j].off), slots[j].gx);
 }
 template <class P, bool GRAV> __global__ void __launch_bounds__(256) update_batched(const UpdateArgs<P> *args, const BatchSlot *slots, int n) {
   int bx, by, bz;

@@ -401,6 +401,8 @@ EmfArgs<P> corner_args(chq_mesh *m, const int *done, const int *need) {
   a.e1 = as<P>(m->e[0]); a.e2 = as<P>(m->e[1]); a.e3 = as<P>(m->e[2]);
   a.done = done;
   a.need = need;
+  a.list = m->bad_list;
+  a.cap = m->bad_cap;
   return a;
 }
 
@@ -417,6 +419,21 @@ int do_corner(chq_mesh *m, const int *done, const int *need, cudaStream_t s) {
   const Launch3 L = corner_grid(m);
   m->nlaunch += 1;
   corner_emf_kernel<P><<<L.grid, L.block, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+Launch3 repair_grid(long faces, long max_blocks);
+
+// FOFC re-run of the corner EMFs over the edges of the flagged cells only (need = the
+// device count of flagged cells); grid-stride, at most kRepairBlocks blocks
+template <class P>
+int do_corner_rerun(chq_mesh *m, const int *done, const int *need, cudaStream_t s) {
+  const EmfArgs<P> a = corner_args<P>(m, done, need);
+  const Geom &g = m->g;
+  const long pts = (long)(g.ie + 2 - g.is) * (g.je + 2 - g.js) * (g.three_d ? g.ke + 2 - g.ks : 1);
+  m->nlaunch += 1;
+  corner_rerun_kernel<P><<<repair_grid(pts, kRepairBlocks).grid, 256, 0, s>>>(a);
   CHQ_CUDA(cudaGetLastError());
   return CHQ_OK;
 }
@@ -865,7 +882,10 @@ int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, c
     if (m->mixed) rc = do_repair_d<float>(m, cur, dstage, done, nbad, s);
     else rc = do_repair_d<double>(m, cur, dstage, done, nbad, s);
     if (rc) return rc;
-    if ((rc = DISPATCH_P(m, do_corner)(m, done, nbad, s))) return rc;
+    // with explicit diffusion eta J is added to every edge afterwards, so every edge is redone
+    if (dstage) rc = DISPATCH_P(m, do_corner)(m, done, nbad, s);
+    else rc = DISPATCH_P(m, do_corner_rerun)(m, done, nbad, s);
+    if (rc) return rc;
     if (dstage && (rc = DISPATCH_P(m, do_res_emf)(m, bc1, bc2, bc3, done, nbad, s))) return rc;
     if ((rc = DISPATCH_P(m, do_update)(m, out, g0, g1, bdt, bdt_dev, done, nbad, s))) return rc;
   }
@@ -1193,7 +1213,7 @@ struct chq_batch {
   // the update epilogue; cooling is split after the step
   int diff = 0, grav = 0, cool = 0;
   int sts = 0;   // RKL2 members: their super-time-stepping stages run per member after the batched stages
-  Kind k_diff, k_res, k_rho, k_cool;
+  Kind k_diff, k_res, k_rho, k_cool, k_corner_rerun;
   void *a_diff[4] = {}, *a_res[4] = {}, *a_res_need[4] = {};
   void *a_rho = nullptr, *a_cool = nullptr, *a_c2p_split[2] = {}, *a_bc0[3] = {};
   void *a_flux[4] = {}, *a_update[4] = {}, *a_update_need[4] = {}, *a_repair[4] = {}, *a_limit[4] = {},
@@ -1277,6 +1297,11 @@ int batch_build(chq_batch *B) {
     return linear(tot, 256);
   }, B->k_diff.nblocks);
   const size_t o_res_s = slots_of(h, J, [](chq_mesh *m) { return res_emf_grid(m); }, B->k_res.nblocks);
+  const size_t o_crr_s = slots_of(h, J, [](chq_mesh *m) {
+    const Geom &g = m->g;
+    const long pts = (long)(g.ie + 2 - g.is) * (g.je + 2 - g.js) * (g.three_d ? g.ke + 2 - g.ks : 1);
+    return repair_grid(pts, kRepairBlocksBatched);
+  }, B->k_corner_rerun.nblocks);
   const size_t o_rho_s = slots_of(h, J, [](chq_mesh *m) {
     return m->diff ? active_grid(m) : Launch3{dim3(0, 1, 1), dim3(32, 8)};
   }, B->k_rho.nblocks);
@@ -1384,6 +1409,7 @@ int batch_build(chq_batch *B) {
   B->status = (double *)(d + o_status);
   B->k_diff.slots = (BatchSlot *)(d + o_diff_s);
   B->k_res.slots = (BatchSlot *)(d + o_res_s);
+  B->k_corner_rerun.slots = (BatchSlot *)(d + o_crr_s);
   B->k_rho.slots = (BatchSlot *)(d + o_rho_s);
   B->k_cool.slots = (BatchSlot *)(d + o_cool_s);
   B->a_rho = d + o_rho;
@@ -1497,7 +1523,11 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
       CHQ_CUDA(cudaGetLastError());
       fofc_repair_batched<P><<<(unsigned)B->k_repair.nblocks, 256, 0, s>>>((const RepairArgs<P> *)B->a_repair[st], B->k_repair.slots, n);
       CHQ_CUDA(cudaGetLastError());
-      corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner_need, B->k_corner.slots, n);
+      // (with explicit diffusion eta J is added to every edge afterwards: every edge is redone)
+      if (B->diff)
+        corner_emf_batched<P><<<(unsigned)B->k_corner.nblocks, b2, 0, s>>>((const EmfArgs<P> *)B->a_corner_need, B->k_corner.slots, n);
+      else
+        corner_rerun_batched<P><<<(unsigned)B->k_corner_rerun.nblocks, 256, 0, s>>>((const EmfArgs<P> *)B->a_corner_need, B->k_corner_rerun.slots, n);
       CHQ_CUDA(cudaGetLastError());
       L += 3;
       CHQ_CUDA(res_emf(B->a_res_need[st]));
