@@ -1,5 +1,6 @@
-/* Oracle (test infrastructure): a plain-C restatement of Chasqui's per-RK-stage ideal-MHD
- * path, written per face like the published algorithm, on the reference's packed
+/* Oracle (test infrastructure): a plain-C restatement of Chasqui's per-RK-stage MHD path
+ * (ideal MHD, explicit diffusion, RKL2, gravity, cooling), written per face like the
+ * published algorithm, on the reference's packed
  * LayoutRight arrays (cells (ncomp,nk,nj,ni), faces/edges (ncomp,nk+1,nj+1,ni+1)).
  * Every function cites the reference file:line it restates. It is pinned against the
  * reference's own kernels (oracle/_ref) by tests/test_oracle_port.py. The product never
@@ -14,6 +15,14 @@ typedef struct port_cfg {
   int bc[3];
   double gamma, dfloor, pfloor, cfl, de_eta, lhlld_phi, tlim;
   int dual_energy, low_mach, flatten, characteristic, fofc, flux_limiter;
+  /* explicit diffusion / RKL2 (src/diffusion.hpp, src/sts.hpp) and source terms
+   * (src/srcterms.hpp); zero = off */
+  double nu, kappa, eta;
+  int sts;
+  int grav_uniform, grav_point;
+  double g1, g2, g3, gm, gx0, gy0, gz0, rsoft;
+  int cooling;
+  double lambda0, cool_alpha, tfloor;
 } port_cfg;
 
 typedef struct port_mesh port_mesh;
@@ -39,6 +48,7 @@ void port_prime(port_mesh *m, double t);
 int port_cycles(port_mesh *m, int n);
 void port_clock(port_mesh *m, double *t, int *cycle, double *min_dt, long *fofc_count);
 void port_history(port_mesh *m, double out[10]);
+long port_sts_stages(port_mesh *m);   /* RKL2 stages taken so far */
 
 /* point functions */
 void port_recon(int scheme, const double q[6], double *ql, double *qr);

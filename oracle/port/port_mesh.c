@@ -19,7 +19,10 @@ struct port_mesh {
   int *flag;
   double t, min_dt;
   int cycle;
-  long fofc_count, limiter_count;
+  long fofc_count, limiter_count, sts_stages;
+  /* RKL2 scratch (src/sts.hpp:16-31), allocated on first use: three states, two operator
+   * values, each with three face fields */
+  double *sy[3], *sm[2], *syb[3][3], *smb[2][3];
 };
 
 /* cell (n,k,j,i) and face/edge (n,k,j,i) linear indices of the packed layouts */
@@ -66,6 +69,12 @@ void port_destroy(port_mesh *m) {
   free(m->u[0]); free(m->u[1]); free(m->w); free(m->bcc); free(m->ecc); free(m->flag);
   for (q = 0; q < 3; ++q) {
     free(m->b[0][q]); free(m->b[1][q]); free(m->f[q]); free(m->et2[q]); free(m->et1[q]); free(m->e[q]);
+    free(m->sy[q]);
+    for (int r = 0; r < 3; ++r) free(m->syb[q][r]);
+  }
+  for (q = 0; q < 2; ++q) {
+    free(m->sm[q]);
+    for (int r = 0; r < 3; ++r) free(m->smb[q][r]);
   }
   free(m);
 }
@@ -364,9 +373,8 @@ void port_update(port_mesh *m, int out, double g0, double g1, double bdt) {
 #undef F
 }
 
-/* Boundaries (src/physics.hpp:354-432); the three directions in order */
-void port_boundaries(port_mesh *m, int buf) {
-  double *u = m->u[buf], *b1 = m->b[buf][0], *b2 = m->b[buf][1], *b3 = m->b[buf][2];
+/* Boundaries (src/physics.hpp:354-432) of any state; the three directions in order */
+static void bc_on(port_mesh *m, double *u, double *b1, double *b2, double *b3) {
   const int ng = m->ng;
   int k;
 #define F(a, k, j, i) (a)[FI(m, 0, k, j, i)]
@@ -452,10 +460,11 @@ void port_boundaries(port_mesh *m, int buf) {
 #undef F
 }
 
-/* ConsToPrim (src/physics.hpp:437-494); returns min dt over active cells (huge if none) */
-double port_cons_to_prim(port_mesh *m, int buf, int compute_dt) {
-  double *u = m->u[buf];
-  const double *b1 = m->b[buf][0], *b2 = m->b[buf][1], *b3 = m->b[buf][2];
+void port_boundaries(port_mesh *m, int buf) { bc_on(m, m->u[buf], m->b[buf][0], m->b[buf][1], m->b[buf][2]); }
+
+/* ConsToPrim (src/physics.hpp:437-494) of any state; returns min dt over active cells (huge
+ * if none) */
+static double c2p_on(port_mesh *m, double *u, const double *b1, const double *b2, const double *b3, int compute_dt) {
   const port_cfg *c = &m->c;
   double mdt = 1.79769313486231570815e+308;
   int k;
@@ -504,6 +513,346 @@ double port_cons_to_prim(port_mesh *m, int buf, int compute_dt) {
   return mdt;
 }
 
+double port_cons_to_prim(port_mesh *m, int buf, int compute_dt) {
+  return c2p_on(m, m->u[buf], m->b[buf][0], m->b[buf][1], m->b[buf][2], compute_dt);
+}
+
+/* ---- explicit diffusion (src/diffusion.hpp) ----------------------------------------- */
+static int diff_any(const port_mesh *m) { return m->c.nu > 0 || m->c.kappa > 0 || m->c.eta > 0; }
+
+/* edge current density from face fields (src/diffusion.hpp:24-44): J1 at (k-1/2, j-1/2, i),
+ * J2 at (k-1/2, j, i-1/2), J3 at (k, j-1/2, i-1/2) */
+typedef struct { const double *b1, *b2, *b3; double idx1, idx2, idx3; } curl_ctx;
+#define FB(a, k, j, i) (a)[FI(m, 0, k, j, i)]
+static double cur1(const port_mesh *m, const curl_ctx *J, int k, int j, int i) {
+  double r = 0.0;
+  if (m->two_d) r += (FB(J->b3, k, j, i) - FB(J->b3, k, j - 1, i)) * J->idx2;
+  if (m->three_d) r -= (FB(J->b2, k, j, i) - FB(J->b2, k - 1, j, i)) * J->idx3;
+  return r;
+}
+static double cur2(const port_mesh *m, const curl_ctx *J, int k, int j, int i) {
+  double r = -(FB(J->b3, k, j, i) - FB(J->b3, k, j, i - 1)) * J->idx1;
+  if (m->three_d) r += (FB(J->b1, k, j, i) - FB(J->b1, k - 1, j, i)) * J->idx3;
+  return r;
+}
+static double cur3(const port_mesh *m, const curl_ctx *J, int k, int j, int i) {
+  double r = (FB(J->b2, k, j, i) - FB(J->b2, k, j, i - 1)) * J->idx1;
+  if (m->two_d) r -= (FB(J->b1, k, j, i) - FB(J->b1, k, j - 1, i)) * J->idx2;
+  return r;
+}
+static curl_ctx curl_of(const port_mesh *m, const double *b1, const double *b2, const double *b3) {
+  curl_ctx J;
+  J.b1 = b1; J.b2 = b2; J.b3 = b3;
+  J.idx1 = 1.0 / m->dx1; J.idx2 = 1.0 / m->dx2; J.idx3 = 1.0 / m->dx3;
+  return J;
+}
+
+/* viscous, conductive and resistive-Poynting fluxes added to face (k, j, i) of direction dir
+ * (FaceCtx::Add, src/diffusion.hpp:74-136) */
+static void diff_face(port_mesh *m, int dir, const curl_ctx *J, int k, int j, int i) {
+  const int t1 = (dir + 1) % 3, t2 = (dir + 2) % 3;
+  const int has[3] = {1, m->two_d, m->three_d};
+  const int has1 = has[t1], has2 = has[t2];
+  const double idx[3] = {1.0 / m->dx1, 1.0 / m->dx2, 1.0 / m->dx3};
+  const double idn = idx[dir], idt1 = idx[t1], idt2 = idx[t2];
+  const int dk = (dir == 2), dj = (dir == 1), di = (dir == 0);
+  const int dk1 = (t1 == 2), dj1 = (t1 == 1), di1 = (t1 == 0), dk2 = (t2 == 2), dj2 = (t2 == 1), di2 = (t2 == 0);
+  const int IVU = 1 + dir, IVV = 1 + t1, IVW = 1 + t2;
+  const int kL = k - dk, jL = j - dj, iL = i - di;
+  const double *w = m->w;
+  double *flx = m->f[dir];
+#define W(n, kk, jj, ii) w[CI(m, n, kk, jj, ii)]
+  if (m->c.nu > 0) {
+    const double mu = m->c.nu * 0.5 * (W(IDN, kL, jL, iL) + W(IDN, k, j, i));
+    const double dun = (W(IVU, k, j, i) - W(IVU, kL, jL, iL)) * idn;
+    const double dvn = (W(IVV, k, j, i) - W(IVV, kL, jL, iL)) * idn;
+    const double dwn = (W(IVW, k, j, i) - W(IVW, kL, jL, iL)) * idn;
+    double dut1 = 0, dvt1 = 0, dut2 = 0, dwt2 = 0;
+    if (has1) {
+      dut1 = 0.25 * idt1 * ((W(IVU, k + dk1, j + dj1, i + di1) - W(IVU, k - dk1, j - dj1, i - di1)) +
+                            (W(IVU, kL + dk1, jL + dj1, iL + di1) - W(IVU, kL - dk1, jL - dj1, iL - di1)));
+      dvt1 = 0.25 * idt1 * ((W(IVV, k + dk1, j + dj1, i + di1) - W(IVV, k - dk1, j - dj1, i - di1)) +
+                            (W(IVV, kL + dk1, jL + dj1, iL + di1) - W(IVV, kL - dk1, jL - dj1, iL - di1)));
+    }
+    if (has2) {
+      dut2 = 0.25 * idt2 * ((W(IVU, k + dk2, j + dj2, i + di2) - W(IVU, k - dk2, j - dj2, i - di2)) +
+                            (W(IVU, kL + dk2, jL + dj2, iL + di2) - W(IVU, kL - dk2, jL - dj2, iL - di2)));
+      dwt2 = 0.25 * idt2 * ((W(IVW, k + dk2, j + dj2, i + di2) - W(IVW, k - dk2, j - dj2, i - di2)) +
+                            (W(IVW, kL + dk2, jL + dj2, iL + di2) - W(IVW, kL - dk2, jL - dj2, iL - di2)));
+    }
+    {
+      const double divv = dun + dvt1 + dwt2;
+      const double tnn = mu * (2.0 * dun - (2.0 / 3.0) * divv);
+      const double tnt1 = mu * (dvn + dut1), tnt2 = mu * (dwn + dut2);
+      const double uf = 0.5 * (W(IVU, kL, jL, iL) + W(IVU, k, j, i));
+      const double vf = 0.5 * (W(IVV, kL, jL, iL) + W(IVV, k, j, i));
+      const double wf = 0.5 * (W(IVW, kL, jL, iL) + W(IVW, k, j, i));
+      flx[FI(m, IVU, k, j, i)] -= tnn;
+      flx[FI(m, IVV, k, j, i)] -= tnt1;
+      flx[FI(m, IVW, k, j, i)] -= tnt2;
+      flx[FI(m, IEN, k, j, i)] -= tnn * uf + tnt1 * vf + tnt2 * wf;
+    }
+  }
+  if (m->c.kappa > 0) {
+    const double tL = W(4, kL, jL, iL) / W(IDN, kL, jL, iL), tR = W(4, k, j, i) / W(IDN, k, j, i);
+    flx[FI(m, IEN, k, j, i)] -= m->c.kappa * (tR - tL) * idn;
+  }
+  if (m->c.eta > 0) {
+    const double eta = m->c.eta;
+    double et1, et2;
+    if (dir == 0) {
+      et1 = eta * 0.5 * (cur2(m, J, k, j, i) + (has2 ? cur2(m, J, k + 1, j, i) : cur2(m, J, k, j, i)));
+      et2 = eta * 0.5 * (cur3(m, J, k, j, i) + (has1 ? cur3(m, J, k, j + 1, i) : cur3(m, J, k, j, i)));
+    } else if (dir == 1) {
+      et1 = eta * 0.5 * (cur3(m, J, k, j, i) + cur3(m, J, k, j, i + 1));
+      et2 = eta * 0.5 * (cur1(m, J, k, j, i) + (has1 ? cur1(m, J, k + 1, j, i) : cur1(m, J, k, j, i)));
+    } else {
+      et1 = eta * 0.5 * (cur1(m, J, k, j, i) + cur1(m, J, k, j + 1, i));
+      et2 = eta * 0.5 * (cur2(m, J, k, j, i) + cur2(m, J, k, j, i + 1));
+    }
+    {
+      const double bt1 = 0.5 * (m->bcc[CI(m, t1, kL, jL, iL)] + m->bcc[CI(m, t1, k, j, i)]);
+      const double bt2 = 0.5 * (m->bcc[CI(m, t2, kL, jL, iL)] + m->bcc[CI(m, t2, k, j, i)]);
+      flx[FI(m, IEN, k, j, i)] += et1 * bt2 - et2 * bt1;
+    }
+  }
+#undef W
+}
+
+/* diffusive fluxes on the faces of the active cells of one direction (src/diffusion.hpp:139-146) */
+static void diff_fluxes(port_mesh *m, int dir, const double *b1, const double *b2, const double *b3) {
+  const curl_ctx J = curl_of(m, b1, b2, b3);
+  const int iu = (dir == 0) ? m->ie + 1 : m->ie, ju = (dir == 1) ? m->je + 1 : m->je, ku = (dir == 2) ? m->ke + 1 : m->ke;
+  int k;
+  if (!diff_any(m)) return;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (k = m->ks; k <= ku; ++k)
+    for (int j = m->js; j <= ju; ++j)
+      for (int i = m->is; i <= iu; ++i) diff_face(m, dir, &J, k, j, i);
+}
+
+/* eta J added to the edge EMFs (src/diffusion.hpp:149-161) */
+static void res_emf(port_mesh *m, const double *b1, const double *b2, const double *b3) {
+  const curl_ctx J = curl_of(m, b1, b2, b3);
+  const int ku = m->three_d ? m->ke + 1 : m->ks + 1, ju = m->two_d ? m->je + 1 : m->js + 1;
+  const double eta = m->c.eta;
+  int k;
+  if (!(eta > 0)) return;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (k = m->ks; k <= ku; ++k)
+    for (int j = m->js; j <= ju; ++j)
+      for (int i = m->is; i <= m->ie + 1; ++i) {
+        if (i <= m->ie) FB(m->e[0], k, j, i) += eta * cur1(m, &J, k, j, i);
+        if (j <= m->je || !m->two_d) FB(m->e[1], k, j, i) += eta * cur2(m, &J, k, j, i);
+        if (k <= m->ke || !m->three_d) FB(m->e[2], k, j, i) += eta * cur3(m, &J, k, j, i);
+      }
+}
+
+/* parabolic time-step limit over the active cells (src/diffusion.hpp:164-174) */
+static double parabolic_dt(port_mesh *m) {
+  const int ndim = 1 + m->two_d + m->three_d;
+  double dxmin = m->dx1, rho_min = 1e300, chi, dmax;
+  int k;
+  if (!diff_any(m)) return 1e300;
+  if (m->two_d) dxmin = fmin(dxmin, m->dx2);
+  if (m->three_d) dxmin = fmin(dxmin, m->dx3);
+#pragma omp parallel for collapse(2) schedule(static) reduction(min : rho_min)
+  for (k = m->ks; k <= m->ke; ++k)
+    for (int j = m->js; j <= m->je; ++j)
+      for (int i = m->is; i <= m->ie; ++i) rho_min = fmin(rho_min, m->w[CI(m, IDN, k, j, i)]);
+  chi = (m->c.kappa > 0) ? m->c.kappa * m->gm1 / rho_min : 0.0;
+  dmax = fmax(fmax(m->c.nu, m->c.eta), chi);
+  return dxmin * dxmin / (2.0 * ndim * dmax);
+}
+
+/* ---- source terms (src/srcterms.hpp) ------------------------------------------------- */
+/* gravity on the stage output with the stage primitives and beta*dt (srcterms.hpp:20-41) */
+static void gravity(port_mesh *m, double *uo, double bdt) {
+  const port_cfg *c = &m->c;
+  int k;
+  if (!(c->grav_uniform || c->grav_point)) return;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (k = m->ks; k <= m->ke; ++k)
+    for (int j = m->js; j <= m->je; ++j)
+      for (int i = m->is; i <= m->ie; ++i) {
+        double a1 = c->g1, a2 = c->g2, a3 = c->g3, d;
+        if (c->grav_point) {
+          const double dx = (c->x1min + (i - m->is + 0.5) * m->dx1) - c->gx0;
+          const double dy = m->two_d ? (c->x2min + (j - m->js + 0.5) * m->dx2) - c->gy0 : 0.0;
+          const double dz = m->three_d ? (c->x3min + (k - m->ks + 0.5) * m->dx3) - c->gz0 : 0.0;
+          const double r2 = dx * dx + dy * dy + dz * dz + c->rsoft * c->rsoft;
+          const double f = -c->gm / (r2 * sqrt(r2));
+          a1 += f * dx; a2 += f * dy; a3 += f * dz;
+        }
+        d = m->w[CI(m, IDN, k, j, i)];
+        uo[CI(m, IM1, k, j, i)] += bdt * d * a1;
+        uo[CI(m, IM2, k, j, i)] += bdt * d * a2;
+        uo[CI(m, IM3, k, j, i)] += bdt * d * a3;
+        uo[CI(m, IEN, k, j, i)] += bdt * d * (m->w[CI(m, 1, k, j, i)] * a1 + m->w[CI(m, 2, k, j, i)] * a2 +
+                                               m->w[CI(m, 3, k, j, i)] * a3);
+      }
+}
+
+/* exact power-law cooling of u over dt with the current primitives (srcterms.hpp:51-70) */
+static void cooling(port_mesh *m, double *u, double dt) {
+  const port_cfg *c = &m->c;
+  int k;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (k = m->ks; k <= m->ke; ++k)
+    for (int j = m->js; j <= m->je; ++j)
+      for (int i = m->is; i <= m->ie; ++i) {
+        const double d = m->w[CI(m, IDN, k, j, i)], p = m->w[CI(m, 4, k, j, i)];
+        const double t0 = p / d, cc = m->gm1 * d * c->lambda0;
+        double t1;
+        if (fabs(c->cool_alpha - 1.0) < 1e-12) {
+          t1 = t0 * exp(-cc * dt);
+        } else {
+          const double e = 1.0 - c->cool_alpha;
+          const double base = pow(t0, e) + (c->cool_alpha - 1.0) * cc * dt;
+          t1 = (base > 0.0) ? pow(base, 1.0 / e) : c->tfloor;
+        }
+        t1 = fmax(t1, c->tfloor);
+        u[CI(m, IEN, k, j, i)] += d * (t1 - t0) / m->gm1;
+      }
+}
+
+/* ---- RKL2 super-time-stepping (src/sts.hpp) ------------------------------------------ */
+static int sts_count(double tau, double dt_par) {   /* Stages, sts.hpp:35-39 */
+  const double r = tau / dt_par;
+  const int s = (int)ceil(0.5 * (-1.0 + sqrt(9.0 + 16.0 * r)));
+  return (s < 2) ? 2 : s;
+}
+static double sts_bj(int j) { return (j <= 2) ? 1.0 / 3.0 : ((double)j * j + j - 2.0) / (2.0 * j * (j + 1.0)); }
+
+/* M(U, B) = -div F_diff, -curl(eta J) of the state whose primitives are in m->w, face fields
+ * b (Operator, sts.hpp:43-96) */
+static void sts_op(port_mesh *m, double *const b[3], double *mu, double *const mb[3]) {
+  const double idx1 = 1.0 / m->dx1, idx2 = 1.0 / m->dx2, idx3 = 1.0 / m->dx3;
+  int q, k;
+  for (q = 0; q < 3; ++q) {
+    memset(m->f[q], 0, NVAR * m->nface * sizeof(double));
+    memset(m->e[q], 0, m->nface * sizeof(double));
+  }
+  diff_fluxes(m, 0, b[0], b[1], b[2]);
+  if (m->two_d) diff_fluxes(m, 1, b[0], b[1], b[2]);
+  if (m->three_d) diff_fluxes(m, 2, b[0], b[1], b[2]);
+  res_emf(m, b[0], b[1], b[2]);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (k = m->ks; k <= m->ke + 1; ++k)
+    for (int j = m->js; j <= m->je + 1; ++j)
+      for (int i = m->is; i <= m->ie + 1; ++i) {
+        const double *e1 = m->e[0], *e2 = m->e[1], *e3 = m->e[2];
+        if (i <= m->ie && j <= m->je && k <= m->ke)
+          for (int n = 0; n < NVAR; ++n) {
+            double d = (m->f[0][FI(m, n, k, j, i + 1)] - m->f[0][FI(m, n, k, j, i)]) * idx1;
+            if (m->two_d) d += (m->f[1][FI(m, n, k, j + 1, i)] - m->f[1][FI(m, n, k, j, i)]) * idx2;
+            if (m->three_d) d += (m->f[2][FI(m, n, k + 1, j, i)] - m->f[2][FI(m, n, k, j, i)]) * idx3;
+            mu[CI(m, n, k, j, i)] = -d;
+          }
+        if (j <= m->je && k <= m->ke) {
+          double c = 0.0;
+          if (m->two_d) c += (FB(e3, k, j + 1, i) - FB(e3, k, j, i)) * idx2;
+          if (m->three_d) c -= (FB(e2, k + 1, j, i) - FB(e2, k, j, i)) * idx3;
+          FB(mb[0], k, j, i) = -c;
+        }
+        if (i <= m->ie && k <= m->ke && (m->two_d || j == m->js)) {
+          double c = -(FB(e3, k, j, i + 1) - FB(e3, k, j, i)) * idx1;
+          if (m->three_d) c += (FB(e1, k + 1, j, i) - FB(e1, k, j, i)) * idx3;
+          FB(mb[1], k, j, i) = -c;
+          if (!m->two_d) FB(mb[1], k, j + 1, i) = -c;
+        }
+        if (i <= m->ie && j <= m->je && (m->three_d || k == m->ks)) {
+          double c = (FB(e2, k, j, i + 1) - FB(e2, k, j, i)) * idx1;
+          if (m->two_d) c -= (FB(e1, k, j + 1, i) - FB(e1, k, j, i)) * idx2;
+          FB(mb[2], k, j, i) = -c;
+          if (!m->three_d) FB(mb[2], k + 1, j, i) = -c;
+        }
+      }
+}
+
+/* out = ((a x + b y) + c z) + (d p + e q) on the active cells and the update-range faces
+ * (Combine / CombineB, sts.hpp:99-114) */
+static void sts_comb(port_mesh *m, double *out, double *const ob[3], double a, const double *x, double *const xb[3],
+                     double b, const double *y, double *const yb[3], double c, const double *z, double *const zb[3],
+                     double d, const double *p, double *const pb[3], double e, const double *q, double *const qb[3]) {
+  int k;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (k = m->ks; k <= m->ke; ++k)
+    for (int j = m->js; j <= m->je; ++j)
+      for (int i = m->is; i <= m->ie; ++i)
+        for (int n = 0; n < NVAR; ++n) {
+          const long l = CI(m, n, k, j, i);
+          out[l] = ((a * x[l] + b * y[l]) + c * z[l]) + (d * p[l] + e * q[l]);
+        }
+  for (int f = 0; f < 3; ++f) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (k = m->ks; k <= m->ke + 1; ++k)
+      for (int j = m->js; j <= m->je + 1; ++j)
+        for (int i = m->is; i <= m->ie + 1; ++i) {
+          const long l = FI(m, 0, k, j, i);
+          ob[f][l] = ((a * xb[f][l] + b * yb[f][l]) + c * zb[f][l]) + (d * pb[f][l] + e * qb[f][l]);
+        }
+  }
+}
+
+/* advance the diffusive terms of (u0, b?f0) over tau (Advance, sts.hpp:118-156); the stage
+ * states rotate through three scratch states and u1 / b?f1 as in the reference */
+static int sts_advance(port_mesh *m, double tau, double dt_par) {
+  const int s = sts_count(tau, dt_par);
+  const double w1 = 4.0 / ((double)s * s + s - 2.0);
+  const long cb = NVAR * m->ncell * sizeof(double), fb = m->nface * sizeof(double);
+  double *y[4], *yb[4][3];
+  int a = 0, b = 1, cn = 2, j, q;
+  if (!m->sy[0])
+    for (q = 0; q < 3; ++q) {
+      m->sy[q] = calloc(NVAR * m->ncell, 8);
+      for (int r = 0; r < 3; ++r) m->syb[q][r] = calloc(m->nface, 8);
+      if (q < 2) {
+        m->sm[q] = calloc(NVAR * m->ncell, 8);
+        for (int r = 0; r < 3; ++r) m->smb[q][r] = calloc(m->nface, 8);
+      }
+    }
+  for (q = 0; q < 3; ++q) {
+    y[q] = m->sy[q];
+    for (int r = 0; r < 3; ++r) yb[q][r] = m->syb[q][r];
+  }
+  y[3] = m->u[1];
+  for (q = 0; q < 3; ++q) yb[3][q] = m->b[1][q];
+  /* Y0 = (u0, b?f0); M0 = M(Y0) */
+  memcpy(y[0], m->u[0], cb);
+  for (q = 0; q < 3; ++q) memcpy(yb[0][q], m->b[0][q], fb);
+  c2p_on(m, y[0], yb[0][0], yb[0][1], yb[0][2], 0);
+  sts_op(m, yb[0], m->sm[0], m->smb[0]);
+  {
+    const double mt1 = (sts_bj(1) * w1) * tau;
+    sts_comb(m, y[1], yb[1], 1.0, y[0], yb[0], 0.0, y[0], yb[0], 0.0, y[0], yb[0], mt1, m->sm[0], m->smb[0], 0.0,
+             m->sm[0], m->smb[0]);
+  }
+  bc_on(m, y[1], yb[1][0], yb[1][1], yb[1][2]);
+  /* a = Y_{j-2}, b = Y_{j-1}, cn = Y_j (indices into y); the reference's spare is u1 */
+  for (j = 2; j <= s; ++j) {
+    const double b_j = sts_bj(j), b_jm1 = sts_bj(j - 1), b_jm2 = sts_bj(j - 2);
+    const double mu = (2.0 * j - 1.0) / j * b_j / b_jm1;
+    const double nu = -(j - 1.0) / j * b_j / b_jm2;
+    const double mut = mu * w1;
+    const double gt = -(1.0 - b_jm1) * mut;
+    int freed;
+    c2p_on(m, y[b], yb[b][0], yb[b][1], yb[b][2], 0);
+    sts_op(m, yb[b], m->sm[1], m->smb[1]);
+    sts_comb(m, y[cn], yb[cn], mu, y[b], yb[b], nu, y[a], yb[a], 1.0 - mu - nu, y[0], yb[0], mut * tau, m->sm[1],
+             m->smb[1], gt * tau, m->sm[0], m->smb[0]);
+    bc_on(m, y[cn], yb[cn][0], yb[cn][1], yb[cn][2]);
+    freed = (j == 2) ? 3 : a;
+    a = b;
+    b = cn;
+    cn = freed;
+  }
+  memcpy(m->u[0], y[b], cb);
+  for (q = 0; q < 3; ++q) memcpy(m->b[0][q], yb[b][q], fb);
+  return s;
+}
+#undef FB
+
 /* FlagBadCells (src/fofc.hpp:17-43) */
 int port_fofc_flag(port_mesh *m, int buf) {
   const double *u = m->u[buf], *b1 = m->b[buf][0], *b2 = m->b[buf][1], *b3 = m->b[buf][2];
@@ -534,9 +883,12 @@ int port_fofc_flag(port_mesh *m, int buf) {
   return nbad;
 }
 
-/* RepairFluxes<DIR> without diffusion (src/fofc.hpp:46-95) */
+/* RepairFluxes<DIR> (src/fofc.hpp:46-95); the diffusive fluxes are re-added on the repaired
+ * faces of active cells when diffusion runs inside the stage (no RKL2) */
 void port_fofc_repair(port_mesh *m, int dir, int cur) {
   const int di = (dir == 0), dj = (dir == 1), dk = (dir == 2);
+  const int dcr = !m->c.sts && diff_any(m);
+  const curl_ctx J = curl_of(m, m->b[cur][0], m->b[cur][1], m->b[cur][2]);
   const int IVU = 1 + dir, IVV = 1 + (dir + 1) % 3, IVW = 1 + (dir + 2) % 3, IBT1 = (dir + 1) % 3, IBT2 = (dir + 2) % 3;
   const double *bn = m->b[cur][dir];
   int lo[3], hi[3], k;
@@ -571,6 +923,12 @@ void port_fofc_repair(port_mesh *m, int dir, int cur) {
         }
         m->et2[dir][lf] = -f[5];
         m->et1[dir][lf] = f[6];
+        if (dcr) {
+          const int af = (dir == 0)   ? (i >= m->is && i <= m->ie + 1 && j >= m->js && j <= m->je && k >= m->ks && k <= m->ke)
+                         : (dir == 1) ? (j >= m->js && j <= m->je + 1 && i >= m->is && i <= m->ie && k >= m->ks && k <= m->ke)
+                                      : (k >= m->ks && k <= m->ke + 1 && i >= m->is && i <= m->ie && j >= m->js && j <= m->je);
+          if (af) diff_face(m, dir, &J, k, j, i);
+        }
       }
 }
 
@@ -657,31 +1015,40 @@ long port_limit_fluxes(port_mesh *m, int dir, double bdt) {
   return cnt;
 }
 
-/* Stage (src/main.cpp:46-93) without diffusion and source terms */
+/* Stage (src/main.cpp:46-93): hyperbolic fluxes, in-stage diffusive fluxes (no RKL2), the
+ * positivity limiter, corner EMFs plus eta J, the update and gravity, then the FOFC pass */
 void port_stage(port_mesh *m, int cur, int out, double g0, double g1, double bdt) {
   const int nd = 1 + m->two_d + m->three_d;
+  double *b1c = m->b[cur][0], *b2c = m->b[cur][1], *b3c = m->b[cur][2];
   int d;
   for (d = 0; d < nd; ++d) port_fluxes(m, d, cur);
+  if (!m->c.sts)
+    for (d = 0; d < nd; ++d) diff_fluxes(m, d, b1c, b2c, b3c);
   if (m->c.flux_limiter)
     for (d = 0; d < nd; ++d) port_limit_fluxes(m, d, bdt);
   port_corner_emf(m);
+  if (!m->c.sts) res_emf(m, b1c, b2c, b3c);
   port_update(m, out, g0, g1, bdt);
+  gravity(m, m->u[out], bdt);
   if (m->c.fofc) {
     const int nbad = port_fofc_flag(m, out);
     if (nbad > 0) {
       m->fofc_count += nbad;
       for (d = 0; d < nd; ++d) port_fofc_repair(m, d, cur);
       port_corner_emf(m);
+      if (!m->c.sts) res_emf(m, b1c, b2c, b3c);
       port_update(m, out, g0, g1, bdt);
+      gravity(m, m->u[out], bdt);
     }
   }
   port_boundaries(m, out);
 }
 
-/* src/main.cpp:200-201 */
+/* src/main.cpp:200-202 */
 void port_prime(port_mesh *m, double t) {
   port_boundaries(m, 0);
   m->min_dt = port_cons_to_prim(m, 0, 1);
+  if (!m->c.sts) m->min_dt = fmin(m->min_dt, parabolic_dt(m));
   m->t = t;
   m->cycle = 0;
 }
@@ -702,7 +1069,8 @@ static void table(int ns, int s, double *g0, double *g1, double *beta, int *cur,
   *out = (s == ns) ? 0 : 1;
 }
 
-/* src/main.cpp:246-297 (no outputs, no operator-split terms) */
+/* src/main.cpp:246-297 without the outputs: the stages, then RKL2 and cooling split after
+ * the last stage on (u0, b?f0) */
 int port_cycles(port_mesh *m, int n) {
   int c, done = 0;
   for (c = 0; c < n; ++c) {
@@ -717,9 +1085,23 @@ int port_cycles(port_mesh *m, int n) {
       table(m->c.nstage, s, &g0, &g1, &beta, &cur, &out);
       port_stage(m, cur, out, g0, g1, beta * dt);
       {
-        const double mdt = port_cons_to_prim(m, out, s == m->c.nstage);
-        if (s == m->c.nstage) m->min_dt = mdt;
+        const int last = (s == m->c.nstage), split = last && (m->c.sts || m->c.cooling);
+        const double mdt = port_cons_to_prim(m, out, last && !split);
+        if (last && !split) m->min_dt = fmin(mdt, parabolic_dt(m));
       }
+    }
+    if (m->c.sts) {
+      m->sts_stages += sts_advance(m, dt, parabolic_dt(m));
+      port_boundaries(m, 0);
+    }
+    if (m->c.cooling) {
+      port_cons_to_prim(m, 0, 0);
+      cooling(m, m->u[0], dt);
+      port_boundaries(m, 0);
+    }
+    if (m->c.sts || m->c.cooling) {
+      m->min_dt = port_cons_to_prim(m, 0, 1);
+      if (!m->c.sts) m->min_dt = fmin(m->min_dt, parabolic_dt(m));
     }
     m->t += dt;
     ++m->cycle;
@@ -727,6 +1109,8 @@ int port_cycles(port_mesh *m, int n) {
   }
   return done;
 }
+
+long port_sts_stages(port_mesh *m) { return m->sts_stages; }
 
 void port_clock(port_mesh *m, double *t, int *cycle, double *min_dt, long *fofc_count) {
   if (t) *t = m->t;

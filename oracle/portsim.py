@@ -20,7 +20,12 @@ class port_cfg(C.Structure):
                 ("gamma", C.c_double), ("dfloor", C.c_double), ("pfloor", C.c_double), ("cfl", C.c_double),
                 ("de_eta", C.c_double), ("lhlld_phi", C.c_double), ("tlim", C.c_double),
                 ("dual_energy", C.c_int), ("low_mach", C.c_int), ("flatten", C.c_int), ("characteristic", C.c_int),
-                ("fofc", C.c_int), ("flux_limiter", C.c_int)]
+                ("fofc", C.c_int), ("flux_limiter", C.c_int),
+                ("nu", C.c_double), ("kappa", C.c_double), ("eta", C.c_double), ("sts", C.c_int),
+                ("grav_uniform", C.c_int), ("grav_point", C.c_int), ("g1", C.c_double), ("g2", C.c_double),
+                ("g3", C.c_double), ("gm", C.c_double), ("gx0", C.c_double), ("gy0", C.c_double),
+                ("gz0", C.c_double), ("rsoft", C.c_double), ("cooling", C.c_int), ("lambda0", C.c_double),
+                ("cool_alpha", C.c_double), ("tfloor", C.c_double)]
 
 
 _P, _D = C.c_void_p, C.POINTER(C.c_double)
@@ -35,6 +40,7 @@ _SIGS = [("port_create", _P, [C.POINTER(port_cfg)]), ("port_destroy", None, [_P]
          ("port_prime", None, [_P, C.c_double]), ("port_cycles", C.c_int, [_P, C.c_int]),
          ("port_clock", None, [_P, _D, C.POINTER(C.c_int), _D, C.POINTER(C.c_long)]),
          ("port_history", None, [_P, _D]), ("port_set_threads", None, [C.c_int]),
+         ("port_sts_stages", C.c_long, [_P]),
          ("port_recon", None, [C.c_int, _D, _D, _D]),
          ("port_riemann", None, [C.c_int, _D, _D, C.c_double, C.c_double, C.c_double, C.c_double, _D])]
 _lib = None
@@ -63,6 +69,14 @@ def cfg_from_chq(c: dict) -> port_cfg:
               "dfloor", "pfloor", "cfl", "de_eta", "lhlld_phi", "tlim", "dual_energy", "low_mach", "flatten",
               "characteristic", "fofc", "flux_limiter"):
         setattr(p, k, c[k])
+    for k in ("nu", "kappa", "eta", "sts", "g1", "g2", "g3", "gm", "gx0", "gy0", "gz0", "rsoft", "cooling",
+              "lambda0", "cool_alpha", "tfloor"):
+        if k in c:
+            setattr(p, k, c[k])
+    p.grav_uniform = c.get("gravity_uniform", 0)
+    p.grav_point = c.get("gravity_point", 0)
+    if "cool_alpha" not in c:
+        p.cool_alpha = 1.0
     p.ng = c["nghost"]
     p.nstage = c["integrator"]
     p.bc[0], p.bc[1], p.bc[2] = c["bc1"], c["bc2"], c["bc3"]
@@ -114,6 +128,9 @@ class PortSim:
         cyc, nf = C.c_int(), C.c_long()
         lib().port_clock(self._h, C.byref(t), C.byref(cyc), C.byref(mdt), C.byref(nf))
         return {"t": t.value, "cycle": cyc.value, "min_dt": mdt.value, "fofc": nf.value}
+
+    def sts_stages(self):
+        return lib().port_sts_stages(self._h)
 
     def history(self):
         out = np.zeros(10)

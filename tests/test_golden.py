@@ -3,8 +3,8 @@ reference's own kernels, compiled in place, on each case's input file): the init
 the state after N cycles, the clock, the FOFC count and the history sums.
 
 CPU: the fixtures agree with the reference when it is built here (re-run, bit for bit), and
-the project's C restatement of the path (oracle/port) reproduces the ideal-MHD fixtures bit
-for bit. GPU: the device path reproduces every fixture (relative L1 <= 1e-12 per field, the
+the project's C restatement of the path (oracle/port) reproduces every fixture bit for bit,
+including those with diffusion, RKL2 and source terms. GPU: the device path reproduces every fixture (relative L1 <= 1e-12 per field, the
 same clock and FOFC count) with no reference present at run time."""
 import glob
 import os
@@ -19,8 +19,6 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 FILES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
 NAMES = [os.path.basename(f)[:-4] for f in FILES]
 FIELDS = ("u0", "b1f0", "b2f0", "b3f0")
-# cases the C restatement covers (it has no diffusion and no source terms)
-IDEAL = [n for n in NAMES if "diffusion" not in n and "gravity" not in n and "cooling" not in n]
 
 
 def _load(name):
@@ -62,7 +60,7 @@ def test_fixture_is_the_reference_output(name):
     ref.close()
 
 
-@pytest.mark.parametrize("name", IDEAL)
+@pytest.mark.parametrize("name", NAMES)
 def test_port_reproduces_fixture_bitwise(name):
     from oracle import portsim
     if not portsim.available():
