@@ -213,7 +213,43 @@ def config_rates(steps: int = 5, warmup: int = 3) -> dict:
                 r["rkl2_stages_per_cycle"] = m.sts_stages() / (warmup + steps)
             out[name + ("_mixed" if prec else "_fp64")] = r
             m.close()
+    out["ot2d_256_hst_every_cycle_fp64"] = history_rates()
     return out
+
+
+def history_rates(n: int = 400) -> dict:
+    """OT 2D 256^2 with a .hst row after every cycle, both ways the C ABI offers: rows recorded
+    on the device (chq_history_record: the sums ride on the end-of-cycle con2prim, the cycles
+    stay queued as replayed graphs, one drain at the end) against the per-cycle host output test
+    (chq_cycles(1), chq_clock, chq_history: two synchronisations and a separate history pass
+    per cycle). Host wall clock from an idle device to the last row on the host."""
+    from chasqui_b200 import Mesh, make_config
+    kw = dict(nx1=256, nx2=256, nx3=1, cfl=0.4, tlim=1e9)
+    cells = 256 * 256
+    m = Mesh(make_config(precision=0, **kw))
+    m.init_problem("orszag_tang", [-1.0])
+    m.prime(0.0)
+    m.cycles(5)
+    m.clock()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        m.cycles(1)
+        m.clock()
+        m.history()
+    host_s = time.perf_counter() - t0
+    m.record_history(1e-12, 0.0, 0.0, capacity=n)
+    m.cycles(5)
+    m.drain_history(n)
+    t0 = time.perf_counter()
+    m.cycles(n)
+    rows, lost, _ = m.drain_history(n)
+    dev_s = time.perf_counter() - t0
+    m.record_history(0.0, 0.0, 0.0, capacity=0)
+    m.close()
+    return {"device_rows": {"value": cells * n / dev_s, "rows": int(len(rows)), "lost": int(lost)},
+            "host_rows": {"value": cells * n / host_s, "rows": n},
+            "speedup": host_s / dev_s, "cycles": n, "unit": "zone-updates/s",
+            "timing": "host wall clock, device idle at both ends"}
 
 
 def tune_summary(tune):

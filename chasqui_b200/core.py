@@ -82,6 +82,8 @@ SIGNATURES = [
     ("chq_set_seglen", C.c_int, [_P, C.c_int]),
     ("chq_get_seglen", C.c_int, [_P]),
     ("chq_history", C.c_int, [_P, _D, _P]),
+    ("chq_history_record", C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int]),
+    ("chq_history_drain", C.c_int, [_P, _D, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
     ("chq_run_host", C.c_int, [_P, _D, _D, _D, _D, C.c_int, C.c_double, _P]),
     ("chq_run_host_async", C.c_int, [_P, _D, _D, _D, _D, C.c_int, C.c_double]),
     ("chq_run_host_wait", C.c_int, [_P, C.POINTER(C.c_int)]),
@@ -341,6 +343,19 @@ class Mesh:
         out = np.zeros(10)
         _check(load_library().chq_history(self._h, _dptr(out), None))
         return out
+
+    def record_history(self, dt_hst: float, next_t: float, eps: float = 0.0, capacity: int = 256) -> None:
+        """Record .hst rows on the device at the end of each cycle reaching the next output time
+        (capacity 0: off)."""
+        _check(load_library().chq_history_record(self._h, float(dt_hst), float(next_t), float(eps), int(capacity)))
+
+    def drain_history(self, max_rows: int = 256):
+        """(rows (n x 12: t, dt, the ten history values), rows lost, next output time)."""
+        rows = np.zeros((max(int(max_rows), 1), 12))
+        n, lost, nxt = C.c_int(), C.c_int(), np.zeros(1)
+        _check(load_library().chq_history_drain(self._h, _dptr(rows), int(max_rows), C.byref(n), C.byref(lost),
+                                                _dptr(nxt)))
+        return rows[:n.value].copy(), lost.value, float(nxt[0])
 
     def run_host(self, u: np.ndarray, b1: np.ndarray, b2: np.ndarray, b3: np.ndarray, ncycles: int,
                  t0: float = 0.0) -> int:

@@ -685,6 +685,19 @@ template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs
 
 // ---------------------------------------------------------------------------------------
 // K5
+// .hst rows recorded on the device (chq_history_record): the con2prim of each cycle's final
+// state also reduces the history sums (src/output.hpp:91-119) when that cycle reaches the next
+// output time, and the row is appended to a ring the host drains.
+struct HstRec {
+  int due;                  // this cycle's final state is an output (set after ctl_begin)
+  int count, cap, lost;     // rows in the ring, its capacity, rows dropped on a full ring
+  double next, dt_hst, eps; // next output time, interval, tolerance (src/main.cpp:212)
+  double vol, ncell, idx1, idx2, idx3;
+  long nblk, nfold;         // K5 blocks (partials), second-level partials
+  double *part, *fold;      // nblk x 10, nfold x 10
+  double *rows;             // cap x 12: t, dt, mass mom1 mom2 mom3 etot ekin emag eint divB_max divB_L1
+};
+
 template <class P> struct C2pArgs {
   Geom g;
   EOSp eos;
@@ -695,10 +708,16 @@ template <class P> struct C2pArgs {
   unsigned long long *mdt_bits;   // atomic min of dt over active cells
   StepCtl *ctl;                   // when set: fold the FOFC count and reset it (block 0)
   const int *done;
+  const HstRec *hst;              // K5 of a cycle's final state with recording on (HST form)
 };
 
-template <class P> CHQ_D void c2p_body(const C2pArgs<P> &A, int bx, int by, int bz) {
+CHQ_D double hsq(double x) { return x * x; }
+
+template <class P, bool HST = false> CHQ_D void c2p_body(const C2pArgs<P> &A, int bx, int by, int bz) {
   if (A.done && *A.done) return;
+  // history terms of this thread's cell (active cells, output cycles, HST form only)
+  double hv[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const bool hdue = HST && A.hst->due;
   const Geom &g = A.g;
   if (A.ctl && bx == 0 && by == 0 && bz == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
     A.ctl->fofc_count += A.ctl->nbad;
@@ -724,10 +743,12 @@ template <class P> CHQ_D void c2p_body(const C2pArgs<P> &A, int bx, int by, int 
     const double eint = etot - ke - 0.5 * bsq;
     double p = e.gm1 * eint;
     double sent = A.u[IENT * vs + l] * id;
+    double en = etot;   // the energy left in u
     if (e.dual_energy && eint < e.de_eta * fabs(etot)) {
       p = sent * pow(d, e.gamma);
       p = fmax(p, e.pfloor);
-      A.u[IEN * vs + l] = ke + 0.5 * bsq + p / e.gm1;
+      en = ke + 0.5 * bsq + p / e.gm1;
+      A.u[IEN * vs + l] = en;
     } else {
       p = fmax(p, e.pfloor);
       sent = p / pow(d, e.gamma);
@@ -757,11 +778,104 @@ template <class P> CHQ_D void c2p_body(const C2pArgs<P> &A, int bx, int by, int 
       if (g.three_d) dt = fmin(dt, g.dx3 / (fabs(vz) + cf(bz)));
       mdt = dt;
     }
+    if (hdue && i >= g.is && i <= g.ie && j >= g.js && j <= g.je && k >= g.ks && k <= g.ke) {
+      // the stored (P) primitives and centred field, as the separate history pass reads them
+      const double wd = (double)P(d), wx = (double)P(vx), wy = (double)P(vy), wz = (double)P(vz);
+      const double cx = (double)P(bx), cy = (double)P(by), cz = (double)P(bz);
+      const HstRec &H = *A.hst;
+      hv[0] = A.u[IDN * vs + l];
+      hv[1] = A.u[IM1 * vs + l];
+      hv[2] = A.u[IM2 * vs + l];
+      hv[3] = A.u[IM3 * vs + l];
+      hv[4] = en;
+      hv[5] = 0.5 * wd * (hsq(wx) + hsq(wy) + hsq(wz));
+      hv[6] = 0.5 * (hsq(cx) + hsq(cy) + hsq(cz));
+      hv[7] = en - 0.5 * wd * (hsq(wx) + hsq(wy) + hsq(wz)) - 0.5 * (hsq(cx) + hsq(cy) + hsq(cz));
+      double db = (A.b1[l + 1] - A.b1[l]) * H.idx1;
+      if (g.two_d) db += (A.b2[l + g.sj] - A.b2[l]) * H.idx2;
+      if (g.three_d) db += (A.b3[l + g.sk] - A.b3[l]) * H.idx3;
+      hv[8] = fabs(db);
+      hv[9] = fabs(db);
+    }
   }
   if (A.compute_dt) block_min_pos(A.mdt_bits, mdt);   // one atomic per block (the whole block is here)
+  if (hdue) {
+    // fixed-order block partial: warp shuffles, then the block's 8 warps in order
+    __shared__ double hs[10][8];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_down_sync(0xffffffffu, hv[q], o);
+        hv[q] = (q == 8) ? fmax(hv[q], x) : hv[q] + x;
+      }
+    }
+    const int lane = threadIdx.x, wid = threadIdx.y;   // blockDim (32, 8)
+    if (lane == 0)
+      for (int q = 0; q < 10; ++q) hs[q][wid] = hv[q];
+    __syncthreads();
+    if (wid == 0 && lane < 10) {
+      double r = hs[lane][0];
+      for (int w = 1; w < 8; ++w) r = (lane == 8) ? fmax(r, hs[lane][w]) : r + hs[lane][w];
+      const long b = ((long)bz * gridDim.y + by) * gridDim.x + bx;
+      A.hst->part[b * 10 + lane] = r;
+    }
+  }
 }
 
-template <class P> __global__ void __launch_bounds__(256) c2p_kernel(const C2pArgs<P> A) { c2p_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+template <class P, bool HST = false>
+__global__ void __launch_bounds__(256) c2p_kernel(const C2pArgs<P> A) { c2p_body<P, HST>(A, blockIdx.x, blockIdx.y, blockIdx.z); }
+
+// Output test of the cycle just begun: its end time t + dt reaches the next output time
+// (the driver's check after t += dt, src/main.cpp:212-223).
+__global__ void hst_due_kernel(const StepCtl *c, HstRec *h) {
+  h->due = (!c->done && c->t + c->dt >= h->next - h->eps) ? 1 : 0;
+}
+
+// Fixed-order folds of the K5 partials: block f of hst_fold_kernel folds its contiguous range
+// (warp q: value q, lanes strided, then a shuffle tree), hst_commit_kernel folds the block
+// results the same way and appends the scaled row (t, dt, sums) after ctl_end has advanced t.
+CHQ_D double hst_fold_range(const double *src, long lo, long hi, int q, int lane) {
+  double r = 0.0;
+  for (long b = lo + lane; b < hi; b += 32) r = (q == 8) ? fmax(r, src[b * 10 + q]) : r + src[b * 10 + q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double x = __shfl_down_sync(0xffffffffu, r, o);
+    r = (q == 8) ? fmax(r, x) : r + x;
+  }
+  return r;
+}
+__global__ void __launch_bounds__(320) hst_fold_kernel(HstRec *h) {
+  if (!h->due) return;
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long per = (h->nblk + h->nfold - 1) / h->nfold;
+  const long lo = (long)blockIdx.x * per, hi = min(h->nblk, lo + per);
+  const double r = hst_fold_range(h->part, lo, hi, q, lane);
+  if (lane == 0) h->fold[(long)blockIdx.x * 10 + q] = r;
+}
+__global__ void __launch_bounds__(320) hst_commit_kernel(const StepCtl *c, HstRec *h) {
+  if (!h->due) return;
+  __shared__ double v[10];
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double r = hst_fold_range(h->fold, 0, h->nfold, q, lane);
+  if (lane == 0) v[q] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (h->count < h->cap) {
+      double *row = h->rows + (long)h->count * 12;
+      row[0] = c->t;
+      row[1] = c->dt;
+      for (int n = 0; n < 8; ++n) row[2 + n] = v[n] * h->vol;
+      row[10] = v[8];
+      row[11] = v[9] / h->ncell;
+      h->count += 1;
+    } else {
+      h->lost += 1;
+    }
+    h->next += h->dt_hst;
+    h->due = 0;
+  }
+}
 
 // ---------------------------------------------------------------------------------------
 // Batched forms: the same bodies, one launch over the blocks of many meshes (chq_batch).

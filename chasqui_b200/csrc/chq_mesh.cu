@@ -194,6 +194,9 @@ struct chq_mesh {
   StepCtl *ctl;            // device
   double *hst_part, *hst_out;
   int hst_blocks;
+  HstRec *hrec = nullptr;  // device .hst recording (chq_history_record): header, partials, rows
+  long hrec_nfold = 0;
+  int hrec_cap = 0;
   // flux launch geometry
   int lo[3][3], hi[3][3], active[3];
   int act_lo[3][3], act_hi[3][3];
@@ -684,6 +687,20 @@ template <class P>
 int do_c2p(chq_mesh *m, int buf, int compute_dt, unsigned long long *bits, StepCtl *fold, const int *done,
            cudaStream_t s) {
   return launch_c2p<P>(m, c2p_args<P>(m, buf, compute_dt, bits, fold, done), s);
+}
+
+// K5 of a cycle's final state (u0, with the dt reduction); with .hst recording on, the form
+// that also reduces the history sums when the cycle is an output
+template <class P>
+int do_c2p_end(chq_mesh *m, const int *done, cudaStream_t s) {
+  if (!m->hrec) return do_c2p<P>(m, 0, 1, &m->ctl->mdt_bits, m->ctl, done, s);
+  C2pArgs<P> a = c2p_args<P>(m, 0, 1, &m->ctl->mdt_bits, m->ctl, done);
+  a.hst = m->hrec;
+  const Launch3 L = c2p_grid(m);
+  m->nlaunch += 1;
+  c2p_kernel<P, true><<<L.grid, L.block, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
 }
 
 // ---- explicit diffusion (src/diffusion.hpp) --------------------------------------------
@@ -1823,6 +1840,7 @@ int chq_mesh_destroy(chq_mesh *m) {
   if (m->snap_landed) cudaEventDestroy(m->snap_landed);
   if (m->snap) cudaFree(m->snap);
   if (m->stage_buf) cudaFree(m->stage_buf);
+  if (m->hrec) cudaFree(m->hrec);
   if (m->cyc_exec) cudaGraphExecDestroy(m->cyc_exec);
   if (m->cyc_graph) cudaGraphDestroy(m->cyc_graph);
   for (auto &p : m->pending) { m->pool.push_back(p.b); m->pool.push_back(p.e); }
@@ -2121,6 +2139,10 @@ int plain_cycles(chq_mesh *m, int n, cudaStream_t s) {
       Prof p(m, PK_CTL, s);
       ctl_begin_kernel<<<1, 1, 0, s>>>(m->ctl, 0);
       m->nlaunch += 1;
+      if (m->hrec) {
+        hst_due_kernel<<<1, 1, 0, s>>>(m->ctl, m->hrec);
+        m->nlaunch += 1;
+      }
     }
     CHQ_CUDA(cudaGetLastError());
     int rc;
@@ -2133,7 +2155,8 @@ int plain_cycles(chq_mesh *m, int n, cudaStream_t s) {
       const bool last = (st == m->nstage);
       {
         Prof p(m, PK_C2P, s);
-        rc = DISPATCH_P(m, do_c2p)(m, out, (last && !split) ? 1 : 0, &m->ctl->mdt_bits, m->ctl, done, s);
+        rc = (last && !split) ? DISPATCH_P(m, do_c2p_end)(m, done, s)
+                              : DISPATCH_P(m, do_c2p)(m, out, 0, &m->ctl->mdt_bits, m->ctl, done, s);
       }
       if (rc) return rc;
       if (last && m->diff && (!split || sts)) {
@@ -2168,7 +2191,7 @@ int plain_cycles(chq_mesh *m, int n, cudaStream_t s) {
     if (split) {
       {
         Prof p(m, PK_C2P, s);
-        if ((rc = DISPATCH_P(m, do_c2p)(m, 0, 1, &m->ctl->mdt_bits, m->ctl, done, s))) return rc;
+        if ((rc = DISPATCH_P(m, do_c2p_end)(m, done, s))) return rc;
       }
       if (m->diff && !sts) {
         Prof p(m, PK_DIFF, s);
@@ -2179,6 +2202,11 @@ int plain_cycles(chq_mesh *m, int n, cudaStream_t s) {
       Prof p(m, PK_CTL, s);
       ctl_end_kernel<<<1, 1, 0, s>>>(m->ctl);
       m->nlaunch += 1;
+      if (m->hrec) {
+        hst_fold_kernel<<<(unsigned)m->hrec_nfold, 320, 0, s>>>(m->hrec);
+        hst_commit_kernel<<<1, 320, 0, s>>>(m->ctl, m->hrec);
+        m->nlaunch += 2;
+      }
     }
     CHQ_CUDA(cudaGetLastError());
   }
@@ -2299,6 +2327,66 @@ int chq_history(chq_mesh *m, double out[10], void *stream) {
   for (int q = 0; q < 8; ++q) out[q] = h[q] * vol;
   out[8] = h[8];
   out[9] = h[9] / ncell;
+  return CHQ_OK;
+}
+
+static_assert(sizeof(HstRec) <= 256, "HstRec header exceeds its slot");
+
+int chq_history_record(chq_mesh *m, double dt_hst, double next, double eps, int capacity) {
+  if (!m || capacity < 0) return fail(CHQ_ERR_ARG, "bad argument");
+  if (capacity > 0 && !(dt_hst > 0)) return fail(CHQ_ERR_ARG, "history recording needs dt_hst > 0");
+  cudaStream_t s = S(m, nullptr);
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  drop_cycle_graph(m);   // the captured cycle has the old end-of-cycle launches
+  if (m->hrec) {
+    CHQ_CUDA(cudaFree(m->hrec));
+    m->hrec = nullptr;
+    m->hrec_cap = 0;
+  }
+  if (capacity == 0) return CHQ_OK;
+  const Geom &g = m->g;
+  const Launch3 L = c2p_grid(m);
+  HstRec h{};
+  h.cap = capacity;
+  h.next = next;
+  h.dt_hst = dt_hst;
+  h.eps = eps;
+  h.vol = g.dx1 * (g.two_d ? g.dx2 : 1.0) * (g.three_d ? g.dx3 : 1.0);
+  h.ncell = (double)g.nx1 * g.nx2 * g.nx3;
+  h.idx1 = 1.0 / g.dx1;
+  h.idx2 = 1.0 / g.dx2;
+  h.idx3 = 1.0 / g.dx3;
+  h.nblk = (long)L.grid.x * L.grid.y * L.grid.z;
+  h.nfold = std::min<long>(h.nblk, kHstBlocks);
+  const size_t head = 256;
+  const size_t bytes = head + sizeof(double) * ((size_t)h.nblk * 10 + (size_t)h.nfold * 10 + (size_t)capacity * 12);
+  char *p = nullptr;
+  CHQ_CUDA(cudaMalloc(&p, bytes));
+  h.part = reinterpret_cast<double *>(p + head);
+  h.fold = h.part + h.nblk * 10;
+  h.rows = h.fold + h.nfold * 10;
+  CHQ_CUDA(cudaMemcpy(p, &h, sizeof(h), cudaMemcpyHostToDevice));
+  m->hrec = reinterpret_cast<HstRec *>(p);
+  m->hrec_nfold = h.nfold;
+  m->hrec_cap = capacity;
+  return CHQ_OK;
+}
+
+int chq_history_drain(chq_mesh *m, double *rows, int max_rows, int *n, int *lost, double *next) {
+  if (!m || max_rows < 0 || (max_rows > 0 && !rows)) return fail(CHQ_ERR_ARG, "bad argument");
+  if (!m->hrec) return fail(CHQ_ERR_ARG, "history recording is off (chq_history_record)");
+  cudaStream_t s = S(m, nullptr);
+  HstRec h;
+  CHQ_CUDA(cudaMemcpyAsync(&h, m->hrec, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  const int k = std::min(h.count, max_rows);
+  if (k > 0) CHQ_CUDA(cudaMemcpyAsync(rows, h.rows, sizeof(double) * 12 * (size_t)k, cudaMemcpyDeviceToHost, s));
+  const int cleared[3] = {0, h.cap, 0};   // count, cap, lost
+  CHQ_CUDA(cudaMemcpyAsync(&m->hrec->count, cleared, sizeof(cleared), cudaMemcpyHostToDevice, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  if (n) *n = k;
+  if (lost) *lost = h.lost + (h.count - k);
+  if (next) *next = h.next;
   return CHQ_OK;
 }
 

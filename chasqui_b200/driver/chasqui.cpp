@@ -225,6 +225,7 @@ int run(int argc, char **argv) {
     for (auto &w : pending) w();
     pending.clear();
   };
+  bool hst_on_device = false;
   auto do_outputs = [&](double dt, bool force, bool final_dump) {
     const double eps = 1e-10 * (tlim > 0 ? tlim : 1.0);
     const bool vtk_now = dt_vtk > 0 && (t >= next_vtk - eps || force);
@@ -264,7 +265,8 @@ int run(int argc, char **argv) {
         next_rst += dt_rst;
       }
     }
-    if (dt_hst > 0 && (t >= next_hst - eps || force)) {
+    // with device recording on, the cycles' rows come from chq_history_drain instead
+    if (dt_hst > 0 && (force || (!hst_on_device && t >= next_hst - eps))) {
       double hv[10];
       check(chq_history(m, hv, nullptr), "history");
       hst << std::setprecision(12) << t << " " << dt;
@@ -279,6 +281,30 @@ int run(int argc, char **argv) {
 
   // ---- time loop on the device ----
   const bool outputs_on = dt_vtk > 0 || dt_hst > 0 || dt_rst > 0;
+  // .hst rows are recorded on the device (the history sums ride on the con2prim of each
+  // output cycle), so history alone does not stop the queue after every cycle; VTK and
+  // restart dumps still do, since their snapshot is queued from the host
+  const bool dumps_on = dt_vtk > 0 || dt_rst > 0;
+  const int kHstRing = 256;
+  if (dt_hst > 0) {
+    const double eps = 1e-10 * (tlim > 0 ? tlim : 1.0);
+    check(chq_history_record(m, dt_hst, next_hst, eps, kHstRing), "history record");
+    hst_on_device = true;
+  }
+  std::vector<double> hrows(12 * (size_t)kHstRing);
+  auto drain_hst = [&]() {
+    if (!hst_on_device) return;
+    int nrow = 0, nlost = 0;
+    check(chq_history_drain(m, hrows.data(), kHstRing, &nrow, &nlost, &next_hst), "history drain");
+    if (nlost > 0) throw std::runtime_error("history ring overflow");
+    for (int r = 0; r < nrow; ++r) {
+      const double *row = &hrows[12 * (size_t)r];
+      hst << std::setprecision(12) << row[0] << " " << row[1];
+      for (int q = 2; q < 12; ++q) hst << " " << row[q];
+      hst << "\n";
+    }
+    if (nrow) hst.flush();
+  };
   const int cycle0 = cycle;
   {
     double tt, dd, mm;
@@ -288,8 +314,8 @@ int run(int argc, char **argv) {
   auto t0 = std::chrono::steady_clock::now();
   while (true) {
     int chunk = 1;
-    if (!outputs_on) {
-      chunk = 256;
+    if (!dumps_on) {
+      chunk = hst_on_device ? kHstRing : 256;
       if (ndiag > 0) chunk = std::min(chunk, ndiag - (cycle % ndiag));
     }
     check(chq_cycles(m, chunk, nullptr), "cycles");
@@ -300,6 +326,7 @@ int run(int argc, char **argv) {
     const int advanced = cycle0 + cdev - cycle;
     t = tdev;
     cycle = cycle0 + cdev;
+    drain_hst();
     if (advanced == 0) break;
     if (ndiag > 0 && cycle % ndiag == 0)
       std::cout << "cycle=" << cycle << " time=" << std::setprecision(8) << t << " dt=" << dt << "\n";
@@ -308,6 +335,10 @@ int run(int argc, char **argv) {
   }
   flush();
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (hst_on_device) {
+    check(chq_history_record(m, 0.0, 0.0, 0.0, 0), "history record");
+    hst_on_device = false;
+  }
   if (outputs_on) do_outputs(0.0, true, true);
   flush();
 

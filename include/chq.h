@@ -158,6 +158,20 @@ CHQ_API long long chq_sts_stages(const chq_mesh *m);
 /* output::History (src/output.hpp:91-119) of u0/b?f0: mass mom1 mom2 mom3 etot ekin emag
  * eint divB_max divB_L1 (volume-weighted like the reference). Synchronises. */
 CHQ_API int chq_history(chq_mesh *m, double out[10], void *stream);
+/* .hst rows recorded on the device, so that history output does not stop the queue of cycles
+ * (the reference computes output::History on the host side after each cycle whose time
+ * reaches the next output time, src/main.cpp:212-223, src/output.hpp:91-119). With recording
+ * on, every cycle of chq_cycles tests on the device whether its end time t satisfies
+ * t >= next - eps; if so, the con2prim of the cycle's final state also reduces the history
+ * sums (fixed-order, deterministic), the row {t, dt, the ten chq_history values} is appended
+ * to a device ring of `capacity` rows, and next advances by dt_hst. capacity 0 turns recording
+ * off. Synchronises the mesh stream; drops the captured cycle graph. */
+CHQ_API int chq_history_record(chq_mesh *m, double dt_hst, double next, double eps, int capacity);
+/* Synchronises the mesh stream, copies up to max_rows recorded rows (12 doubles each, oldest
+ * first) into rows and empties the ring. *n: rows copied; *lost: rows dropped on a full ring
+ * or beyond max_rows since the last drain; *next: the next output time. Any of the three
+ * pointers may be null. CHQ_ERR_ARG if recording is off. */
+CHQ_API int chq_history_drain(chq_mesh *m, double *rows, int max_rows, int *n, int *lost, double *next);
 
 /* ---- host-buffer job entry point (end-to-end path) ---------------------------------------
  * Upload a reference-layout state (u: 6 x cells, b1/b2/b3: faces), prime it, run n cycles

@@ -131,6 +131,9 @@ DRIVER_RUNS = {
                                    "output.rst_dt=100"]),
     "gravity_cooling": (cases.ot(24), ["gravity.uniform=true", "gravity.g2=-0.3", "cooling.enabled=true",
                                        "cooling.lambda0=0.2", "time.nlim=10", "output.hst_dt=0.005"]),
+    # history alone: rows recorded on the device while cycles run in chunks of replayed graphs
+    "blast_hst_chunks": (cases.blast(16), ["time.nlim=40", "problem.pres_in=100", "output.hst_dt=0.009",
+                                           "time.ndiag=16"]),
 }
 
 
