@@ -39,6 +39,11 @@ SETS = {
                         (cases.cpaw3d_extruded(16, 8), ("mhd.reconstruct=ppm",))],
     "wenoz_mixed_precision": [(cases.cpaw2d(32), ()), (cases.cpaw3d_extruded(16, 8), ()),
                               (cases.blast(12), ("mhd.reconstruct=wenoz",))],
+    # odd and prime extents side by side: each member's blocks cut to its own shape
+    "ragged_shapes_fp64": [(cases.blast(16), ("mesh.nx1=17", "mesh.nx2=13", "mesh.nx3=11")),
+                           (cases.ot(32), ("mesh.nx1=33", "mesh.nx2=47")), (cases.ot(32), ("mesh.nx1=97", "mesh.nx2=5")),
+                           (cases.blast(16), ("mesh.nx1=31", "mesh.nx2=9", "mesh.nx3=7", "problem.pres_in=1e4",
+                                              "problem.pres_out=1e-3", "time.cfl=0.5"))],
 }
 
 
