@@ -214,7 +214,59 @@ def config_rates(steps: int = 5, warmup: int = 3) -> dict:
             out[name + ("_mixed" if prec else "_fp64")] = r
             m.close()
     out["ot2d_256_hst_every_cycle_fp64"] = history_rates()
+    out["rkl2_batch_64x_ot2d_64_fp64"] = rkl2_batch_rates()
     return out
+
+
+def rkl2_batch_rates(jobs: int = 64, n: int = 64, cycles: int = 20) -> dict:
+    """64 Orszag-Tang 64^2 jobs with RKL2 resistivity (eta from 0.02 to 0.2, so 2 to 5
+    super-time-stepping stages per cycle, different per job) stepped as one batch (one host
+    read of the stage counts per cycle, then each stage one launch per kernel kind over all
+    jobs) against the same jobs one after another through chq_cycles. Host wall clock,
+    device synchronised at both ends."""
+    from chasqui_b200 import Batch, Mesh, make_config
+
+    def make():
+        ms = []
+        for q in range(jobs):
+            eta = 0.02 + 0.18 * q / (jobs - 1)
+            m = Mesh(make_config(nx1=n, nx2=n, nx3=1, cfl=0.4, tlim=1e9, eta=eta, sts=1))
+            m.init_problem("orszag_tang", [-1.0])
+            m.prime(0.0)
+            ms.append(m)
+        return ms
+
+    cells = n * n * jobs
+    seq = make()
+    for m in seq:
+        m.cycles(2)
+        m.clock()
+    t0 = time.perf_counter()
+    for m in seq:
+        m.cycles(cycles)
+    for m in seq:
+        m.clock()
+    seq_s = time.perf_counter() - t0
+    stages = sum(m.sts_stages() for m in seq)
+    for m in seq:
+        m.close()
+    mem = make()
+    b = Batch(mem)
+    b.cycles(2)
+    b.status()
+    t0 = time.perf_counter()
+    b.cycles(cycles)
+    b.status()
+    bat_s = time.perf_counter() - t0
+    launches = b.kernel_launches()
+    b.close()
+    for m in mem:
+        m.close()
+    return {"batched": {"value": cells * cycles / bat_s, "seconds": bat_s},
+            "sequential": {"value": cells * cycles / seq_s, "seconds": seq_s},
+            "speedup": seq_s / bat_s, "rkl2_stages_per_job_cycle": stages / (jobs * (cycles + 2)),
+            "batch_launches_per_cycle": launches / (cycles + 2), "unit": "zone-updates/s",
+            "timing": "host wall clock, device synchronised at both ends"}
 
 
 def history_rates(n: int = 400) -> dict:

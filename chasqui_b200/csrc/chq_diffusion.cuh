@@ -232,13 +232,15 @@ template <class P> struct StsDivArgs {
   const P *f1, *f2, *f3, *e1, *e2, *e3;
   double *mu, *mb1, *mb2, *mb3;
   double idx1, idx2, idx3;
+  const int *done;   // batched RKL2: this member takes no stage here
 };
 
-template <class P> __global__ void __launch_bounds__(256) sts_div_kernel(const StsDivArgs<P> A) {
+template <class P> CHQ_D void sts_div_body(const StsDivArgs<P> &A, int bx, int by, int bz) {
+  if (A.done && *A.done) return;
   const Geom &g = A.g;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   if (i > g.ie + 1 || j > g.je + 1 || k > g.ke + 1) return;
   const long l = g.idx(k, j, i);
   const long vs = g.vstride;
@@ -271,6 +273,10 @@ template <class P> __global__ void __launch_bounds__(256) sts_div_kernel(const S
   }
 }
 
+template <class P> __global__ void __launch_bounds__(256) sts_div_kernel(const StsDivArgs<P> A) {
+  sts_div_body<P>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // out = ((a x + b y) + c z) + (d p + e q) on active cells (6 components) and on the faces of
 // the update range (3 face fields); coefficients in double as the reference's Real
 struct StsCombArgs {
@@ -280,23 +286,83 @@ struct StsCombArgs {
   const double *x, *y, *z, *p, *q;           // cell arrays (6 components)
   double *bo[3];
   const double *bx[3], *by[3], *bz[3], *bp[3], *bq[3];
+  const int *done;   // batched RKL2: this member takes no stage here
 };
 
-__global__ void __launch_bounds__(256) sts_combine_kernel(const StsCombArgs A) {
+// cf: the five coefficients (a, b, c, d, e)
+CHQ_D void sts_combine_body(const StsCombArgs &A, const double *cf, int bx, int by, int bz) {
+  if (A.done && *A.done) return;
   const Geom &g = A.g;
-  const int i = g.is + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g.js + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = g.ks + blockIdx.z;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
   if (i > g.ie + 1 || j > g.je + 1 || k > g.ke + 1) return;
+  const double a = cf[0], b = cf[1], c = cf[2], d = cf[3], e = cf[4];
   const long l = g.idx(k, j, i);
   if (i <= g.ie && j <= g.je && k <= g.ke) {
     for (int n = 0; n < NVAR; ++n) {
       const long q = n * g.vstride + l;
-      A.out[q] = ((A.a * A.x[q] + A.b * A.y[q]) + A.c * A.z[q]) + (A.d * A.p[q] + A.e * A.q[q]);
+      A.out[q] = ((a * A.x[q] + b * A.y[q]) + c * A.z[q]) + (d * A.p[q] + e * A.q[q]);
     }
   }
-  for (int c = 0; c < 3; ++c)
-    A.bo[c][l] = ((A.a * A.bx[c][l] + A.b * A.by[c][l]) + A.c * A.bz[c][l]) + (A.d * A.bp[c][l] + A.e * A.bq[c][l]);
+  for (int f = 0; f < 3; ++f)
+    A.bo[f][l] = ((a * A.bx[f][l] + b * A.by[f][l]) + c * A.bz[f][l]) + (d * A.bp[f][l] + e * A.bq[f][l]);
+}
+
+__global__ void __launch_bounds__(256) sts_combine_kernel(const StsCombArgs A) {
+  const double cf[5] = {A.a, A.b, A.c, A.d, A.e};
+  sts_combine_body(A, cf, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---- batched RKL2 stages (many meshes, one launch per kernel kind and stage) -----------
+// Every member advances its own stage count s_m; at stage j the members with j > s_m (or a
+// finished clock) skip: skip[m] is rewritten before each stage.
+__global__ void sts_skip_kernel(int *skip, const int *nst, int n, int j) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < n) skip[m] = (j > nst[m]) ? 1 : 0;
+}
+
+template <class P> __global__ void __launch_bounds__(256) sts_div_batched(const StsDivArgs<P> *args, const BatchSlot *slots, int n) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  __shared__ __align__(16) unsigned char sa[sizeof(StsDivArgs<P>)];
+  const StsDivArgs<P> &A = stage_args(args, j, sa);
+  sts_div_body<P>(A, bx, by, bz);
+}
+
+// coef: this stage's five coefficients of every member (member m at coef[5 m])
+__global__ void __launch_bounds__(256) sts_combine_batched(const StsCombArgs *args, const BatchSlot *slots, int n,
+                                                           const double *coef) {
+  int bx, by, bz;
+  const int j = batch_job(slots, n, blockIdx.x);
+  batch_block(slots[j], blockIdx.x, bx, by, bz);
+  __shared__ __align__(16) unsigned char sa[sizeof(StsCombArgs)];
+  const StsCombArgs &A = stage_args(args, j, sa);
+  sts_combine_body(A, coef + 5 * j, bx, by, bz);
+}
+
+// Whole-array copies and zero fills of up to six spans of 8-byte words per member, the
+// member's blocks striding over each span (the RKL2 state copies and flux/EMF zeroing).
+struct SpanArgs {
+  unsigned long long *dst[6];
+  const unsigned long long *src[6];   // null: zero fill
+  long words[6];
+  int nspan;
+  const int *done;
+};
+
+__global__ void __launch_bounds__(256) span_batched(const SpanArgs *args, const BatchSlot *slots, int n) {
+  const int j = batch_job(slots, n, blockIdx.x);
+  __shared__ __align__(16) unsigned char sa[sizeof(SpanArgs)];
+  const SpanArgs &A = stage_args(args, j, sa);
+  if (A.done && *A.done) return;
+  const long b = blockIdx.x - slots[j].off, nb = slots[j].gx;
+  for (int q = 0; q < A.nspan; ++q) {
+    unsigned long long *d = A.dst[q];
+    const unsigned long long *src = A.src[q];
+    for (long w = b * blockDim.x + threadIdx.x; w < A.words[q]; w += nb * blockDim.x) d[w] = src ? src[w] : 0ull;
+  }
 }
 
 }  // namespace chq

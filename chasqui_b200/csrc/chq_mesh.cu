@@ -1229,8 +1229,16 @@ struct chq_batch {
   // stage adds the diffusive fluxes after K1 and eta J after the corner EMFs; gravity runs in
   // the update epilogue; cooling is split after the step
   int diff = 0, grav = 0, cool = 0;
-  int sts = 0;   // RKL2 members: their super-time-stepping stages run per member after the batched stages
+  int sts = 0;   // RKL2 members: super-time-stepping stages batched after the hyperbolic stages
   Kind k_diff, k_res, k_rho, k_cool, k_corner_rerun;
+  // batched RKL2 stages: argument tables per state buffer (Y0, Y1, Y2, u1) and per stage form,
+  // built once; stage counts, coefficients and the final copies are uploaded every cycle
+  Kind k_span;
+  void *a_sts_c2p[4] = {}, *a_sts_diff[4] = {}, *a_sts_res[4] = {}, *a_sts_div[2] = {}, *a_sts_comb[5] = {},
+       *a_sts_bc[4][3] = {}, *a_sts_zero = nullptr, *a_sts_copy0 = nullptr;
+  int *sts_skip = nullptr;   // per member: skip the current RKL2 stage
+  char *sts_dyn = nullptr;   // per cycle: stage counts | coefficients | final copies
+  size_t sts_dyn_bytes = 0;
   void *a_diff[4] = {}, *a_res[4] = {}, *a_res_need[4] = {};
   void *a_rho = nullptr, *a_cool = nullptr, *a_c2p_split[2] = {}, *a_bc0[3] = {};
   void *a_flux[4] = {}, *a_update[4] = {}, *a_update_need[4] = {}, *a_repair[4] = {}, *a_limit[4] = {},
@@ -1405,6 +1413,113 @@ int batch_build(chq_batch *B) {
     for (int d = 0; d < 3; ++d) o_bc[st - 1][d] = push_vec(h, bc[d]);
     o_c2p[st - 1] = push_vec(h, ca);
   }
+  // batched RKL2 stages (src/sts.hpp:111-157 per member): the state buffers of stage j rotate
+  // as in the reference, the same way for every member, so their tables are fixed
+  size_t o_span_s = 0, o_sts_c2p[4] = {}, o_sts_diff[4] = {}, o_sts_res[4] = {}, o_sts_div[2] = {}, o_sts_comb[5] = {},
+         o_sts_bc[4][3] = {}, o_sts_zero = 0, o_sts_copy0 = 0;
+  if (B->sts) {
+    cudaError_t e0 = cudaMalloc(&B->sts_skip, sizeof(int) * (size_t)n);
+    if (e0 == cudaSuccess) e0 = cudaMemset(B->sts_skip, 0, sizeof(int) * (size_t)n);
+    if (e0 != cudaSuccess) return cuda_fail(e0, "batch RKL2 flags");
+    o_span_s = slots_of(h, J, [](chq_mesh *m) {
+      const long words = (long)(3 * NVAR + 3) * (long)m->g.vstride * (long)m->psize / 8;
+      return Launch3{dim3((unsigned)std::max(1L, std::min(1184L, (words + 4095) / 4096)), 1, 1), dim3(256)};
+    }, B->k_span.nblocks);
+    std::vector<C2pArgs<P>> c2(n);
+    std::vector<DiffArgs<P>> df(n);
+    std::vector<ResEmfArgs<P>> rs(n);
+    std::vector<StsDivArgs<P>> dv(n);
+    std::vector<StsCombArgs> cb(n);
+    std::vector<BcArgs> bb(n);
+    auto U = [](chq_mesh *m, int b) { return b < 3 ? m->sy[b] : m->u[1]; };
+    auto BF = [](chq_mesh *m, int b, int d) { return b < 3 ? m->sb[b][d] : m->bf[1][d]; };
+    for (int b = 0; b < 4; ++b) {
+      for (int j = 0; j < n; ++j) {
+        chq_mesh *m = J[j];
+        const int *skip = B->sts_skip + j;
+        long nd = 0;
+        c2[j] = c2p_args_ptr<P>(m, U(m, b), BF(m, b, 0), BF(m, b, 1), BF(m, b, 2), 0, nullptr, nullptr, skip);
+        df[j] = diff_args<P>(m, BF(m, b, 0), BF(m, b, 1), BF(m, b, 2), skip, nd);
+        rs[j] = res_emf_args<P>(m, BF(m, b, 0), BF(m, b, 1), BF(m, b, 2), skip, nullptr);
+      }
+      o_sts_c2p[b] = push_vec(h, c2);
+      o_sts_diff[b] = push_vec(h, df);
+      o_sts_res[b] = push_vec(h, rs);
+      for (int d = 0; d < 3; ++d) {
+        for (int j = 0; j < n; ++j) {
+          bb[j] = bc_args(J[j], 0, B->sts_skip + j, d);
+          bb[j].u = U(J[j], b);
+          bb[j].b1 = BF(J[j], b, 0); bb[j].b2 = BF(J[j], b, 1); bb[j].b3 = BF(J[j], b, 2);
+        }
+        o_sts_bc[b][d] = push_vec(h, bb);
+      }
+    }
+    for (int v = 0; v < 2; ++v) {   // M0 (first stage) or Mj
+      for (int j = 0; j < n; ++j) {
+        chq_mesh *m = J[j];
+        const Geom &g = m->g;
+        StsDivArgs<P> a{};
+        a.g = g;
+        a.f1 = as<P>(m->flx[0]); a.f2 = as<P>(m->flx[1]); a.f3 = as<P>(m->flx[2]);
+        a.e1 = as<P>(m->e[0]); a.e2 = as<P>(m->e[1]); a.e3 = as<P>(m->e[2]);
+        a.mu = v ? m->smj : m->sm0;
+        a.mb1 = v ? m->smbj[0] : m->smb0[0]; a.mb2 = v ? m->smbj[1] : m->smb0[1]; a.mb3 = v ? m->smbj[2] : m->smb0[2];
+        a.idx1 = 1.0 / g.dx1; a.idx2 = 1.0 / g.dx2; a.idx3 = 1.0 / g.dx3;
+        a.done = B->sts_skip + j;
+        dv[j] = a;
+      }
+      o_sts_div[v] = push_vec(h, dv);
+    }
+    // (out, x, y) buffers of the five stage forms: stage 1, stage 2, then j = 3, 4, 5 mod 3
+    const int form[5][3] = {{1, 0, 0}, {2, 1, 0}, {3, 2, 1}, {1, 3, 2}, {2, 1, 3}};
+    for (int v = 0; v < 5; ++v) {
+      for (int j = 0; j < n; ++j) {
+        chq_mesh *m = J[j];
+        StsCombArgs a{};
+        a.g = m->g;
+        a.out = U(m, form[v][0]); a.x = U(m, form[v][1]); a.y = U(m, form[v][2]); a.z = U(m, 0);
+        a.p = v ? m->smj : m->sm0;
+        a.q = m->sm0;
+        for (int d = 0; d < 3; ++d) {
+          a.bo[d] = BF(m, form[v][0], d); a.bx[d] = BF(m, form[v][1], d); a.by[d] = BF(m, form[v][2], d);
+          a.bz[d] = BF(m, 0, d);
+          a.bp[d] = v ? m->smbj[d] : m->smb0[d];
+          a.bq[d] = m->smb0[d];
+        }
+        a.done = B->sts_skip + j;
+        cb[j] = a;
+      }
+      o_sts_comb[v] = push_vec(h, cb);
+    }
+    std::vector<SpanArgs> zero(n), copy0(n);
+    for (int j = 0; j < n; ++j) {   // flux and EMF zero fill; Y0 = (u0, b?f0)
+      chq_mesh *m = J[j];
+      const long vs = (long)m->g.vstride;
+      SpanArgs z{}, c{};
+      for (int d = 0; d < 3; ++d) {
+        z.dst[d] = (unsigned long long *)m->flx[d];
+        z.words[d] = NVAR * vs * (long)m->psize / 8;
+        z.dst[3 + d] = (unsigned long long *)m->e[d];
+        z.words[3 + d] = vs * (long)m->psize / 8;
+      }
+      z.nspan = 6;
+      z.done = B->sts_skip + j;
+      zero[j] = z;
+      c.dst[0] = (unsigned long long *)m->sy[0];
+      c.src[0] = (const unsigned long long *)m->u[0];
+      c.words[0] = NVAR * vs;
+      for (int d = 0; d < 3; ++d) {
+        c.dst[1 + d] = (unsigned long long *)m->sb[0][d];
+        c.src[1 + d] = (const unsigned long long *)m->bf[0][d];
+        c.words[1 + d] = vs;
+      }
+      c.nspan = 4;
+      c.done = &m->ctl->done;
+      copy0[j] = c;
+    }
+    o_sts_zero = push_vec(h, zero);
+    o_sts_copy0 = push_vec(h, copy0);
+  }
   const size_t o_status = h.push(std::vector<double>(3 * n + 1).data(), (3 * n + 1) * sizeof(double));
   cudaError_t e = cudaMalloc(&B->dev, h.b.size());
   if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("batch tables: ") + cudaGetErrorString(e));
@@ -1434,6 +1549,19 @@ int batch_build(chq_batch *B) {
   B->a_c2p_split[0] = d + o_split0;
   B->a_c2p_split[1] = d + o_split1;
   for (int q = 0; q < 3; ++q) B->a_bc0[q] = d + o_bc0[q];
+  if (B->sts) {
+    B->k_span.slots = (BatchSlot *)(d + o_span_s);
+    for (int b = 0; b < 4; ++b) {
+      B->a_sts_c2p[b] = d + o_sts_c2p[b];
+      B->a_sts_diff[b] = d + o_sts_diff[b];
+      B->a_sts_res[b] = d + o_sts_res[b];
+      for (int q = 0; q < 3; ++q) B->a_sts_bc[b][q] = d + o_sts_bc[b][q];
+    }
+    for (int v = 0; v < 2; ++v) B->a_sts_div[v] = d + o_sts_div[v];
+    for (int v = 0; v < 5; ++v) B->a_sts_comb[v] = d + o_sts_comb[v];
+    B->a_sts_zero = d + o_sts_zero;
+    B->a_sts_copy0 = d + o_sts_copy0;
+  }
   for (int st = 0; st < B->nstage; ++st) {
     B->a_diff[st] = d + o_diff[st];
     B->a_res[st] = d + o_res[st];
@@ -1465,32 +1593,127 @@ cudaError_t batch_flux(const chq_batch *B, const FluxArgs<P> *args, cudaStream_t
   }
 }
 
-// The RKL2 part of a batched cycle (src/main.cpp:274-281): the stage count of each member is a
-// host decision on its dt and density minimum, so the batch stream is synchronised once, and
-// every member that is not done advances its diffusive terms with its own launches on the
-// batch stream, exactly as chq_cycles does for a single mesh.
+// The RKL2 part of a batched cycle (src/main.cpp:274-281, src/sts.hpp:111-157). Each member's
+// stage count is a host decision on its dt and density minimum, so the batch stream is
+// synchronised once; then stage j of every member runs in one launch per kernel kind (members
+// with fewer stages skip), the coefficients read from a per-cycle table, and each member's
+// result is copied back from the buffer its last stage wrote.
 template <class P>
-int batch_sts(chq_batch *B, cudaStream_t s) {
+int batch_sts(chq_batch *B, cudaStream_t s, long long &L) {
   const int n = (int)B->jobs.size();
   std::vector<StepCtl> h(n);
   for (int j = 0; j < n; ++j)
     CHQ_CUDA(cudaMemcpyAsync(&h[j], B->jobs[j]->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s));
   CHQ_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> nst(n, 0);
+  int smax = 0;
   for (int j = 0; j < n; ++j) {
     if (h[j].done) continue;
-    chq_mesh *m = B->jobs[j];
     double rho_min;
     std::memcpy(&rho_min, &h[j].rho_bits, sizeof(rho_min));
-    const double dt_par = host_parabolic_dt(m, rho_min);
-    int nst = 0;
-    const long long l0 = m->nlaunch;
-    int rc = sts_advance<P>(m, h[j].dt, dt_par, s, nst);
-    if (!rc) rc = do_bc(m, 0, nullptr, s);
-    if (rc) return rc;
-    m->sts_stages += nst;
-    B->nlaunch += m->nlaunch - l0;
-    m->nlaunch = l0;
+    nst[j] = sts_stage_count(h[j].dt, host_parabolic_dt(B->jobs[j], rho_min));
+    smax = std::max(smax, nst[j]);
   }
+  if (smax == 0) return CHQ_OK;
+  // buffer written by stage j (0: Y0): Y1, Y2, then u1, Y1, Y2, ... (the reference's rotation)
+  auto wrote = [](int j) { return j == 0 ? 0 : j == 1 ? 1 : j == 2 ? 2 : (j % 3 == 0) ? 3 : (j % 3 == 1) ? 1 : 2; };
+  // per-cycle table: stage counts | coefficients (stage j, member m: 5 doubles) | final copies
+  const size_t o_coef = align_up(sizeof(int) * (size_t)n, 256);
+  const size_t o_fin = align_up(o_coef + sizeof(double) * 5 * (size_t)n * smax, 256);
+  const size_t bytes = o_fin + sizeof(SpanArgs) * (size_t)n;
+  std::vector<char> tab(bytes, 0);
+  std::memcpy(tab.data(), nst.data(), sizeof(int) * (size_t)n);
+  double *coef = reinterpret_cast<double *>(tab.data() + o_coef);
+  SpanArgs *fin = reinterpret_cast<SpanArgs *>(tab.data() + o_fin);
+  for (int j = 0; j < n; ++j) {
+    chq_mesh *m = B->jobs[j];
+    const long vs = (long)m->g.vstride;
+    const int ns = nst[j];
+    if (ns) {
+      const double tau = h[j].dt;
+      const double w1 = 4.0 / (double(ns) * ns + ns - 2.0);
+      double *c = coef + 5 * (size_t)j;
+      c[0] = 1.0; c[1] = 0.0; c[2] = 0.0; c[3] = double(sts_b(1) * w1) * tau; c[4] = 0.0;
+      for (int st = 2; st <= ns; ++st) {
+        const double b_j = sts_b(st), b_jm1 = sts_b(st - 1), b_jm2 = sts_b(st - 2);
+        const double mu = (2.0 * st - 1.0) / st * b_j / b_jm1;
+        const double nu = -(st - 1.0) / st * b_j / b_jm2;
+        const double mut = mu * w1;
+        const double gt = -(1.0 - b_jm1) * mut;
+        c = coef + 5 * ((size_t)(st - 1) * n + j);
+        c[0] = mu; c[1] = nu; c[2] = 1.0 - mu - nu; c[3] = mut * tau; c[4] = gt * tau;
+      }
+    }
+    const int b = wrote(ns);
+    SpanArgs &f = fin[j];
+    f.dst[0] = (unsigned long long *)m->u[0];
+    f.src[0] = (const unsigned long long *)(b < 3 ? m->sy[b] : m->u[1]);
+    f.words[0] = NVAR * vs;
+    for (int d = 0; d < 3; ++d) {
+      f.dst[1 + d] = (unsigned long long *)m->bf[0][d];
+      f.src[1 + d] = (const unsigned long long *)(b < 3 ? m->sb[b][d] : m->bf[1][d]);
+      f.words[1 + d] = vs;
+    }
+    f.nspan = 4;
+    f.done = &m->ctl->done;
+    m->sts_stages += ns;
+  }
+  if (bytes > B->sts_dyn_bytes) {
+    if (B->sts_dyn) CHQ_CUDA(cudaFree(B->sts_dyn));
+    B->sts_dyn = nullptr;
+    B->sts_dyn_bytes = 0;
+    CHQ_CUDA(cudaMalloc(&B->sts_dyn, bytes));
+    B->sts_dyn_bytes = bytes;
+  }
+  CHQ_CUDA(cudaMemcpyAsync(B->sts_dyn, tab.data(), bytes, cudaMemcpyHostToDevice, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));   // the host table is freed on return
+  const int *nst_dev = reinterpret_cast<const int *>(B->sts_dyn);
+  const double *coef_dev = reinterpret_cast<const double *>(B->sts_dyn + o_coef);
+  const dim3 b2(32, 8);
+  const unsigned nspan = (unsigned)B->k_span.nblocks;
+  span_batched<<<nspan, 256, 0, s>>>((const SpanArgs *)B->a_sts_copy0, B->k_span.slots, n);
+  CHQ_CUDA(cudaGetLastError());
+  ++L;
+  for (int st = 1; st <= smax; ++st) {
+    const int bi = wrote(st - 1), bo = wrote(st);
+    const int form = st == 1 ? 0 : st == 2 ? 1 : 2 + (st % 3);
+    sts_skip_kernel<<<(n + 127) / 128, 128, 0, s>>>(B->sts_skip, nst_dev, n, st);
+    c2p_batched<P><<<(unsigned)B->k_c2p.nblocks, b2, 0, s>>>((const C2pArgs<P> *)B->a_sts_c2p[bi], B->k_c2p.slots, n);
+    span_batched<<<nspan, 256, 0, s>>>((const SpanArgs *)B->a_sts_zero, B->k_span.slots, n);
+    CHQ_CUDA(cudaGetLastError());
+    L += 3;
+    if (B->k_diff.nblocks) {
+      diff_flux_batched<P><<<(unsigned)B->k_diff.nblocks, 256, 0, s>>>((const DiffArgs<P> *)B->a_sts_diff[bi],
+                                                                        B->k_diff.slots, n);
+      ++L;
+    }
+    if (B->k_res.nblocks) {
+      resistive_emf_batched<P><<<(unsigned)B->k_res.nblocks, b2, 0, s>>>((const ResEmfArgs<P> *)B->a_sts_res[bi],
+                                                                         B->k_res.slots, n);
+      ++L;
+    }
+    sts_div_batched<P><<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const StsDivArgs<P> *)B->a_sts_div[st == 1 ? 0 : 1],
+                                                                      B->k_update.slots, n);
+    sts_combine_batched<<<(unsigned)B->k_update.nblocks, b2, 0, s>>>((const StsCombArgs *)B->a_sts_comb[form],
+                                                                      B->k_update.slots, n,
+                                                                      coef_dev + 5 * (size_t)(st - 1) * n);
+    CHQ_CUDA(cudaGetLastError());
+    L += 2;
+    if (B->k_bc[0].nblocks) bc_batched<0><<<(unsigned)B->k_bc[0].nblocks, 256, 0, s>>>((const BcArgs *)B->a_sts_bc[bo][0], B->k_bc[0].slots, n);
+    if (B->k_bc[1].nblocks) bc_batched<1><<<(unsigned)B->k_bc[1].nblocks, 256, 0, s>>>((const BcArgs *)B->a_sts_bc[bo][1], B->k_bc[1].slots, n);
+    if (B->k_bc[2].nblocks) bc_batched<2><<<(unsigned)B->k_bc[2].nblocks, 256, 0, s>>>((const BcArgs *)B->a_sts_bc[bo][2], B->k_bc[2].slots, n);
+    CHQ_CUDA(cudaGetLastError());
+    L += (B->k_bc[0].nblocks > 0) + (B->k_bc[1].nblocks > 0) + (B->k_bc[2].nblocks > 0);
+  }
+  span_batched<<<nspan, 256, 0, s>>>((const SpanArgs *)(B->sts_dyn + o_fin), B->k_span.slots, n);
+  CHQ_CUDA(cudaGetLastError());
+  ++L;
+  // the boundaries of the result in u0 / b?f0 (src/main.cpp:280)
+  if (B->k_bc[0].nblocks) bc_batched<0><<<(unsigned)B->k_bc[0].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[0], B->k_bc[0].slots, n);
+  if (B->k_bc[1].nblocks) bc_batched<1><<<(unsigned)B->k_bc[1].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[1], B->k_bc[1].slots, n);
+  if (B->k_bc[2].nblocks) bc_batched<2><<<(unsigned)B->k_bc[2].nblocks, 256, 0, s>>>((const BcArgs *)B->a_bc0[2], B->k_bc[2].slots, n);
+  CHQ_CUDA(cudaGetLastError());
+  L += (B->k_bc[0].nblocks > 0) + (B->k_bc[1].nblocks > 0) + (B->k_bc[2].nblocks > 0);
   return CHQ_OK;
 }
 
@@ -1573,7 +1796,7 @@ int batch_cycle(chq_batch *B, cudaStream_t s) {
     }
   }
   if (B->sts) {
-    const int rc = batch_sts<P>(B, s);
+    const int rc = batch_sts<P>(B, s, L);
     if (rc) return rc;
   }
   if (B->cool) {
@@ -1618,6 +1841,11 @@ void batch_free(chq_batch *B) {
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
   if (B->dev) cudaFree(B->dev);
+  if (B->sts_skip) cudaFree(B->sts_skip);
+  if (B->sts_dyn) cudaFree(B->sts_dyn);
+  B->sts_skip = nullptr;
+  B->sts_dyn = nullptr;
+  B->sts_dyn_bytes = 0;
   if (B->stream) cudaStreamDestroy(B->stream);
   B->exec = nullptr;
   B->graph = nullptr;

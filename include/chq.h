@@ -239,8 +239,9 @@ CHQ_API int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launch
  * member keeps its own dt (the parabolic limit included), clock, boundaries and FOFC
  * decisions, and stops at its own tlim, so its results are identical to stepping it alone.
  * With RKL2 the stage count of every member is a host decision each cycle: the batch
- * synchronises once per cycle and runs each member's super-time-stepping stages with its own
- * launches (no graph replay for such batches).
+ * synchronises once per cycle, then runs super-time-stepping stage j of all members in one
+ * launch per kernel kind, members past their own count skipping (no graph replay for such
+ * batches).
  * Membership is fixed at creation; meshes must outlive the batch. */
 typedef struct chq_batch chq_batch;
 CHQ_API int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out);

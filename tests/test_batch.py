@@ -63,15 +63,19 @@ SETS.update({
     "cooling_fp64": [(cases.ot(32), ("cooling.enabled=true", "cooling.lambda0=0.5")),
                      (cases.blast(16), ("cooling.enabled=true", "cooling.lambda0=5.0", "cooling.alpha=2.0",
                                         "cooling.tfloor=0.05"))],
-    # RKL2: the batched stages, then each member's own super-time-stepping stages
-    "rkl2_fp64": [(cases.ot(32), ("diffusion.eta=0.02", "diffusion.sts=true")),
-                  (cases.diffusion("temp", 1, 32, 8), ("diffusion.kappa=0.02", "diffusion.sts=true",
+    # RKL2: the hyperbolic stages, then the super-time-stepping stages batched across members
+    # with different stage counts (members past their count skip)
+    "rkl2_fp64": [(cases.ot(32), ("diffusion.eta=0.2", "diffusion.sts=true")),
+                  (cases.diffusion("temp", 1, 32, 8), ("diffusion.kappa=0.2", "diffusion.sts=true",
                                                       "mhd.reconstruct=ppm")),
                   (cases.blast(16), STRONG + ("diffusion.nu=5e-3", "diffusion.eta=5e-3", "diffusion.sts=true"))],
     "rkl2_cooling_fp64": [(cases.ot(32), ("diffusion.eta=0.02", "diffusion.sts=true", "cooling.enabled=true",
                                           "cooling.lambda0=0.2")),
                           (cases.blast(16), ("diffusion.nu=2e-3", "diffusion.sts=true", "cooling.enabled=true",
                                              "cooling.lambda0=1.0"))],
+    "rkl2_mixed_precision": [(cases.ot(32), ("diffusion.eta=0.02", "diffusion.sts=true")),
+                             (cases.diffusion("b", 2, 32, 8), ("diffusion.eta=0.1", "diffusion.sts=true",
+                                                              "mhd.reconstruct=ppm"))],
     "all_terms_fp64": [(cases.ot(32), GRAV_U + ("cooling.enabled=true", "cooling.lambda0=0.2", "diffusion.nu=2e-3",
                                                 "diffusion.kappa=2e-3")),
                        (cases.blast(16), STRONG + GRAV_P + ("cooling.enabled=true", "cooling.lambda0=1.0",
@@ -122,6 +126,10 @@ def test_batched_members_equal_solo(name, graph):
             assert st[j]["cycle"] == 7 and st[j]["t"] == clocks[j]["t"], (j, st[j], clocks[j])
             for f in FIELDS:
                 assert np.array_equal(m.get(f), expect[j][f]), (name, j, f)
+            assert m.sts_stages() == solo[j].sts_stages(), (name, j)
+        if name == "rkl2_fp64":
+            counts = [m.sts_stages() for m in solo]
+            assert min(counts) > 0 and len(set(counts)) > 1, counts   # members of unequal stage counts
     assert b.kernel_launches() > 0
     b.close()
 
