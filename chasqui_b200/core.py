@@ -216,6 +216,8 @@ class Mesh:
         return int(load_library().chq_mesh_bytes(self._h))
 
     def shape(self, name: str) -> tuple:
+        if name == "vtk":   # the VTK dump's cell data: 8 big-endian float32 per cell, in doubles
+            return (int(load_library().chq_array_size(self._h, b"vtk")),)
         nc = NCOMP.get(name, 1)
         if name in CELL_FIELDS:
             return (nc, self.nk, self.nj, self.ni)

@@ -1102,6 +1102,27 @@ __global__ void __launch_bounds__(256) pack_planes_kernel(const T *src, T *dst, 
   }
 }
 
+// The cell data of the reference's VTK dump (src/output.hpp:71-84) built on the device: rho,
+// prs, vx1, vx2, vx3, Bx1, Bx2, Bx3 over the active cells, i fastest, each value rounded to
+// float and stored big-endian, so the host writes the downloaded bytes as they are.
+template <class P>
+__global__ void __launch_bounds__(256) vtk_cells_kernel(Geom g, const P *w, const P *bcc, unsigned *dst) {
+  const long ncell = (long)g.nx1 * g.nx2 * g.nx3, total = 8 * ncell, vs = g.vstride;
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(q / ncell);
+    const long r0 = q - c * ncell;
+    const int i = g.is + (int)(r0 % g.nx1);
+    const long r = r0 / g.nx1;
+    const int j = g.js + (int)(r % g.nx2);
+    const int k = g.ks + (int)(r / g.nx2);
+    const long l = g.idx(k, j, i);
+    const P v = (c == 0) ? w[IDN * vs + l] : (c == 1) ? w[IPR * vs + l] : (c < 5) ? w[(c - 1) * vs + l]
+                                                                          : bcc[(c - 5) * vs + l];
+    const float f = (float)v;
+    dst[q] = __byte_perm(__float_as_uint(f), 0u, 0x0123u);
+  }
+}
+
 const size_t kStageBytes = 64ull << 20;   // per staging slot; planes per chunk: as many as fit
 const int kStageSlots = 4;
 
@@ -2144,6 +2165,7 @@ int chq_init_problem(chq_mesh *m, int problem, const double *prm, int nprm, void
 
 long chq_array_size(const chq_mesh *m, const char *name) {
   FieldRef f;
+  if (m && name && !std::strcmp(name, "vtk")) return 4L * m->g.nx1 * m->g.nx2 * m->g.nx3;   // 8 floats per cell
   if (!m || !name || !field_by_name(const_cast<chq_mesh *>(m), name, f)) return -1;
   return field_size(m, f);
 }
@@ -2183,7 +2205,15 @@ int snapshot_enqueue(chq_mesh *m, int nfields, const char *const *names, double 
   const Geom &g = m->g;
   std::vector<FieldRef> fr(nfields);
   size_t need = 0;
+  std::vector<char> vtk(nfields, 0);
+  const long ncell = (long)g.nx1 * g.nx2 * g.nx3;
   for (int q = 0; q < nfields; ++q) {
+    if (names[q] && host[q] && !std::strcmp(names[q], "vtk")) {
+      if (n[q] != 4 * ncell) return fail(CHQ_ERR_ARG, "size mismatch for field vtk");
+      vtk[q] = 1;
+      need += align_up((size_t)ncell * 32, 256);
+      continue;
+    }
     if (!names[q] || !host[q] || !field_by_name(m, names[q], fr[q]))
       return fail(CHQ_ERR_ARG, std::string("unknown field: ") + (names[q] ? names[q] : "(null)"));
     if (field_size(m, fr[q]) != n[q]) return fail(CHQ_ERR_ARG, std::string("size mismatch for field ") + names[q]);
@@ -2210,6 +2240,18 @@ int snapshot_enqueue(chq_mesh *m, int nfields, const char *const *names, double 
   char *p = m->snap;
   items.clear();
   for (int q = 0; q < nfields; ++q) {
+    if (vtk[q]) {
+      const unsigned blocks = (unsigned)std::max(1L, std::min<long>((8 * ncell + 255) / 256, 148L * 16));
+      m->nlaunch += 1;
+      if (m->mixed)
+        vtk_cells_kernel<float><<<blocks, 256, 0, s>>>(g, as<float>(m->w), as<float>(m->bcc), reinterpret_cast<unsigned *>(p));
+      else
+        vtk_cells_kernel<double><<<blocks, 256, 0, s>>>(g, as<double>(m->w), as<double>(m->bcc), reinterpret_cast<unsigned *>(p));
+      CHQ_CUDA(cudaGetLastError());
+      items.push_back(chq_mesh::SnapItem{host[q], n[q], 1, 0, sizeof(double), 0, p, {}});
+      p += align_up((size_t)ncell * 32, 256);
+      continue;
+    }
     // packed into the snapshot area in the host layout
     const FieldRef &f = fr[q];
     const int nx = f.face ? g.ni + 1 : g.ni, ny = f.face ? g.nj + 1 : g.nj, nz = f.face ? g.nk + 1 : g.nk;

@@ -205,8 +205,9 @@ int run(int argc, char **argv) {
     long n = 0;
     ~Pinned() { if (p) chq_host_free(p); }
   };
-  const char *snap_names[6] = {"w", "bcc", "u0", "b1f0", "b2f0", "b3f0"};
-  Pinned snap_buf[6];
+  // "vtk": the dump's cell data as the device builds it (big-endian float32 planes)
+  const char *snap_names[5] = {"vtk", "u0", "b1f0", "b2f0", "b3f0"};
+  Pinned snap_buf[5];
   std::vector<std::function<void()>> pending;
   auto buf = [&](int q) -> Pinned & {
     Pinned &b = snap_buf[q];
@@ -233,8 +234,8 @@ int run(int argc, char **argv) {
     if (vtk_now || rst_now) {
       flush();
       std::vector<int> fields;
-      if (vtk_now) fields.insert(fields.end(), {0, 1});
-      if (rst_now) fields.insert(fields.end(), {2, 3, 4, 5});
+      if (vtk_now) fields.push_back(0);
+      if (rst_now) fields.insert(fields.end(), {1, 2, 3, 4});
       std::vector<const char *> names;
       std::vector<double *> ptrs;
       std::vector<long> sizes;
@@ -251,7 +252,9 @@ int run(int argc, char **argv) {
         char fn[512];
         std::snprintf(fn, sizeof(fn), "%s.%04d.vtk", basename.c_str(), nvtk++);
         const std::string f = fn;
-        pending.push_back([&, f, tw, cw]() { chqd::write_vtk(g, as_vec(snap_buf[0]), as_vec(snap_buf[1]), f, tw, cw); });
+        pending.push_back([&, f, tw, cw]() {
+          chqd::write_vtk(g, reinterpret_cast<const char *>(snap_buf[0].p), f, tw, cw);
+        });
         next_vtk += dt_vtk;
       }
       if (rst_now) {
@@ -259,8 +262,8 @@ int run(int argc, char **argv) {
         std::snprintf(fn, sizeof(fn), "%s.%04d.rst", basename.c_str(), nrst++);
         const std::string f = fn;
         pending.push_back([&, f, tw, cw]() {
-          chqd::write_restart(g, f, tw, cw, as_vec(snap_buf[2]), as_vec(snap_buf[3]), as_vec(snap_buf[4]),
-                              as_vec(snap_buf[5]));
+          chqd::write_restart(g, f, tw, cw, as_vec(snap_buf[1]), as_vec(snap_buf[2]), as_vec(snap_buf[3]),
+                              as_vec(snap_buf[4]));
         });
         next_rst += dt_rst;
       }

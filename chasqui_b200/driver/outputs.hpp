@@ -35,8 +35,11 @@ inline void put_be_int(std::ofstream &f, int32_t v) {
 }
 
 // w: (6, nk, nj, ni) primitives, bcc: (3, nk, nj, ni) cell-centred field, both downloaded
-inline void write_vtk(const Grid &g, const std::vector<double> &w, const std::vector<double> &bcc,
-                      const std::string &path, double time, int cycle) {
+// Legacy VTK dump in the reference's layout (src/output.hpp:32-84). `cells` holds the eight
+// big-endian float32 scalar planes (rho, prs, vx1, vx2, vx3, Bx1, Bx2, Bx3 over the active
+// cells, i fastest) exactly as the file stores them; the device builds them (the "vtk"
+// snapshot field), so the host writes them without touching the values.
+inline void write_vtk(const Grid &g, const char *cells, const std::string &path, double time, int cycle) {
   std::ofstream f(path, std::ios::binary);
   if (!f) throw std::runtime_error("cannot write " + path);
   f << "# vtk DataFile Version 2.0\nChasqui MHD VTK Data\nBINARY\nDATASET RECTILINEAR_GRID\n";
@@ -58,26 +61,14 @@ inline void write_vtk(const Grid &g, const std::vector<double> &w, const std::ve
   f << "\nZ_COORDINATES " << n3 << " float\n";
   put_be_floats(f, z);
   f << "\n";
-  const size_t ncell = (size_t)g.nx1 * g.nx2 * g.nx3, nc = g.cells();
+  const size_t ncell = (size_t)g.nx1 * g.nx2 * g.nx3;
   f << "CELL_DATA " << ncell << "\n";
-  std::vector<float> buf(ncell);
-  auto dump = [&](const char *name, const std::vector<double> &src, int comp) {
-    size_t n = 0;
-    for (int k = g.ks; k <= g.ke; ++k)
-      for (int j = g.js; j <= g.je; ++j)
-        for (int i = g.is; i <= g.ie; ++i) buf[n++] = (float)src[comp * nc + g.c(k, j, i)];
-    f << "SCALARS " << name << " float\nLOOKUP_TABLE default\n";
-    put_be_floats(f, buf);
+  const char *names[8] = {"rho", "prs", "vx1", "vx2", "vx3", "Bx1", "Bx2", "Bx3"};
+  for (int q = 0; q < 8; ++q) {
+    f << "SCALARS " << names[q] << " float\nLOOKUP_TABLE default\n";
+    f.write(cells + (size_t)q * ncell * 4, (std::streamsize)(ncell * 4));
     f << "\n";
-  };
-  dump("rho", w, QD);
-  dump("prs", w, QP);
-  dump("vx1", w, QVX);
-  dump("vx2", w, QVY);
-  dump("vx3", w, QVZ);
-  dump("Bx1", bcc, 0);
-  dump("Bx2", bcc, 1);
-  dump("Bx3", bcc, 2);
+  }
 }
 
 struct RestartHeader {

@@ -101,7 +101,12 @@ CHQ_API int chq_download(chq_mesh *m, const char *name, double *host, long n, vo
  * from chq_host_alloc make the download asynchronous; pageable ones work but may block.
  * The host buffers must stay untouched until chq_snapshot_wait returns. One snapshot per
  * mesh is in flight; a new one waits for the previous. The snapshot area is allocated on
- * first use and kept with the mesh. */
+ * first use and kept with the mesh.
+ * The name "vtk" (snapshot only) is the cell data of the reference's VTK dump
+ * (src/output.hpp:71-84) built on the device: rho, prs, vx1, vx2, vx3, Bx1, Bx2, Bx3 over the
+ * active cells, i fastest, each rounded to float and stored big-endian, 32 bytes per cell
+ * (chq_array_size(m, "vtk") = 4 nx1 nx2 nx3 doubles of storage); a file writer emits the
+ * bytes unchanged after each SCALARS header. */
 CHQ_API int chq_snapshot(chq_mesh *m, int nfields, const char *const *names, double *const *host, const long *n);
 CHQ_API int chq_snapshot_wait(chq_mesh *m);
 
