@@ -31,7 +31,7 @@ def _rank_main(rank, world, port, q):
     mx = bench.dist_max(dist, 10.0 + rank)           # slowest rank's time wins
     buf = io.StringIO()
     with redirect_stdout(buf):
-        rc = bench.main_reference(type("A", (), {"cpu_n": 8, "warmup": 0, "steps": 1, "gpus": world})(), rank)
+        rc = bench.main_reference(type("A", (), {"n": 512, "cpu_n": 8, "warmup": 0, "steps": 1, "gpus": world})(), rank)
     bench.barrier(dist)
     dist.destroy_process_group()
     q.put((rank, mx, rc, buf.getvalue()))
