@@ -3,7 +3,7 @@ input file is run by the reference's own kernels compiled in place (oracle/_ref/
 built by `make -C oracle` from the reference sources) and the initial and final states, the
 clock and the history sums are stored in tests/golden/<case>.npz.
 
-    python tests/golden/make_golden.py        # needs oracle/_ref (the reference sources)
+    python tests/golden/make_golden.py [case ...]   # needs oracle/_ref (the reference sources)
 
 The fixtures let the parity tests run where the reference is not available."""
 import os
@@ -30,6 +30,13 @@ CASES = {
                                                 "cooling.enabled=true", "cooling.lambda0=0.5"], 5),
     "shock1d_64_plm_hlle_rk2": (cases.shock_tube(64), ["mhd.reconstruct=plm", "mhd.rsolver=hlle",
                                                        "time.integrator=rk2"], 10),
+    # RKL2 resistivity with five super-time-stepping stages per cycle
+    "ot2d_16_rkl2_eta": (cases.ot(16), ["diffusion.eta=0.2", "diffusion.sts=true"], 5),
+    # softened point mass on the strong blast, with first-order flux corrections
+    "blast3d_12_point_mass_fofc": (cases.blast(12), ["gravity.point_mass=true", "gravity.gm=0.05", "gravity.x0=0.05",
+                                                     "gravity.y0=-0.1", "gravity.z0=0.02", "gravity.rsoft=0.05",
+                                                     "problem.pres_in=1e4", "problem.pres_out=1e-3",
+                                                     "time.cfl=0.5"], 4),
 }
 
 
@@ -37,7 +44,10 @@ def main():
     from oracle.refsim import RefSim, available
     if not available():
         raise SystemExit("oracle/_ref is not built (make -C oracle with the reference sources present)")
+    only = set(sys.argv[1:])
     for name, (text, ov, ncyc) in CASES.items():
+        if only and name not in only:
+            continue
         ref = RefSim(text, list(ov))
         data = {"text": np.array(text), "overrides": np.array(ov if ov else [""]), "cycles": np.array(ncyc)}
         for f in FIELDS:
