@@ -2651,11 +2651,19 @@ int chq_history_drain(chq_mesh *m, double *rows, int max_rows, int *n, int *lost
   CHQ_CUDA(cudaStreamSynchronize(s));
   const int k = std::min(h.count, max_rows);
   if (k > 0) CHQ_CUDA(cudaMemcpyAsync(rows, h.rows, sizeof(double) * 12 * (size_t)k, cudaMemcpyDeviceToHost, s));
-  const int cleared[3] = {0, h.cap, 0};   // count, cap, lost
-  CHQ_CUDA(cudaMemcpyAsync(&m->hrec->count, cleared, sizeof(cleared), cudaMemcpyHostToDevice, s));
+  // rows that did not fit stay in the ring, oldest first, for the next drain
+  std::vector<double> rest((size_t)(h.count - k) * 12);
+  if (!rest.empty()) {
+    CHQ_CUDA(cudaMemcpyAsync(rest.data(), h.rows + (size_t)k * 12, sizeof(double) * rest.size(),
+                             cudaMemcpyDeviceToHost, s));
+    CHQ_CUDA(cudaStreamSynchronize(s));
+    CHQ_CUDA(cudaMemcpyAsync(h.rows, rest.data(), sizeof(double) * rest.size(), cudaMemcpyHostToDevice, s));
+  }
+  const int kept[3] = {h.count - k, h.cap, 0};   // count, cap, lost
+  CHQ_CUDA(cudaMemcpyAsync(&m->hrec->count, kept, sizeof(kept), cudaMemcpyHostToDevice, s));
   CHQ_CUDA(cudaStreamSynchronize(s));
   if (n) *n = k;
-  if (lost) *lost = h.lost + (h.count - k);
+  if (lost) *lost = h.lost;
   if (next) *next = h.next;
   return CHQ_OK;
 }

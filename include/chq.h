@@ -172,10 +172,10 @@ CHQ_API int chq_history(chq_mesh *m, double out[10], void *stream);
  * to a device ring of `capacity` rows, and next advances by dt_hst. capacity 0 turns recording
  * off. Synchronises the mesh stream; drops the captured cycle graph. */
 CHQ_API int chq_history_record(chq_mesh *m, double dt_hst, double next, double eps, int capacity);
-/* Synchronises the mesh stream, copies up to max_rows recorded rows (12 doubles each, oldest
- * first) into rows and empties the ring. *n: rows copied; *lost: rows dropped on a full ring
- * or beyond max_rows since the last drain; *next: the next output time. Any of the three
- * pointers may be null. CHQ_ERR_ARG if recording is off. */
+/* Synchronises the mesh stream and moves up to max_rows recorded rows (12 doubles each, oldest
+ * first) into rows; rows that do not fit stay in the ring for the next drain. *n: rows copied;
+ * *lost: rows dropped on a full ring since the last drain; *next: the next output time. Any
+ * of the three pointers may be null. CHQ_ERR_ARG if recording is off. */
 CHQ_API int chq_history_drain(chq_mesh *m, double *rows, int max_rows, int *n, int *lost, double *next);
 
 /* ---- host-buffer job entry point (end-to-end path) ---------------------------------------

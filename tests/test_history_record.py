@@ -80,8 +80,10 @@ def test_ring_counts_lost_rows_and_turns_off():
     rows, lost, _ = a.drain_history(8)
     assert len(rows) == 3 and lost == 2
     a.cycles(2)
-    rows, lost, _ = a.drain_history(1)
-    assert len(rows) == 1 and lost == 1
+    first, lost, _ = a.drain_history(1)   # the second row stays in the ring
+    assert len(first) == 1 and lost == 0
+    second, lost, _ = a.drain_history(8)
+    assert len(second) == 1 and lost == 0 and second[0, 0] > first[0, 0]
     a.record_history(0.0, 0.0, 0.0, capacity=0)
     with pytest.raises(ChqError):
         a.drain_history()
