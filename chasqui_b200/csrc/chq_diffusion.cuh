@@ -352,6 +352,16 @@ struct SpanArgs {
   const int *done;
 };
 
+// the same copies and zero fills for one mesh (all blocks of the launch)
+__global__ void __launch_bounds__(256) span_kernel(const SpanArgs A) {
+  for (int q = 0; q < A.nspan; ++q) {
+    unsigned long long *d = A.dst[q];
+    const unsigned long long *src = A.src[q];
+    for (long w = (long)blockIdx.x * blockDim.x + threadIdx.x; w < A.words[q]; w += (long)gridDim.x * blockDim.x)
+      d[w] = src ? src[w] : 0ull;
+  }
+}
+
 __global__ void __launch_bounds__(256) span_batched(const SpanArgs *args, const BatchSlot *slots, int n) {
   const int j = batch_job(slots, n, blockIdx.x);
   __shared__ __align__(16) unsigned char sa[sizeof(SpanArgs)];

@@ -927,13 +927,30 @@ struct StsState {
 
 // M(U, B) of (cell state whose primitives are in w, face fields b) into (mu, mb): zeroed
 // flux and EMF arrays, the diffusive fluxes, eta J, then -div F and -curl E (sts::Operator)
+// one launch for up to six whole-array copies or zero fills of one mesh
+int launch_spans(chq_mesh *m, const SpanArgs &a, cudaStream_t s) {
+  long words = 0;
+  for (int q = 0; q < a.nspan; ++q) words = std::max(words, a.words[q]);
+  const unsigned blocks = (unsigned)std::max(1L, std::min(1184L, (words + 1023) / 1024));
+  m->nlaunch += 1;
+  span_kernel<<<blocks, 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
 template <class P>
 int sts_operator(chq_mesh *m, double *const b[3], double *mu, double *const mb[3], cudaStream_t s) {
   const Geom &g = m->g;
-  const size_t fbytes = (size_t)g.vstride * m->psize;
-  for (int d = 0; d < 3; ++d) {
-    CHQ_CUDA(cudaMemsetAsync(m->flx[d], 0, fbytes * NVAR, s));
-    CHQ_CUDA(cudaMemsetAsync(m->e[d], 0, fbytes, s));
+  {
+    SpanArgs z{};   // the flux and EMF arrays start from zero (sts::Operator)
+    for (int d = 0; d < 3; ++d) {
+      z.dst[d] = (unsigned long long *)m->flx[d];
+      z.words[d] = NVAR * (long)g.vstride * (long)m->psize / 8;
+      z.dst[3 + d] = (unsigned long long *)m->e[d];
+      z.words[3 + d] = (long)g.vstride * (long)m->psize / 8;
+    }
+    z.nspan = 6;
+    if (int rc = launch_spans(m, z, s)) return rc;
   }
   int rc = do_diff<P>(m, b[0], b[1], b[2], nullptr, s);
   if (rc) return rc;
@@ -986,8 +1003,21 @@ int sts_advance(chq_mesh *m, double tau, double dt_par, cudaStream_t s, int &nst
   double *M0 = m->sm0, *Mj = m->smj;
   double *MB0[3] = {m->smb0[0], m->smb0[1], m->smb0[2]}, *MBj[3] = {m->smbj[0], m->smbj[1], m->smbj[2]};
   int rc;
-  CHQ_CUDA(cudaMemcpyAsync(Y0.u, m->u[0], ub, cudaMemcpyDeviceToDevice, s));
-  for (int k = 0; k < 3; ++k) CHQ_CUDA(cudaMemcpyAsync(Y0.b[k], m->bf[0][k], fb, cudaMemcpyDeviceToDevice, s));
+  // Y0 = (u0, b?f0) and, at the end, (u0, b?f0) = Y_s: whole arrays, one launch each
+  auto copy = [&](double *du, double *const db[3], const double *su, const double *const sb[3]) {
+    SpanArgs c{};
+    c.dst[0] = (unsigned long long *)du;
+    c.src[0] = (const unsigned long long *)su;
+    c.words[0] = (long)(ub / 8);
+    for (int k = 0; k < 3; ++k) {
+      c.dst[1 + k] = (unsigned long long *)db[k];
+      c.src[1 + k] = (const unsigned long long *)sb[k];
+      c.words[1 + k] = (long)(fb / 8);
+    }
+    c.nspan = 4;
+    return launch_spans(m, c, s);
+  };
+  if ((rc = copy(Y0.u, Y0.b, m->u[0], m->bf[0]))) return rc;
   if ((rc = launch_c2p<P>(m, c2p_args_ptr<P>(m, Y0.u, Y0.b[0], Y0.b[1], Y0.b[2], 0, nullptr, nullptr, nullptr), s)))
     return rc;
   if ((rc = sts_operator<P>(m, Y0.b, M0, MB0, s))) return rc;
@@ -1013,9 +1043,7 @@ int sts_advance(chq_mesh *m, double tau, double dt_par, cudaStream_t s, int &nst
     yjm1 = yj;
     yj = freed;
   }
-  CHQ_CUDA(cudaMemcpyAsync(m->u[0], yjm1.u, ub, cudaMemcpyDeviceToDevice, s));
-  for (int k = 0; k < 3; ++k) CHQ_CUDA(cudaMemcpyAsync(m->bf[0][k], yjm1.b[k], fb, cudaMemcpyDeviceToDevice, s));
-  return CHQ_OK;
+  return copy(m->u[0], m->bf[0], yjm1.u, yjm1.b);
 }
 
 // dx_min^2 / (2 ndim max(nu, eta, chi)) on the host, same operations as parabolic_dt
