@@ -800,19 +800,35 @@ template <class P, bool HST = false> CHQ_D void c2p_body(const C2pArgs<P> &A, in
   }
   if (A.compute_dt) block_min_pos(A.mdt_bits, mdt);   // one atomic per block (the whole block is here)
   if (hdue) {
-    // fixed-order block partial: warp shuffles, then the block's 8 warps in order
+    // fixed-order block partial. Warp level: a butterfly over the ten values padded to 16.
+    // At each xor step every lane keeps half of its values, sends the other half to its
+    // partner and combines (value 8 is a maximum, the rest sums), so 8 + 4 + 2 + 1 + 1
+    // shuffles replace ten separate 5-step reductions; afterwards lanes 2q and 2q + 1 hold
+    // value q of the warp. Then the block's 8 warps in order.
     __shared__ double hs[10][8];
-#pragma unroll
-    for (int q = 0; q < 10; ++q) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double x = __shfl_down_sync(0xffffffffu, hv[q], o);
-        hv[q] = (q == 8) ? fmax(hv[q], x) : hv[q] + x;
-      }
-    }
     const int lane = threadIdx.x, wid = threadIdx.y;   // blockDim (32, 8)
-    if (lane == 0)
-      for (int q = 0; q < 10; ++q) hs[q][wid] = hv[q];
+    double v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = (q < 10) ? hv[q] : 0.0;
+    int base = 0;   // value index of v[0] on this lane
+#pragma unroll
+    for (int half = 8; half >= 1; half >>= 1) {
+      const bool up = (lane & (2 * half)) != 0;   // this lane keeps the upper half
+#pragma unroll
+      for (int q = 0; q < half; ++q) {
+        const double keep = up ? v[half + q] : v[q];
+        const double give = up ? v[q] : v[half + q];
+        const double got = __shfl_xor_sync(0xffffffffu, give, 2 * half);
+        const int idx = base + (up ? half : 0) + q;
+        v[q] = (idx == 8) ? fmax(keep, got) : keep + got;
+      }
+      base += up ? half : 0;
+    }
+    {
+      const double got = __shfl_xor_sync(0xffffffffu, v[0], 1);
+      v[0] = (base == 8) ? fmax(v[0], got) : v[0] + got;
+    }
+    if ((lane & 1) == 0 && base < 10) hs[base][wid] = v[0];
     __syncthreads();
     if (wid == 0 && lane < 10) {
       double r = hs[lane][0];
