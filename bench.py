@@ -145,7 +145,33 @@ def blast_config(n: int, precision: int):
 BLAST_PARAMS = [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 20261203.0]   # p_in, p_out, r, b0, angle, noise, seed
 
 
-def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, profile_cycles=2):
+STATE_FIELDS = ("u0", "b1f0", "b2f0", "b3f0")
+L1_NAMES = ("rho", "m1", "m2", "m3", "E", "rho_s", "b1f", "b2f", "b3f")
+
+
+def active_views(st: dict, ng: int = 3):
+    """the active cells of u (6 variables) and the active faces of the three face fields"""
+    u = st["u0"]
+    out = [u[c, ng:-ng, ng:-ng, ng:-ng] for c in range(6)]
+    out.append(st["b1f0"][ng:-ng, ng:-ng, ng:-ng - 1 or None])
+    out.append(st["b2f0"][ng:-ng, ng:-ng - 1 or None, ng:-ng])
+    out.append(st["b3f0"][ng:-ng - 1 or None, ng:-ng, ng:-ng])
+    return out
+
+
+def l1_per_field(a: dict, b: dict) -> tuple[dict, dict]:
+    """per conserved variable and face field over the active region: relative L1
+    sum|a - b| / sum|b|, and the mean absolute difference per cell (or face)"""
+    rel, mean = {}, {}
+    for name, x, y in zip(L1_NAMES, active_views(a), active_views(b)):
+        den = float(np.sum(np.abs(y), dtype=np.float64))
+        num = float(np.sum(np.abs(x - y), dtype=np.float64))
+        rel[name] = num / den if den > 0 else num
+        mean[name] = num / y.size
+    return rel, mean
+
+
+def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, profile_cycles=2, keep_state=False):
     from chasqui_b200 import Mesh
     mesh = Mesh(blast_config(n, precision))
     mesh.init_problem("blast", BLAST_PARAMS)
@@ -177,8 +203,10 @@ def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, pro
     prof = mesh.profile_read(reset=True)
     mesh.profile(False)
     fofc, _ = mesh.counters()
+    state = {f: mesh.get(f) for f in STATE_FIELDS} if keep_state else None
     return mesh, {"ms": ms, "ms_max": ms_max, "launches": launches, "clock": ck, "prof": prof,
-                  "clocks": sampler.summary() if sampler else None, "fofc": fofc, "tune": tune}
+                  "clocks": sampler.summary() if sampler else None, "fofc": fofc, "tune": tune,
+                  "cycles_total": warmup + steps + profile_cycles, "state": state, "t_end": mesh.clock()["t"]}
 
 
 def config_rates(steps: int = 5, warmup: int = 3) -> dict:
@@ -430,15 +458,22 @@ name = blast
     return times
 
 
-def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 192)) -> dict:
+def _job_ok(m, cycles: int) -> bool:
+    """a job finished: its clock ran all cycles and its history sums are finite"""
+    return m.clock()["cycle"] == cycles and bool(np.isfinite(m.history()).all())
+
+
+def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 192), jobs=None) -> dict:
     """The ensemble configuration: njobs seeded jobs (OT 2D sizes[0]^2..sizes[1]^2, CPAW /
     blast 3D sizes[2]^3..sizes[3]^3, PPM or WENO-Z, mixed precision), `cycles` cycles each:
     all submitted at once to the batching server vs the same jobs as sequential one-job runs
-    and vs every job on its own stream at once."""
+    and vs every job on its own stream at once. Every arm checks each job (all cycles run,
+    finite state); the rates count the zone updates of the jobs that finished in that arm."""
     from chasqui_b200 import Mesh, Server, workloads
-    jobs = workloads.draw_jobs(njobs, seed=seed, precision=1, nlim=cycles, nmin2=sizes[0], nmax2=sizes[1],
-                               nmin3=sizes[2], nmax3=sizes[3])
-    zu = sum(j["cells"] for j in jobs) * cycles
+    if jobs is None:
+        jobs = workloads.draw_jobs(njobs, seed=seed, precision=1, nlim=cycles, nmin2=sizes[0], nmax2=sizes[1],
+                                   nmin3=sizes[2], nmax3=sizes[3])
+    zu_all = sum(j["cells"] for j in jobs) * cycles
     srv = Server(150 << 30, max_active=100000, cycles_per_step=cps)
     t0 = time.perf_counter()
     ids = [srv.submit(j["cfg"], j["problem"], j["params"]) for j in jobs]
@@ -446,15 +481,16 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
     while srv.step() > 0:
         steps += 1
     t_batched = time.perf_counter() - t0
-    ok = sum(srv.status(i)["state"] == "done" for i in ids)
+    done_b = [srv.status(i)["state"] == "done" for i in ids]
     srv.close()
+    done_s = []
     t0 = time.perf_counter()
     for j in jobs:
         m = Mesh(j["cfg"])
         m.init_problem(j["problem"], j["params"])
         m.prime(0.0)
         m.cycles(cycles)
-        m.clock()
+        done_s.append(_job_ok(m, cycles))
         m.close()
     t_seq = time.perf_counter() - t0
     # every job on its own mesh stream at once (no batching, no server)
@@ -470,14 +506,24 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
     for m in meshes:
         m.clock()
     t_con = time.perf_counter() - t0
+    done_c = [_job_ok(m, cycles) for m in meshes]
     for m in meshes:
         m.close()
-    return {"jobs": njobs, "cycles_each": cycles, "zone_updates": zu, "done": ok, "sizes": list(sizes),
-            "batched": {"seconds": t_batched, "value": zu / t_batched, "server_steps": steps},
-            "sequential": {"seconds": t_seq, "value": zu / t_seq},
-            "concurrent_streams": {"seconds": t_con, "value": zu / t_con},
-            "speedup_batched_vs_sequential": t_seq / t_batched,
-            "timing": "host wall clock around submit-to-drain, device synchronised at the end"}
+
+    def zu(done):
+        return sum(j["cells"] for j, d in zip(jobs, done) if d) * cycles
+
+    out = {"jobs": len(jobs), "cycles_each": cycles, "zone_updates": zu_all, "sizes": list(sizes),
+           "done": {"batched": sum(done_b), "sequential": sum(done_s), "concurrent_streams": sum(done_c)},
+           "batched": {"seconds": t_batched, "value": zu(done_b) / t_batched, "server_steps": steps},
+           "sequential": {"seconds": t_seq, "value": zu(done_s) / t_seq},
+           "concurrent_streams": {"seconds": t_con, "value": zu(done_c) / t_con},
+           "speedup_batched_vs_sequential": t_seq / t_batched,
+           "timing": "host wall clock around submit-to-drain, device synchronised at the end"}
+    out["all_done"] = min(out["done"].values()) == len(jobs)
+    if not out["all_done"]:
+        print(f"ensemble: jobs that did not finish: {out['done']} of {len(jobs)}", file=sys.stderr)
+    return out
 
 
 def serving(njobs: int, rate: float, precision: int, seed: int, t_end=(0.005, 0.05), nmax2=512, nmax3=96,
@@ -523,11 +569,17 @@ def host_threads() -> int:
 
 
 # --------------------------------------------------------------------------------------
-def workload_config(n: int, world: int) -> dict:
-    """The `config` of both arms: the workload the metric is quoted on."""
-    return {"workload": f"blast3d {n}^3 ppm+hlld+rk3 fofc flatten, seeded 1e-3 density noise, FP64 form",
-            "cells": int(n) ** 3, "parallelism": "replicas" if world > 1 else "single",
-            "l2": "state (~67 GB) >> L2; no flush needed"}
+def workload_config(n: int, world: int, sample_of: int | None = None) -> dict:
+    """The `config` of an arm: the workload it times. `sample_of`: the size of the workload the
+    timed mesh is a bounded sample of (the reference arm, whose host state at 512^3 the sample
+    budget does not allow)."""
+    gb = 67.0 * (n / 512.0) ** 3   # FP64 state, ~67 GB at 512^3
+    c = {"workload": f"blast3d {n}^3 ppm+hlld+rk3 fofc flatten, seeded 1e-3 density noise, FP64 form",
+         "cells": int(n) ** 3, "parallelism": "replicas" if world > 1 else "single",
+         "l2": f"state (~{gb:.0f} GB) >> L2; no flush needed"}
+    if sample_of is not None and sample_of != n:
+        c["sample_of"] = f"blast3d {sample_of}^3 (same problem, same per-cell work; rate per zone update)"
+    return c
 
 
 def main_reference(args, rank):
@@ -545,12 +597,12 @@ def main_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
         "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args.n, args.gpus),
+        "config": workload_config(n, args.gpus, sample_of=args.n),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"blast3d {n}^3 with 1e-3 noise (a bounded sample of the {args.n}^3 workload, "
-                                   f"whose state the host sample budget does not allow), "
-                                   f"{len(times)} RK3 cycles after {args.warmup} warm-up; reference kernels, "
-                                   f"OpenMP dispatch"},
+                         "sample": f"blast3d {n}^3 with 1e-3 noise (a bounded sample of the {args.n}^3 workload: "
+                                   f"the same problem at the largest size whose host run fits the sample "
+                                   f"budget), {len(times)} RK3 cycles after {args.warmup} warm-up; reference "
+                                   f"kernels, OpenMP dispatch"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -564,7 +616,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="chasqui", choices=["chasqui", "reference"])
     ap.add_argument("--n", type=int, default=512)
-    ap.add_argument("--cpu-n", type=int, default=128)
+    ap.add_argument("--cpu-n", type=int, default=256)
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -588,7 +640,8 @@ def main(argv=None):
     n = args.n
     hbm, peak_kind = peaks()
 
-    mesh, r64 = run_form(n, 0, args.steps, args.warmup, dist, local, sample_clocks=True)
+    mesh, r64 = run_form(n, 0, args.steps, args.warmup, dist, local, sample_clocks=True,
+                         keep_state=not args.no_mixed)
     zones = float(n) ** 3
     value = world * zones * args.steps / (r64["ms_max"] / 1e3)
     ms_step = r64["ms_max"] / args.steps
@@ -622,8 +675,10 @@ def main(argv=None):
 
     mixed = None
     if not args.no_mixed:
-        meshm, rm = run_form(n, 1, args.steps, args.warmup, dist, local)
+        meshm, rm = run_form(n, 1, args.steps, args.warmup, dist, local, keep_state=True)
         vm = world * zones * args.steps / (rm["ms_max"] / 1e3)
+        l1, l1_abs = l1_per_field(rm["state"], r64["state"])
+        rm["state"] = r64["state"] = None
         pm = rm["prof"]
         km, kn = pm["fluxes"]
         mixed = {"value": vm, "ms_per_step": rm["ms_max"] / args.steps,
@@ -631,7 +686,14 @@ def main(argv=None):
                  "k1_gbs": BYTES_K1["mixed"] * zones / ((km / max(kn, 1)) / 1e3) / 1e9,
                  "speedup_vs_fp64": vm / value,
                  "kernel_ms_per_step": {k: v[0] / 2 for k, v in pm.items()},
-                 "autotune": tune_summary(rm["tune"])}
+                 "autotune": tune_summary(rm["tune"]),
+                 "l1_vs_fp64": {"per_field": l1, "max": max(l1.values()), "mean_abs_per_cell": l1_abs,
+                                "cycles": rm["cycles_total"],
+                                "t_fp64": r64["t_end"], "t_mixed": rm["t_end"],
+                                "what": "relative L1 sum|mixed - fp64| / sum|fp64| and mean |mixed - fp64| "
+                                        "over the active cells (u) and faces (b?f) after the same number of "
+                                        "cycles from the same initial state (b3f starts at zero, so its "
+                                        "relative figure is against a small norm)"}}
         meshm.close()
         del meshm
 
@@ -642,9 +704,11 @@ def main(argv=None):
     ens = None
     if not args.no_ensemble:
         ens = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 4)
-        # the same draw restricted to small meshes (32^2..128^2, 16^3..32^3), where one job
-        # alone cannot fill the device and batching is what keeps it busy
-        ens["small_jobs"] = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 16, sizes=(32, 128, 16, 32))
+        # the same draw restricted to small meshes (32^2..128^2, 24^3..48^3), where one job
+        # alone cannot fill the device and batching is what keeps it busy. (Below 24^3 the
+        # blast's r = 0.1 region covers fewer than two cells and the scheme itself breaks down
+        # on many strong-blast WENO-Z draws, in FP64 as in the reference.)
+        ens["small_jobs"] = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 16, sizes=(32, 128, 24, 48))
     srv = None
     if not args.no_serving:
         srv = [serving(args.srv_jobs, float(r), prec, 77 + rank)
@@ -653,7 +717,7 @@ def main(argv=None):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = host_threads()
-        times = cpu_reference(args.cpu_n, 1, 20, 15.0, threads)
+        times = cpu_reference(args.cpu_n, 1, 20, 20.0, threads)
         if times:
             cpu = {"value": args.cpu_n ** 3 / statistics.mean(times), "unit": UNIT, "cores": threads,
                    "kind": "reference",

@@ -2159,13 +2159,24 @@ int chq_init_problem(chq_mesh *m, int problem, const double *prm, int nprm, void
   a.problem = problem;
   a.gamma = m->cfg.gamma;
   for (int q = 0; q < nprm; ++q) a.prm[q] = prm[q];
+  if (problem == PG_BLAST) {
+    // the same operations as the host generator (chasqui_b200/ics.py blast_noise)
+    const double ang = prm[4] * M_PI / 180.0, b0 = prm[3];
+    double bx = b0 * std::cos(ang), by = b0 * std::sin(ang);
+    if (std::fabs(bx) < 1e-14 * b0) bx = 0.0;
+    if (std::fabs(by) < 1e-14 * b0) by = 0.0;
+    a.bxy[0] = bx;
+    a.bxy[1] = by;
+  }
   if (problem == PG_CPAW) {
+    // wavevector 2 pi (m1/L1, m2/L2, m3/L3) = 2 pi |mv| e1, with the host generator's
+    // operation order (chasqui_b200/ics.py cpaw_oblique: e1 = m/|m|, k = 2 pi |m|)
     const double L[3] = {m->g.x1max - m->g.x1min, m->g.x2max - m->g.x2min, m->g.x3max - m->g.x3min};
-    double kv[3], nrm = 0.0;
-    for (int q = 0; q < 3; ++q) { kv[q] = 2.0 * M_PI * prm[q] / L[q]; nrm += kv[q] * kv[q]; }
-    nrm = std::sqrt(nrm);
+    double mv[3];
+    for (int q = 0; q < 3; ++q) mv[q] = prm[q] / L[q];
+    const double nrm = std::sqrt(mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2]);
     if (!(nrm > 0.0)) return fail(CHQ_ERR_ARG, "cpaw: zero wavevector");
-    for (int q = 0; q < 3; ++q) a.e1[q] = kv[q] / nrm;
+    for (int q = 0; q < 3; ++q) a.e1[q] = mv[q] / nrm;
     // e2 perpendicular to e1 (prefer the x-y plane), e3 = e1 x e2
     const double t[3] = {std::fabs(a.e1[2]) < 0.9 ? 0.0 : 1.0, 0.0, std::fabs(a.e1[2]) < 0.9 ? 1.0 : 0.0};
     double e2[3] = {t[1] * a.e1[2] - t[2] * a.e1[1], t[2] * a.e1[0] - t[0] * a.e1[2], t[0] * a.e1[1] - t[1] * a.e1[0]};
@@ -2174,7 +2185,7 @@ int chq_init_problem(chq_mesh *m, int problem, const double *prm, int nprm, void
     a.e3[0] = a.e1[1] * a.e2[2] - a.e1[2] * a.e2[1];
     a.e3[1] = a.e1[2] * a.e2[0] - a.e1[0] * a.e2[2];
     a.e3[2] = a.e1[0] * a.e2[1] - a.e1[1] * a.e2[0];
-    a.kmag = nrm;
+    a.kmag = 2.0 * M_PI * nrm;
   }
   a.u = m->u[0];
   a.b1 = m->bf[0][0];

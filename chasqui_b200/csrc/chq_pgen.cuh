@@ -25,6 +25,8 @@ struct PgenArgs {
   double prm[12];
   // cpaw basis (e1 along k, e2, e3 transverse) and wavenumber
   double e1[3], e2[3], e3[3], kmag;
+  // blast: uniform field (b0 cos(angle), b0 sin(angle)), tiny components flushed to zero
+  double bxy[2];
   double *u, *b1, *b2, *b3;
 };
 
@@ -69,12 +71,10 @@ __global__ void __launch_bounds__(256) pgen_faces_kernel(const PgenArgs a) {
   const long l = g.idx(k, j, i);
   double b1 = 0.0, b2 = 0.0, b3 = 0.0;
   if (a.problem == PG_BLAST) {
-    const double ang = a.prm[4] * M_PI / 180.0, b0 = a.prm[3];
-    double bx = b0 * cos(ang), by = b0 * sin(ang);
-    if (fabs(bx) < 1e-14 * b0) bx = 0.0;
-    if (fabs(by) < 1e-14 * b0) by = 0.0;
-    b1 = bx;
-    b2 = by;
+    // uniform field components, evaluated on the host (chq_init_problem) with the host's
+    // cos/sin so that they carry the same bits as the host generator's
+    b1 = a.bxy[0];
+    b2 = a.bxy[1];
   } else {
     const double xf = pg_x1f(g, i), yf = pg_x2f(g, j), zf = pg_x3f(g, k);
     const double xv = pg_x1v(g, i), yv = pg_x2v(g, j), zv = pg_x3v(g, k);
