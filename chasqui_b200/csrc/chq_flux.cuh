@@ -9,11 +9,14 @@
 // Work decomposition, two launches per stage:
 //   flux_x_kernel : one warp = 32 consecutive cells of a row; lane l computes the (aL, aR)
 //             pair of its cell once (stencil from L1) and receives its left neighbour's aR by
-//             __shfl_up_sync, so a warp emits 31 faces and no cell parabola is evaluated twice.
+//             __shfl_up_sync, so a warp emits 31 faces and no cell parabola is evaluated twice
+//             (PPM: slopes and unlimited interface values are shared between lanes too, and a
+//             warp emits 29 faces).
 //   flux_yz_kernel: lanes run along i (fully coalesced rows); each thread marches `seglen`
 //             faces along y or z with its stencil in a shared-memory window that cp.async
 //             refills one cell ahead, and parks the previous cell's aR in shared memory
-//             during the Riemann solve. z warps come first, then y.
+//             during the Riemann solve (PPM: the march carries each quantity's slope and
+//             unlimited interface value to the next cell). z warps come first, then y.
 // The batched forms (flux_x_batched, flux_yz_batched) run the same sweeps for many meshes.
 #pragma once
 #include "chq_common.cuh"
@@ -41,7 +44,7 @@ template <class P> struct FluxArgs {
   int active[3];
   int seglen;          // faces per thread along y/z sweeps
   long nwarp[3];       // warps per direction
-  int nseg[3];         // segments along the sweep (x: 31-face segments)
+  int nseg[3];         // segments along the sweep (x: XFaces-face segments)
   int nchunk;          // 32-wide i chunks for y/z sweeps (aligned to i = 0)
   const int *skip;     // optional device flag: nonzero -> kernel returns immediately
 };
@@ -91,6 +94,35 @@ template <class P> CHQ_D DirView<P> dir_view(const FluxArgs<P> &A, int d) {
   v.out[6] = A.et2[d];
   v.out[7] = A.et1[d];
   return v;
+}
+
+// ---------------------------------------------------------------------------------------
+// Flattening toward the cell value (PPM, PPMX, WENO-Z; src/recon.hpp:179-187 applied as in
+// src/physics.hpp:152-162) and the donor-cell fallback of a side that reconstructed to
+// rho <= floor or p <= floor, on the cell's (aL, aR) pairs of the 8 quantities.
+template <int R, class P>
+CHQ_D void finish_states(const FluxArgs<P> &A, P aL[8], P aR[8], const P qc[8], const P p5[5], P um1, P up1) {
+  if constexpr (R == R_PPM || R == R_PPMX || R == R_WENOZ) {
+    if (A.flatten) {
+      const P f = flattening<P>(p5, um1, up1);
+      if (f > P(0)) {
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+          aL[n] += f * (qc[n] - aL[n]);
+          aR[n] += f * (qc[n] - aR[n]);
+        }
+      }
+    }
+  }
+  const P dfl = P(A.eos.dfloor), pfl = P(A.eos.pfloor);
+  if (aL[0] <= dfl || aL[4] <= pfl) {
+#pragma unroll
+    for (int n = 0; n < 8; ++n) aL[n] = qc[n];
+  }
+  if (aR[0] <= dfl || aR[4] <= pfl) {
+#pragma unroll
+    for (int n = 0; n < 8; ++n) aR[n] = qc[n];
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -168,28 +200,7 @@ CHQ_D void cell_states_from(const FluxArgs<P> &A, const DirView<P> &V, int lc, P
     recon_cell<R>(q5, aL[7], aR[7]);
     qc[7] = q5[2];
   }
-  if constexpr (R == R_PPM || R == R_PPMX || R == R_WENOZ) {
-    if (A.flatten) {
-      const P f = flattening<P>(p5, um1, up1);
-      if (f > P(0)) {
-#pragma unroll
-        for (int n = 0; n < 8; ++n) {
-          aL[n] += f * (qc[n] - aL[n]);
-          aR[n] += f * (qc[n] - aR[n]);
-        }
-      }
-    }
-  }
-  // donor-cell fallback of a side that reconstructed to rho <= floor or p <= floor
-  const P dfl = P(A.eos.dfloor), pfl = P(A.eos.pfloor);
-  if (aL[0] <= dfl || aL[4] <= pfl) {
-#pragma unroll
-    for (int n = 0; n < 8; ++n) aL[n] = qc[n];
-  }
-  if (aR[0] <= dfl || aR[4] <= pfl) {
-#pragma unroll
-    for (int n = 0; n < 8; ++n) aR[n] = qc[n];
-  }
+  finish_states<R, P>(A, aL, aR, qc, p5, um1, up1);
 }
 
 // Stencil sources of cell_states_from: q5[2-RE .. 2+RE] of quantity n of the cell.
@@ -328,6 +339,160 @@ CHQ_D void sweep_x(const FluxArgs<P> &A, int wid) {
   if (have && lane > 0) face_flux<S, P>(A, V, lc, wl, aL);
 }
 
+// Faces per x-sweep warp: 31 in the per-cell form (lane 0 contributes only its right state),
+// 29 in the streaming PPM form below (lanes 0 and 31 contribute only their slope and interface
+// value, so the states of lanes 1..30 are complete and lanes 2..30 emit faces).
+template <int R, bool CHAR> struct XFaces { static constexpr int v = (R == R_PPM && !CHAR) ? 29 : 31; };
+
+// Streaming PPM (CW84, src/recon.hpp:21-78) along a row of 32 cells, one per lane. The
+// reference evaluates, for face i, the limited parabolas of cells i-1 and i from their
+// monotonised slopes and unlimited interface values, so each slope is evaluated three times
+// and each unlimited interface value twice over a row. Here lane c evaluates its own slope
+// s_c and the unlimited value at its right interface F_{c+1/2} once; the slope of cell c+1
+// and the value F_{c-1/2} come from the neighbouring lanes by warp shuffle. The operands of
+// every expression are the reference's, so the limited states are bitwise the same.
+template <int S, class P>
+CHQ_D void sweep_x_ppm(const FluxArgs<P> &A, int wid) {
+  const int lane = threadIdx.x & 31;
+  const int nseg = A.nseg[0];
+  const int row = wid / nseg;
+  const int seg = (int)(wid - row * nseg);
+  const int nj = A.hi[0][1] - A.lo[0][1] + 1;
+  const int k = A.lo[0][0] + (int)(row / nj);
+  const int j = A.lo[0][1] + (row - (row / nj) * nj);
+  const int c = A.lo[0][2] - 2 + 29 * seg + lane;   // this lane's cell
+  // lanes past the row's last face (and lane 0's stencil at the row start) read clamped
+  // indices inside the row; their states are never used
+  const int last = A.g.ni - 1;
+  const int cm2 = max(c - 2, 0), cm1 = max(c - 1, 0), c0 = min(c, last), cp1 = min(c + 1, last),
+            cp2 = min(c + 2, last);
+  const int base = A.g.idx32(k, j, 0);
+  const DirView<P> V = dir_view(A, 0);
+  P aL[8], aR[8], qc[8], p5[5], um1 = P(0), up1 = P(0);
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const P *src = V.src[n] + base;
+    const P qm = ldg(src + cm1), q0 = ldg(src + c0), qp = ldg(src + cp1);
+    const P sc = mc_slope(qm, q0, qp);
+    const P sp = __shfl_down_sync(0xffffffffu, sc, 1);    // s_{c+1}
+    const P fp = ppm_face(q0, qp, sc, sp);                 // F_{c+1/2}, unlimited
+    P l = __shfl_up_sync(0xffffffffu, fp, 1), r = fp;     // F_{c-1/2}
+    ppm_limit(q0, l, r);
+    aL[n] = l;
+    aR[n] = r;
+    qc[n] = q0;
+    if (n == 1) { um1 = qm; up1 = qp; }
+    if (n == 4) { p5[0] = ldg(src + cm2); p5[1] = qm; p5[2] = q0; p5[3] = qp; p5[4] = ldg(src + cp2); }
+  }
+  finish_states<R_PPM, P>(A, aL, aR, qc, p5, um1, up1);
+  P wl[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) wl[n] = __shfl_up_sync(0xffffffffu, aR[n], 1);
+  if (lane >= 2 && lane <= 30 && c <= A.hi[0][2]) face_flux<S, P>(A, V, base + c, wl, aL);
+}
+
+// Streaming PPM along a y/z march. Each thread's shared-memory column keeps, per quantity,
+// q_c, q_{c+1}, q_{c+2} (the last copied asynchronously one cell ahead), the slope s_c and
+// the unlimited interface value F_{c-1/2} computed at the previous cell; the velocity adds
+// u_{c-1} and the pressure p_{c-2}, p_{c-1} (flattening). A cell then evaluates one slope
+// (s_{c+1}) and one interface value (F_{c+1/2}) per quantity instead of three and two, with
+// the reference's operands (bitwise the same limited states as the per-cell form).
+struct PpmWin {
+  static constexpr int nslot = 43;
+  enum : int { Q0 = 0, Q1 = 1, Q2 = 2, S = 3, F = 4, X1 = 5, X2 = 6 };
+  CHQ_HD static constexpr int off(int n) {
+    return (n == 0) ? 0 : (n == 1) ? 5 : (n == 2) ? 11 : (n == 3) ? 16 : (n == 4) ? 21 : (n == 5) ? 28 : (n == 6) ? 33 : 38;
+  }
+};
+
+template <int S, class P>
+CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
+  const int lane = threadIdx.x & 31;
+  const int nseg = A.nseg[d];
+  const int nchunk = A.nchunk;
+  const int chunk = (int)(wid % nchunk);
+  const int rest = wid / nchunk;
+  const int seg = (int)(rest % nseg);
+  const int outer = (int)(rest / nseg);
+  const int i = 32 * chunk + lane;
+  if (i < A.lo[d][2] || i > A.hi[d][2]) return;
+  const int sweep_lo = (d == 1) ? A.lo[1][1] : A.lo[2][0];
+  const int sweep_hi = (d == 1) ? A.hi[1][1] : A.hi[2][0];
+  const int f0 = sweep_lo + A.seglen * seg;
+  const int f1 = min(f0 + A.seglen - 1, sweep_hi);
+  const DirView<P> V = dir_view(A, d);
+  const int st = V.st;
+  int lc = (d == 1) ? A.g.idx32(A.lo[1][0] + outer, f0 - 1, i) : A.g.idx32(f0 - 1, A.lo[2][1] + outer, i);
+  const int t = threadIdx.x;
+  P *col = win + t;
+#define CHQ_SLOT(n, k) col[(PpmWin::off(n) + PpmWin::k) * kYzThreads]
+  // cell f0-1: its slope, its left interface value and the window, from direct loads
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const P *src = V.src[n] + lc;
+    const P qm2 = ldg(src - 2 * st), qm1 = ldg(src - st), q0 = ldg(src), qp1 = ldg(src + st);
+    const P sm = mc_slope(qm2, qm1, q0), sc = mc_slope(qm1, q0, qp1);
+    CHQ_SLOT(n, Q0) = q0;
+    CHQ_SLOT(n, Q1) = qp1;
+    CHQ_SLOT(n, S) = sc;
+    CHQ_SLOT(n, F) = ppm_face(qm1, q0, sm, sc);
+    if (n == 1) CHQ_SLOT(1, X1) = qm1;
+    if (n == 4) {
+      CHQ_SLOT(4, X1) = qm2;
+      CHQ_SLOT(4, X2) = qm1;
+    }
+    cp_async_elem(&CHQ_SLOT(n, Q2), src + 2 * st);
+  }
+  cp_async_commit();
+  P wl[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) wl[n] = P(0);
+  for (int f = f0 - 1; f <= f1; ++f, lc += st) {
+    cp_async_wait_all();
+    const bool pre = (f < f1);
+    P aL[8], aR[8], qc[8], p5[5], um1 = P(0), up1 = P(0);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const P q0 = CHQ_SLOT(n, Q0), q1 = CHQ_SLOT(n, Q1), q2 = CHQ_SLOT(n, Q2);
+      const P sc = CHQ_SLOT(n, S), fm = CHQ_SLOT(n, F);
+      const P sp = mc_slope(q0, q1, q2);          // s_{c+1}
+      const P fp = ppm_face(q0, q1, sc, sp);      // F_{c+1/2}, unlimited
+      P l = fm, r = fp;
+      ppm_limit(q0, l, r);
+      aL[n] = l;
+      aR[n] = r;
+      qc[n] = q0;
+      if (n == 1) {
+        um1 = CHQ_SLOT(1, X1);
+        up1 = q1;
+        CHQ_SLOT(1, X1) = q0;
+      }
+      if (n == 4) {
+        p5[0] = CHQ_SLOT(4, X1);
+        p5[1] = CHQ_SLOT(4, X2);
+        p5[2] = q0;
+        p5[3] = q1;
+        p5[4] = q2;
+        CHQ_SLOT(4, X1) = p5[1];
+        CHQ_SLOT(4, X2) = q0;
+      }
+      CHQ_SLOT(n, Q0) = q1;
+      CHQ_SLOT(n, Q1) = q2;
+      CHQ_SLOT(n, S) = sp;
+      CHQ_SLOT(n, F) = fp;
+      if (pre) cp_async_elem(&CHQ_SLOT(n, Q2), V.src[n] + lc + 3 * st);
+    }
+    cp_async_commit();
+    finish_states<R_PPM, P>(A, aL, aR, qc, p5, um1, up1);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) park[n * kYzThreads + t] = aR[n];
+    if (f >= f0) face_flux<S, P>(A, V, lc, wl, aL);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) wl[n] = park[n * kYzThreads + t];
+  }
+#undef CHQ_SLOT
+}
+
 // y (d = 1) or z (d = 2) sweep: one code copy, direction in the view. The right state
 // carried to the next face is parked in this thread's shared-memory slot during the
 // Riemann solve, which keeps it out of the registers at the solver's peak. With WIN the
@@ -336,6 +501,10 @@ CHQ_D void sweep_x(const FluxArgs<P> &A, int wid) {
 // cached loads whose lines a y/z march cannot keep in L1.
 template <int R, int S, bool CHAR, bool WIN, class P>
 CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
+  if constexpr (R == R_PPM && !CHAR && WIN) {
+    sweep_yz_ppm<S, P>(A, d, wid, park, win);
+    return;
+  }
   const int lane = threadIdx.x & 31;
   const int nseg = A.nseg[d];
   const int nchunk = A.nchunk;
@@ -411,14 +580,20 @@ template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) ==
 template <class P> struct FluxYzMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUXYZ_MINB_D : CHQ_FLUXYZ_MINB_F; };
 
 template <int R, class P> __host__ __device__ constexpr size_t flux_yz_smem() {
-  return (size_t)(8 + ((Reach<R>::v > 0) ? 8 * (2 * Reach<R>::v + 1) : 0)) * kYzThreads * sizeof(P);
+  // park (8) + window: streaming PPM 43 slots (the characteristic PPM form uses 40 of them),
+  // otherwise 8 quantities x (2 reach + 1)
+  return (size_t)(8 + ((R == R_PPM) ? PpmWin::nslot : (Reach<R>::v > 0) ? 8 * (2 * Reach<R>::v + 1) : 0)) *
+         kYzThreads * sizeof(P);
 }
 
 template <int R, int S, bool CHAR, class P>
 __global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_x_kernel(const FluxArgs<P> A) {
   if (A.skip && *A.skip) return;
   const int wid = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
-  if (wid < (int)A.nwarp[0]) sweep_x<R, S, CHAR, P>(A, wid);
+  if (wid < (int)A.nwarp[0]) {
+    if constexpr (R == R_PPM && !CHAR) sweep_x_ppm<S, P>(A, wid);
+    else sweep_x<R, S, CHAR, P>(A, wid);
+  }
 }
 
 template <int R, int S, bool CHAR, class P>
@@ -442,7 +617,10 @@ __global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_x_batched(const
   const FluxArgs<P> &A = stage_args(args, j, sa);
   if (A.skip && *A.skip) return;
   const int wid = (int)(blockIdx.x - slots[j].off) * 4 + (int)(threadIdx.x >> 5);
-  if (wid < (int)A.nwarp[0]) sweep_x<R, S, CHAR, P>(A, wid);
+  if (wid < (int)A.nwarp[0]) {
+    if constexpr (R == R_PPM && !CHAR) sweep_x_ppm<S, P>(A, wid);
+    else sweep_x<R, S, CHAR, P>(A, wid);
+  }
 }
 
 template <int R, class P> __host__ __device__ constexpr size_t flux_yz_batched_smem() {

@@ -345,8 +345,10 @@ FluxArgs<P> flux_args(chq_mesh *m, int cur, unsigned dirmask) {
   a.lhlld_phi = m->cfg.lhlld_phi;
   a.seglen = m->seglen;
   a.nchunk = (m->g.ni + 1 + 31) / 32;
-  // x: rows x 31-face segments; y/z: i chunks x outer x segments
-  a.nseg[0] = (m->hi[0][2] - m->lo[0][2] + 1 + 30) / 31;
+  // x: rows x segments of XFaces faces (29 for streaming PPM, else 31); y/z: i chunks x
+  // outer x segments
+  const int xf = (m->cfg.recon == R_PPM && !m->cfg.characteristic) ? XFaces<R_PPM, false>::v : XFaces<R_DC, false>::v;
+  a.nseg[0] = (m->hi[0][2] - m->lo[0][2] + 1 + xf - 1) / xf;
   a.nwarp[0] = a.active[0] ? (long)(m->hi[0][0] - m->lo[0][0] + 1) * (m->hi[0][1] - m->lo[0][1] + 1) * a.nseg[0] : 0;
   a.nseg[1] = (m->hi[1][1] - m->lo[1][1] + 1 + a.seglen - 1) / a.seglen;
   a.nwarp[1] = a.active[1] ? (long)a.nchunk * (m->hi[1][0] - m->lo[1][0] + 1) * a.nseg[1] : 0;
