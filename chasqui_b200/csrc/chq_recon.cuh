@@ -106,6 +106,39 @@ template <class T> CHQ_HD T wenoz_right(T fm2, T fm1, T f0, T fp1, T fp2) {
   return inv * (a0 * q0 + a1 * q1 + a2 * q2);
 }
 
+// Both interface values of one cell: aR = wenoz_right(q_{c-2..c+2}) and aL = the same
+// formula on the mirrored stencil. Mirroring maps the smoothness indicators (b0, b1, b2) to
+// (b2, b1, b0) with bitwise-equal values (the sums are commutative and a square does not see
+// the sign), and tau to itself, so both sides share the three indicators and the three
+// quotients tau / (b + eps): 5 divisions per cell instead of 8, same results bit for bit.
+template <class T> CHQ_HD void wenoz_cell(const T q[5], T &aL, T &aR) {
+  const T eps = Tiny<T>::weno_eps;
+  const T c13 = T(13) / T(12);
+  const T b0 = c13 * sqr((q[0] + q[2]) - T(2) * q[1]) + T(0.25) * sqr((T(3) * q[2] + q[0]) - T(4) * q[1]);
+  const T b1 = c13 * sqr((q[1] + q[3]) - T(2) * q[2]) + T(0.25) * sqr(q[1] - q[3]);
+  const T b2 = c13 * sqr((q[4] + q[2]) - T(2) * q[3]) + T(0.25) * sqr((T(3) * q[2] + q[4]) - T(4) * q[3]);
+  const T tau = fabs_(b0 - b2);
+  const T d0 = T(1) + divz(tau, b0 + eps);
+  const T d1 = T(1) + divz(tau, b1 + eps);
+  const T d2 = T(1) + divz(tau, b2 + eps);
+  {
+    const T a0 = T(0.1) * d0, a1 = T(0.6) * d1, a2 = T(0.3) * d2;
+    const T inv = T(1) / (a0 + a1 + a2);
+    const T r0 = div6(T(2) * q[0] - T(7) * q[1] + T(11) * q[2]);
+    const T r1 = div6(-q[1] + T(5) * q[2] + T(2) * q[3]);
+    const T r2 = div6(T(2) * q[2] + T(5) * q[3] - q[4]);
+    aR = inv * (a0 * r0 + a1 * r1 + a2 * r2);
+  }
+  {
+    const T a0 = T(0.1) * d2, a1 = T(0.6) * d1, a2 = T(0.3) * d0;
+    const T inv = T(1) / (a0 + a1 + a2);
+    const T r0 = div6(T(2) * q[4] - T(7) * q[3] + T(11) * q[2]);
+    const T r1 = div6(-q[3] + T(5) * q[2] + T(2) * q[1]);
+    const T r2 = div6(T(2) * q[2] + T(5) * q[1] - q[0]);
+    aL = inv * (a0 * r0 + a1 * r1 + a2 * r2);
+  }
+}
+
 // CW84 flattening coefficient of the cell with pressures p5 = p_{c-2..c+2} and normal
 // velocities um1 = u_{c-1}, up1 = u_{c+1} (src/recon.hpp:179-187)
 template <class T> CHQ_HD T flattening(const T p5[5], T um1, T up1) {
@@ -143,8 +176,7 @@ template <int R, class T> CHQ_HD void recon_cell(const T q5[5], T &aL, T &aR) {
     aR = ppmx_face(q5[1], q5[2], q5[3], q5[4]);
     ppmx_limit(q5[0], q5[1], q5[2], q5[3], q5[4], aL, aR);
   } else {
-    aR = wenoz_right(q5[0], q5[1], q5[2], q5[3], q5[4]);
-    aL = wenoz_right(q5[4], q5[3], q5[2], q5[1], q5[0]);
+    wenoz_cell(q5, aL, aR);
   }
 }
 
