@@ -8,8 +8,11 @@ Default workload: 3D MHD blast, 512^3, PPM + HLLD + RK3, FOFC and flattening on,
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl chasqui|reference] [--n 512]
 
-Multi-GPU: the path does not shard (single-block solver): N ranks run N independent
-replicas ("replicas only"); value = all ranks' zone updates / max-over-ranks device time.
+Multi-GPU: a single mesh does not shard (single-block solver): for the headline N ranks run
+N independent replicas ("replicas only"); value = all ranks' zone updates / max-over-ranks
+device time. The ensemble and serving workloads shard by job (chasqui_b200.dispatch): every
+rank sees the same draw or request stream and runs its share; metrics are gathered on the
+host, with no collective on the data path.
 Every timing is CUDA-event device time on the mesh's stream. The state (~67 GB FP64 at
 512^3) is far larger than L2, so no flush is needed between steps.
 """
@@ -463,17 +466,23 @@ def _job_ok(m, cycles: int) -> bool:
     return m.clock()["cycle"] == cycles and bool(np.isfinite(m.history()).all())
 
 
-def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 192), jobs=None) -> dict:
+def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 192), dist=None, rank: int = 0,
+             world: int = 1) -> dict:
     """The ensemble configuration: njobs seeded jobs (OT 2D sizes[0]^2..sizes[1]^2, CPAW /
     blast 3D sizes[2]^3..sizes[3]^3, PPM or WENO-Z, mixed precision), `cycles` cycles each:
     all submitted at once to the batching server vs the same jobs as sequential one-job runs
     and vs every job on its own stream at once. Every arm checks each job (all cycles run,
-    finite state); the rates count the zone updates of the jobs that finished in that arm."""
-    from chasqui_b200 import Mesh, Server, workloads
-    if jobs is None:
-        jobs = workloads.draw_jobs(njobs, seed=seed, precision=1, nlim=cycles, nmin2=sizes[0], nmax2=sizes[1],
-                                   nmin3=sizes[2], nmax3=sizes[3])
-    zu_all = sum(j["cells"] for j in jobs) * cycles
+    finite state); the rates count the zone updates of the jobs that finished in that arm.
+    With several ranks every rank draws the same jobs and runs its share (dispatch.shard_jobs);
+    each arm starts at a barrier, its time is the slowest rank's and its zone updates the
+    sum over ranks."""
+    from chasqui_b200 import Mesh, Server, dispatch, workloads
+    drawn = workloads.draw_jobs(njobs, seed=seed, precision=1, nlim=cycles, nmin2=sizes[0], nmax2=sizes[1],
+                                nmin3=sizes[2], nmax3=sizes[3])
+    mine = dispatch.shard_jobs([dispatch.job_cost(j) for j in drawn], world)[rank]
+    jobs = [drawn[q] for q in mine]
+    zu_all = sum(j["cells"] for j in drawn) * cycles
+    barrier(dist)
     srv = Server(150 << 30, max_active=100000, cycles_per_step=cps)
     t0 = time.perf_counter()
     ids = [srv.submit(j["cfg"], j["problem"], j["params"]) for j in jobs]
@@ -484,6 +493,7 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
     done_b = [srv.status(i)["state"] == "done" for i in ids]
     srv.close()
     done_s = []
+    barrier(dist)
     t0 = time.perf_counter()
     for j in jobs:
         m = Mesh(j["cfg"])
@@ -494,6 +504,7 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
         m.close()
     t_seq = time.perf_counter() - t0
     # every job on its own mesh stream at once (no batching, no server)
+    barrier(dist)
     t0 = time.perf_counter()
     meshes = []
     for j in jobs:
@@ -513,28 +524,43 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
     def zu(done):
         return sum(j["cells"] for j, d in zip(jobs, done) if d) * cycles
 
-    out = {"jobs": len(jobs), "cycles_each": cycles, "zone_updates": zu_all, "sizes": list(sizes),
-           "done": {"batched": sum(done_b), "sequential": sum(done_s), "concurrent_streams": sum(done_c)},
-           "batched": {"seconds": t_batched, "value": zu(done_b) / t_batched, "server_steps": steps},
-           "sequential": {"seconds": t_seq, "value": zu(done_s) / t_seq},
-           "concurrent_streams": {"seconds": t_con, "value": zu(done_c) / t_con},
-           "speedup_batched_vs_sequential": t_seq / t_batched,
+    g = dispatch.gather(dist, {
+        "done_b_sum": sum(done_b), "done_s_sum": sum(done_s), "done_c_sum": sum(done_c),
+        "zu_b_sum": zu(done_b), "zu_s_sum": zu(done_s), "zu_c_sum": zu(done_c),
+        "t_b_max": t_batched, "t_s_max": t_seq, "t_c_max": t_con, "steps_max": steps, "jobs_list": [len(jobs)]})
+    out = {"jobs": len(drawn), "cycles_each": cycles, "zone_updates": zu_all, "sizes": list(sizes),
+           "done": {"batched": g["done_b_sum"], "sequential": g["done_s_sum"], "concurrent_streams": g["done_c_sum"]},
+           "batched": {"seconds": g["t_b_max"], "value": g["zu_b_sum"] / g["t_b_max"], "server_steps": g["steps_max"]},
+           "sequential": {"seconds": g["t_s_max"], "value": g["zu_s_sum"] / g["t_s_max"]},
+           "concurrent_streams": {"seconds": g["t_c_max"], "value": g["zu_c_sum"] / g["t_c_max"]},
+           "speedup_batched_vs_sequential": g["t_s_max"] / g["t_b_max"],
            "timing": "host wall clock around submit-to-drain, device synchronised at the end"}
-    out["all_done"] = min(out["done"].values()) == len(jobs)
+    if world > 1:
+        out["sharding"] = {"ranks": world, "jobs_per_rank": g["jobs_list"],
+                           "how": "same seeded draw on every rank, longest job first onto the least-loaded rank"}
+    out["all_done"] = min(out["done"].values()) == len(drawn)
     if not out["all_done"]:
-        print(f"ensemble: jobs that did not finish: {out['done']} of {len(jobs)}", file=sys.stderr)
+        print(f"ensemble: jobs that did not finish: {out['done']} of {len(drawn)}", file=sys.stderr)
     return out
 
 
 def serving(njobs: int, rate: float, precision: int, seed: int, t_end=(0.005, 0.05), nmax2=512, nmax3=96,
-            cps=4) -> dict:
+            cps=4, dist=None, rank: int = 0, world: int = 1) -> dict:
     """The serving configuration, scaled: njobs requests with Poisson arrivals at `rate` jobs/s,
     kinds and sizes from the ensemble distribution (capped at nmax2^2 / nmax3^3), end time
-    U[t_end]; submitted to the server as they arrive; time-to-solution per job."""
-    from chasqui_b200 import Server, workloads
-    jobs = workloads.draw_jobs(njobs, seed=seed, precision=precision, nmax2=nmax2, nmax3=nmax3, t_end=t_end)
+    U[t_end]; submitted to the server as they arrive; time-to-solution per job. With several
+    ranks every rank sees the same request stream and serves the requests that
+    dispatch.assign_stream gives it (least assigned work so far); latencies are pooled and
+    the throughput is all ranks' zone updates over the slowest rank's wall time."""
+    from chasqui_b200 import Server, dispatch, workloads
+    drawn = workloads.draw_jobs(njobs, seed=seed, precision=precision, nmax2=nmax2, nmax3=nmax3, t_end=t_end)
     rng = np.random.default_rng(seed + 1)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, njobs))
+    arr_all = np.cumsum(rng.exponential(1.0 / rate, njobs))
+    owner = dispatch.assign_stream([dispatch.job_cost(j) for j in drawn], world)
+    jobs = [j for j, o in zip(drawn, owner) if o == rank]
+    arrivals = np.array([a for a, o in zip(arr_all, owner) if o == rank])
+    njobs = len(jobs)
+    barrier(dist)
     srv = Server(150 << 30, max_active=100000, cycles_per_step=cps)
     ids = []
     nxt = 0
@@ -551,14 +577,21 @@ def serving(njobs: int, rate: float, precision: int, seed: int, t_end=(0.005, 0.
                 break
             time.sleep(max(0.0, min(0.01, arrivals[nxt] - (srv.stats()["clock"] - base))))
     st = [srv.status(i) for i in ids]
-    lat = np.array([s["t_done"] - s["t_submit"] for s in st])
-    zu = sum(s["zone_updates"] for s in st)
-    wall = max(s["t_done"] for s in st) - base
     srv.close()
-    return {"requests": njobs, "rate_jobs_per_s": rate, "precision": "mixed" if precision else "fp64",
-            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "zone_updates_per_s": zu / wall, "done": sum(s["state"] == "done" for s in st),
-            "t_end": list(t_end), "max_n2d": nmax2, "max_n3d": nmax3}
+    g = dispatch.gather(dist, {
+        "lat_list": [s["t_done"] - s["t_submit"] for s in st],
+        "zu_sum": sum(s["zone_updates"] for s in st),
+        "wall_max": (max(s["t_done"] for s in st) - base) if st else 0.0,
+        "done_sum": sum(s["state"] == "done" for s in st)})
+    lat = np.array(g["lat_list"])
+    out = {"requests": len(drawn), "rate_jobs_per_s": rate, "precision": "mixed" if precision else "fp64",
+           "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+           "zone_updates_per_s": g["zu_sum"] / g["wall_max"], "done": g["done_sum"],
+           "t_end": list(t_end), "max_n2d": nmax2, "max_n3d": nmax3}
+    if world > 1:
+        out["sharding"] = {"ranks": world, "how": "same request stream on every rank, each request to the "
+                                                  "rank with the least assigned work"}
+    return out
 
 
 def host_threads() -> int:
@@ -589,7 +622,7 @@ def main_reference(args, rank):
     n = args.cpu_n
     times = cpu_reference(n, args.warmup, args.steps, 1e9, threads)
     if times is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (make -C oracle)"}))
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (make -C oracle REF=<reference source tree>)"}))
         return 0
     per = statistics.mean(times)
     v = n ** 3 / per
@@ -703,15 +736,16 @@ def main(argv=None):
 
     ens = None
     if not args.no_ensemble:
-        ens = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 4)
+        ens = ensemble(args.ens_jobs, args.ens_cycles, 2026, 4, dist=dist, rank=rank, world=world)
         # the same draw restricted to small meshes (32^2..128^2, 24^3..48^3), where one job
         # alone cannot fill the device and batching is what keeps it busy. (Below 24^3 the
         # blast's r = 0.1 region covers fewer than two cells and the scheme itself breaks down
         # on many strong-blast WENO-Z draws, in FP64 as in the reference.)
-        ens["small_jobs"] = ensemble(args.ens_jobs, args.ens_cycles, 2026 + rank, 16, sizes=(32, 128, 24, 48))
+        ens["small_jobs"] = ensemble(args.ens_jobs, args.ens_cycles, 2026, 16, sizes=(32, 128, 24, 48), dist=dist,
+                                     rank=rank, world=world)
     srv = None
     if not args.no_serving:
-        srv = [serving(args.srv_jobs, float(r), prec, 77 + rank)
+        srv = [serving(args.srv_jobs, float(r), prec, 77, dist=dist, rank=rank, world=world)
                for r in args.srv_rates.split(",") for prec in (1, 0)]
 
     cpu = None

@@ -3,8 +3,8 @@
 // App. A), for reconstruction in characteristic variables. Right eigenvectors are the
 // columns of Rm, left eigenvectors the rows of Lm; wave order u-cf, u-ca, u-cs, u, u+cs,
 // u+ca, u+cf. Degenerate limits (B_perp = 0, bx = 0, cf = cs) follow
-// src/eigen_mhd.hpp:14-82. Only the nonzero entries are produced; the projection code
-// skips the structural zeros at compile time.
+// src/eigen_mhd.hpp:14-82. All 49 entries of L and R are written (the structural zeros
+// explicitly), so the projections can run over full 7 x 7 matrices.
 #pragma once
 #include "chq_common.cuh"
 

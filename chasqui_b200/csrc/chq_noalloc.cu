@@ -17,7 +17,6 @@
 // needs clearing, but calls that overlap on the GPU (other streams, other host threads on
 // the same device) race on it and must be serialised by the caller.
 #include <cuda_runtime.h>
-#include <mutex>
 #include <string>
 #include "chq.h"
 
@@ -33,9 +32,11 @@ constexpr int kNoallocSlots = kNoallocMaxUnits * 10 + 16;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoallocSlots];
 
-// device address of g_noalloc_scratch on each device (host code must not use the symbol)
-std::mutex g_mu;
-double *g_addr[64] = {};
+// Host code never dereferences g_noalloc_scratch: in host code the name is a stand-in, not a
+// device address. Each call asks the runtime for the array's address in the calling thread's
+// current context (cudaGetSymbolAddress allocates nothing). The address is not cached: after
+// a cudaDeviceReset, or in another context on the same device, the module is loaded anew at
+// another address, and a cached pointer would be stale.
 
 
 struct Dims {
@@ -124,23 +125,14 @@ extern "C" CHQ_API int chq_history_noalloc(int nx1, int nx2, int nx3, int ng, do
     return err(CHQ_ERR_ARG, "chq_history_noalloc: mesh too large for the fixed scratch (nx3 * ceil(nx2/128) = " +
                                 std::to_string(nunits) + " > " + std::to_string(kNoallocMaxUnits) + ")");
   if (!u || !b1 || !b2 || !b3 || !out) return err(CHQ_ERR_ARG, "chq_history_noalloc: null pointer");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return err(CHQ_ERR_CUDA, std::string("chq_history_noalloc: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= 64) return err(CHQ_ERR_ARG, "chq_history_noalloc: device index out of range");
-  double *scratch;
-  {
-    // first call on a device: resolve the device address of the static array (set-up)
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess)
-        return err(CHQ_ERR_CUDA, std::string("chq_history_noalloc set-up: ") + cudaGetErrorString(e));
-      g_addr[dev] = static_cast<double *>(p);
-    }
-    scratch = g_addr[dev];
-  }
+  // the static array's device address in the current context (the first call on a device
+  // also loads this module there: the set-up step)
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return err(CHQ_ERR_CUDA, std::string("chq_history_noalloc set-up: ") +
+                                 (e != cudaSuccess ? cudaGetErrorString(e) : "no device address"));
+  double *scratch = static_cast<double *>(p);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   Dims d;
   d.nx1 = nx1; d.nx2 = nx2; d.nx3 = nx3; d.ng = ng;

@@ -312,10 +312,14 @@ CHQ_API int chq_server_set_solo_cells(chq_server *s, long long cells);
  * be positive. Nothing is allocated: block partials live in one fixed static device array
  * of 8192 x 10 doubles (about 640 KiB, held by every device that loads the library until
  * the process exits), which limits meshes to nx3 * ceil(nx2 / 128) <= 8192 (e.g. 1024^3);
- * larger ones return CHQ_ERR_ARG. The first call on each device performs a one-time set-up
- * (it looks up that device address), so make it before any stream capture. All calls share
- * the array: calls that overlap on the GPU (other streams or threads on the same device)
- * race and must be serialised by the caller. */
+ * larger ones return CHQ_ERR_ARG. Every call looks up the array's device address in the
+ * current context (no allocation; still right after a cudaDeviceReset or in another context
+ * on the same device); the first call on each device also loads the library's device code
+ * there (a one-time set-up), so make that first call before any stream capture. All calls
+ * share the array: calls that overlap on the GPU (other streams or threads on the same
+ * device) race and must be serialised by the caller. One thread block reduces each k-plane x
+ * 128-row slab, so a 1-D mesh, or a large 2-D mesh with few rows, runs on few blocks and is
+ * slower than chq_history(), with the same results. */
 CHQ_API int chq_history_noalloc(int nx1, int nx2, int nx3, int ng, double dx1, double dx2, double dx3,
                                 const double *u, const double *b1, const double *b2, const double *b3,
                                 double out[10], void *stream);

@@ -65,7 +65,7 @@ def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         if not available():
-            raise RuntimeError(f"reference oracle not built: {REF_LIB} (make -C oracle)")
+            raise RuntimeError(f"reference oracle not built: {REF_LIB} (make -C oracle REF=<reference source tree>)")
         _lib = C.CDLL(REF_LIB)
         for n, r, a in _SIGS:
             f = getattr(_lib, n)

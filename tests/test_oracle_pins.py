@@ -13,7 +13,7 @@ from tests import cases
 
 REF = os.path.join(ROOT, "oracle", "_ref")
 pytestmark = pytest.mark.skipif(not os.path.exists(os.path.join(REF, "libchqref.so")),
-                                reason="oracle/_ref not built (make -C oracle)")
+                                reason="oracle/_ref not built (make -C oracle REF=<reference source tree>)")
 
 
 def test_reference_symmetry_test_passes():

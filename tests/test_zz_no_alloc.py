@@ -44,7 +44,12 @@ class DeviceArrays:
         self.ptrs = []
 
 
-@pytest.mark.parametrize("text,cycles", [(cases.blast(16), 3), (cases.ot(32), 4)], ids=["blast3d", "ot2d"])
+# the 8 x 200 Orszag-Tang mesh splits its rows into two 128-row slabs, the second one clipped
+# at the mesh edge; the shock tube is one-dimensional (one slab of one row)
+@pytest.mark.parametrize("text,cycles", [(cases.blast(16), 3), (cases.ot(32), 4),
+                                         (cases.ORSZAG_TANG.format(n=8).replace("nx2 = 8", "nx2 = 200"), 3),
+                                         (cases.shock_tube(64), 5)],
+                         ids=["blast3d", "ot2d", "ot2d_8x200", "shock1d"])
 def test_noalloc_history_matches_history_twice(text, cycles):
     from chasqui_b200 import load_library
     ref, mesh = make_pair(text, [])
