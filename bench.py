@@ -544,14 +544,52 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
     return out
 
 
+def run_alone(job) -> tuple[float, int, bool]:
+    """One request run by itself through the public Mesh API (create, generate, prime, cycles
+    to its end time, history, close): host wall seconds, zone updates, finished with a
+    finite state."""
+    from chasqui_b200 import Mesh
+    t0 = time.perf_counter()
+    m = Mesh(job["cfg"])
+    m.init_problem(job["problem"], job["params"])
+    m.prime(0.0)
+    tl, nl = float(job["cfg"].tlim), int(job["cfg"].nlim)
+    while True:
+        ck = m.clock()
+        if not ck["t"] < tl or (nl >= 0 and ck["cycle"] >= nl):
+            break
+        m.cycles(32)
+    ok = bool(np.isfinite(m.history()).all())
+    m.close()
+    return time.perf_counter() - t0, int(ck["cycle"]) * int(job["cells"]), ok
+
+
+_ALONE: dict = {}
+
+
+def fifo_one_at_a_time(service, arrivals) -> tuple[np.ndarray, float]:
+    """Completion times of a first-in first-out queue with one job on the device at a time:
+    each request starts when it has arrived and the previous one has finished, and takes its
+    measured service time. Returns the latencies and the last completion time."""
+    done = 0.0
+    lat = []
+    for s, a in zip(service, arrivals):
+        done = max(done, a) + s
+        lat.append(done - a)
+    return np.array(lat), done
+
+
 def serving(njobs: int, rate: float, precision: int, seed: int, t_end=(0.005, 0.05), nmax2=512, nmax3=96,
-            cps=4, dist=None, rank: int = 0, world: int = 1) -> dict:
+            cps=4, dist=None, rank: int = 0, world: int = 1, one_at_a_time: bool = False) -> dict:
     """The serving configuration, scaled: njobs requests with Poisson arrivals at `rate` jobs/s,
     kinds and sizes from the ensemble distribution (capped at nmax2^2 / nmax3^3), end time
     U[t_end]; submitted to the server as they arrive; time-to-solution per job. With several
     ranks every rank sees the same request stream and serves the requests that
     dispatch.assign_stream gives it (least assigned work so far); latencies are pooled and
-    the throughput is all ranks' zone updates over the slowest rank's wall time."""
+    the throughput is all ranks' zone updates over the slowest rank's wall time.
+    one_at_a_time: also the same requests served one job at a time (each request run alone,
+    its service time measured, completions from a first-in first-out queue over the same
+    arrival times; fifo_one_at_a_time)."""
     from chasqui_b200 import Server, dispatch, workloads
     drawn = workloads.draw_jobs(njobs, seed=seed, precision=precision, nmax2=nmax2, nmax3=nmax3, t_end=t_end)
     rng = np.random.default_rng(seed + 1)
@@ -591,7 +629,36 @@ def serving(njobs: int, rate: float, precision: int, seed: int, t_end=(0.005, 0.
     if world > 1:
         out["sharding"] = {"ranks": world, "how": "same request stream on every rank, each request to the "
                                                   "rank with the least assigned work"}
+    if one_at_a_time:
+        # service times do not depend on the arrival rate: measured once per request set
+        key = (precision, seed, tuple(t_end), nmax2, nmax3, len(drawn), rank, world)
+        if key not in _ALONE:
+            _ALONE[key] = [run_alone(j) for j in jobs]
+        runs = _ALONE[key]
+        lat1, last = fifo_one_at_a_time([r[0] for r in runs], arrivals)
+        g1 = dispatch.gather(dist, {"lat_list": lat1.tolist(), "zu_sum": sum(r[1] for r in runs),
+                                    "wall_max": last, "done_sum": sum(r[2] for r in runs)})
+        l1 = np.array(g1["lat_list"])
+        out["one_at_a_time"] = {"p50_s": float(np.percentile(l1, 50)), "p99_s": float(np.percentile(l1, 99)),
+                                "zone_updates_per_s": g1["zu_sum"] / g1["wall_max"], "done": g1["done_sum"],
+                                "how": "each request run alone (measured), first-in first-out over the same "
+                                       "arrival times"}
+        out["server_vs_one_at_a_time"] = {"throughput": out["zone_updates_per_s"] / out["one_at_a_time"]["zone_updates_per_s"],
+                                          "p50": out["one_at_a_time"]["p50_s"] / out["p50_s"],
+                                          "p99": out["one_at_a_time"]["p99_s"] / out["p99_s"]}
     return out
+
+
+def serving_study(args, dist, rank, world) -> dict:
+    """The serving configuration at its own size range: kinds and sizes of the ensemble draw
+    (64^2..1024^2, 32^3..192^3), t_end U[0.05, 0.5], Poisson arrivals, the 150 GB budget, for
+    the mixed and FP64 forms, with the one-job-at-a-time arm. Requests per leg: --srv-jobs."""
+    out = []
+    for prec in (1, 0):
+        for r in args.srv_rates.split(","):
+            out.append(serving(args.srv_jobs, float(r), prec, 77, t_end=(0.05, 0.5), nmax2=1024, nmax3=192, cps=8,
+                               dist=dist, rank=rank, world=world, one_at_a_time=True))
+    return {"serving_study": out}
 
 
 def host_threads() -> int:
@@ -660,6 +727,8 @@ def main(argv=None):
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
+    ap.add_argument("--serving-study", action="store_true",
+                    help="only the serving configuration at its own size range (see serving_study)")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     rank, local = env_int("RANK", 0), env_int("LOCAL_RANK", 0)
@@ -670,6 +739,13 @@ def main(argv=None):
     dist = dist_init()
     world = env_int("WORLD_SIZE", 1)
     set_device(local)
+    if args.serving_study:
+        res = serving_study(args, dist, rank, world)
+        if rank == 0:
+            print(json.dumps(res))
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     n = args.n
     hbm, peak_kind = peaks()
 
@@ -736,7 +812,7 @@ def main(argv=None):
 
     ens = None
     if not args.no_ensemble:
-        ens = ensemble(args.ens_jobs, args.ens_cycles, 2026, 4, dist=dist, rank=rank, world=world)
+        ens = ensemble(args.ens_jobs, args.ens_cycles, 2026, 16, dist=dist, rank=rank, world=world)
         # the same draw restricted to small meshes (32^2..128^2, 24^3..48^3), where one job
         # alone cannot fill the device and batching is what keeps it busy. (Below 24^3 the
         # blast's r = 0.1 region covers fewer than two cells and the scheme itself breaks down
@@ -745,7 +821,7 @@ def main(argv=None):
                                      rank=rank, world=world)
     srv = None
     if not args.no_serving:
-        srv = [serving(args.srv_jobs, float(r), prec, 77, dist=dist, rank=rank, world=world)
+        srv = [serving(args.srv_jobs, float(r), prec, 77, dist=dist, rank=rank, world=world, one_at_a_time=True)
                for r in args.srv_rates.split(",") for prec in (1, 0)]
 
     cpu = None

@@ -1471,6 +1471,9 @@ int batch_build(chq_batch *B) {
   if (B->sts) {
     cudaError_t e0 = cudaMalloc(&B->sts_skip, sizeof(int) * (size_t)n);
     if (e0 == cudaSuccess) e0 = cudaMemset(B->sts_skip, 0, sizeof(int) * (size_t)n);
+    // the memset runs on the legacy default stream, which the batch's non-blocking stream does
+    // not wait for: complete it before any batch kernel can read the flags
+    if (e0 == cudaSuccess) e0 = cudaStreamSynchronize(cudaStreamLegacy);
     if (e0 != cudaSuccess) return cuda_fail(e0, "batch RKL2 flags");
     o_span_s = slots_of(h, J, [](chq_mesh *m) {
       const long words = (long)(3 * NVAR + 3) * (long)m->g.vstride * (long)m->psize / 8;
@@ -1575,6 +1578,10 @@ int batch_build(chq_batch *B) {
   cudaError_t e = cudaMalloc(&B->dev, h.b.size());
   if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("batch tables: ") + cudaGetErrorString(e));
   e = cudaMemcpy(B->dev, h.b.data(), h.b.size(), cudaMemcpyHostToDevice);
+  // from pageable memory cudaMemcpy may return before the transfer has landed, and the
+  // batch's non-blocking stream does not wait for the legacy default stream that carries it:
+  // complete it before any batch kernel can read the tables
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
   if (e != cudaSuccess) return cuda_fail(e, "batch tables upload");
   char *d = B->dev;
   B->k_flux.slots = (BatchSlot *)(d + o_flux_s);
@@ -2677,6 +2684,8 @@ int chq_history_record(chq_mesh *m, double dt_hst, double next, double eps, int 
   h.fold = h.part + h.nblk * 10;
   h.rows = h.fold + h.nfold * 10;
   CHQ_CUDA(cudaMemcpy(p, &h, sizeof(h), cudaMemcpyHostToDevice));
+  // landed before the mesh's non-blocking stream can read it (see batch_build)
+  CHQ_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
   m->hrec = reinterpret_cast<HstRec *>(p);
   m->hrec_nfold = h.nfold;
   m->hrec_cap = capacity;

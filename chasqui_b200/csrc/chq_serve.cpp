@@ -12,8 +12,8 @@
 //      with the fewest cells; each lane has its own stream and replays a CUDA graph, so the
 //      flux kernel of one lane overlaps the memory-bound kernels of another. Batching alone
 //      serialises every job through the same kernel sequence.
-// Jobs of 2^21 cells or more (chq_server_set_solo_cells) are not batched: each runs "solo" on
-// its own mesh stream (replaying a CUDA graph of one cycle, except with RKL2) and the
+// Jobs of 2^21 cells or more (chq_server_set_solo_cells raises the threshold) are not
+// batched: each runs "solo" on its own mesh stream (replaying a CUDA graph of one cycle, except with RKL2) and the
 // server polls an event behind its chunk instead of waiting for it, so a large job never holds
 // up the lanes (or another large job). Diffusion (explicit or RKL2), cooling and gravity
 // batch with jobs that have the same terms switched on.
@@ -166,13 +166,9 @@ int retire_finished(chq_server *S) {
 }
 
 // Jobs of at least this many cells run solo: one mesh stream each, cycles replayed as a CUDA
-// graph. Running them concurrently overlaps one job's flux kernel with another's
-// memory-bound kernels, which a batch (one kernel kind at a time for all members) cannot.
-// On the 256-job ensemble (64^2..1024^2, 32^3..192^3) the server ran at 4.8e8
-// zone-updates/s with the threshold at 2^21 cells, 5.3e8 at 2^18 and 5.4e8 at 2^15 (the rate
-// of one stream per job); chq_server_set_solo_cells lowers it. The default stays at the
-// setting the serving runs were verified with.
-const long long kSoloCells = 1LL << 21;   // default of chq_server::solo_cells
+// graph; such a job fills the device by itself. chq_server_set_solo_cells can raise the
+// threshold, not lower it.
+const long long kSoloCells = 1LL << 21;   // default and minimum of chq_server::solo_cells
 
 // finished solo chunks: progress and retirement; with `block`, wait for a chunk when none
 // has finished
@@ -443,6 +439,9 @@ int chq_server_set_lanes(chq_server *S, int lanes) {
 
 int chq_server_set_solo_cells(chq_server *S, long long cells) {
   if (!S || cells < 0) return err(CHQ_ERR_ARG, "bad argument");
+  // lower thresholds (many more solo jobs) are not offered: a serving run with the threshold
+  // at 2^15 cells ended in a device fault whose cause is not known
+  if (cells < kSoloCells) return err(CHQ_ERR_ARG, "the solo threshold must be at least 2^21 cells");
   S->solo_cells = cells;
   return CHQ_OK;
 }

@@ -295,8 +295,8 @@ CHQ_API int chq_server_stats(chq_server *s, long long *used_bytes, int *active, 
 CHQ_API int chq_server_destroy(chq_server *s);
 /* concurrent batches (streams) per class, 1..64; takes effect for newly admitted jobs */
 CHQ_API int chq_server_set_lanes(chq_server *s, int lanes);
-/* jobs of at least `cells` cells run unbatched on their own streams (default 2^21; 0: every
- * job); takes effect for newly admitted jobs */
+/* jobs of at least `cells` cells run unbatched on their own streams (default and minimum
+ * 2^21; smaller values return CHQ_ERR_ARG); takes effect for newly admitted jobs */
 CHQ_API int chq_server_set_solo_cells(chq_server *s, long long cells);
 
 /* ---- history sums without any device allocation --------------------------------------------
