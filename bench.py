@@ -336,12 +336,15 @@ def history_rates(n: int = 400) -> dict:
 
 
 def tune_summary(tune):
-    """autotuned vs default march length of the flux kernel (ms per launch per length)"""
+    """autotuned vs default launch settings of the flux kernel: march length (x variant 0) and
+    x-sweep variant (at the best length), ms per launch for each candidate"""
     ms = tune["ms"]
     d = tune.get("default", 16)
-    out = {"default_seglen": d, "seglen": tune["seglen"], "flux_ms_per_launch": {str(k): v for k, v in ms.items()}}
-    if ms.get(d, -1) > 0 and ms.get(tune["seglen"], -1) > 0:
-        out["speedup_vs_default"] = ms[d] / ms[tune["seglen"]]
+    out = {"default_seglen": d, "seglen": tune["seglen"], "flux_ms_per_launch": {str(k): v for k, v in ms.items()},
+           "xvar": tune.get("xvar", 0), "flux_ms_per_xvar": {str(k): v for k, v in tune.get("xvar_ms", {}).items()}}
+    best = min([t for t in list(ms.values()) + list(tune.get("xvar_ms", {}).values()) if t > 0], default=-1)
+    if ms.get(d, -1) > 0 and best > 0:
+        out["speedup_vs_default"] = ms[d] / best
     return out
 
 
@@ -482,16 +485,24 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
     mine = dispatch.shard_jobs([dispatch.job_cost(j) for j in drawn], world)[rank]
     jobs = [drawn[q] for q in mine]
     zu_all = sum(j["cells"] for j in drawn) * cycles
-    barrier(dist)
-    srv = Server(150 << 30, max_active=100000, cycles_per_step=cps)
-    t0 = time.perf_counter()
-    ids = [srv.submit(j["cfg"], j["problem"], j["params"]) for j in jobs]
-    steps = 0
-    while srv.step() > 0:
-        steps += 1
-    t_batched = time.perf_counter() - t0
-    done_b = [srv.status(i)["state"] == "done" for i in ids]
-    srv.close()
+
+    def server_arm(autotune):
+        barrier(dist)
+        srv = Server(150 << 30, max_active=100000, cycles_per_step=cps, autotune=autotune)
+        t0 = time.perf_counter()
+        ids = [srv.submit(j["cfg"], j["problem"], j["params"]) for j in jobs]
+        steps = 0
+        while srv.step() > 0:
+            steps += 1
+        t = time.perf_counter() - t0
+        done = [srv.status(i)["state"] == "done" for i in ids]
+        srv.close()
+        return t, steps, done
+
+    # the lanes' batches tuned by the library's autotuner (first tuning of each size class
+    # inside the timed region), then the same with the default launch settings
+    t_batched, steps, done_b = server_arm(True)
+    t_default, _, done_d = server_arm(False)
     done_s = []
     barrier(dist)
     t0 = time.perf_counter()
@@ -525,12 +536,17 @@ def ensemble(njobs: int, cycles: int, seed: int, cps: int, sizes=(64, 1024, 32, 
         return sum(j["cells"] for j, d in zip(jobs, done) if d) * cycles
 
     g = dispatch.gather(dist, {
-        "done_b_sum": sum(done_b), "done_s_sum": sum(done_s), "done_c_sum": sum(done_c),
-        "zu_b_sum": zu(done_b), "zu_s_sum": zu(done_s), "zu_c_sum": zu(done_c),
-        "t_b_max": t_batched, "t_s_max": t_seq, "t_c_max": t_con, "steps_max": steps, "jobs_list": [len(jobs)]})
+        "done_b_sum": sum(done_b), "done_s_sum": sum(done_s), "done_c_sum": sum(done_c), "done_d_sum": sum(done_d),
+        "zu_b_sum": zu(done_b), "zu_s_sum": zu(done_s), "zu_c_sum": zu(done_c), "zu_d_sum": zu(done_d),
+        "t_b_max": t_batched, "t_s_max": t_seq, "t_c_max": t_con, "t_d_max": t_default, "steps_max": steps,
+        "jobs_list": [len(jobs)]})
     out = {"jobs": len(drawn), "cycles_each": cycles, "zone_updates": zu_all, "sizes": list(sizes),
-           "done": {"batched": g["done_b_sum"], "sequential": g["done_s_sum"], "concurrent_streams": g["done_c_sum"]},
-           "batched": {"seconds": g["t_b_max"], "value": g["zu_b_sum"] / g["t_b_max"], "server_steps": g["steps_max"]},
+           "done": {"batched": g["done_b_sum"], "sequential": g["done_s_sum"], "concurrent_streams": g["done_c_sum"],
+                    "batched_default_tiles": g["done_d_sum"]},
+           "batched": {"seconds": g["t_b_max"], "value": g["zu_b_sum"] / g["t_b_max"], "server_steps": g["steps_max"],
+                       "tiles": "autotuned per lane (march length, x-sweep variant)"},
+           "batched_default_tiles": {"seconds": g["t_d_max"], "value": g["zu_d_sum"] / g["t_d_max"]},
+           "autotuned_vs_default": g["t_d_max"] / g["t_b_max"],
            "sequential": {"seconds": g["t_s_max"], "value": g["zu_s_sum"] / g["t_s_max"]},
            "concurrent_streams": {"seconds": g["t_c_max"], "value": g["zu_c_sum"] / g["t_c_max"]},
            "speedup_batched_vs_sequential": g["t_s_max"] / g["t_b_max"],

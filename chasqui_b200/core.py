@@ -81,6 +81,9 @@ SIGNATURES = [
     ("chq_autotune", C.c_int, [_P, C.POINTER(C.c_int), _D]),
     ("chq_set_seglen", C.c_int, [_P, C.c_int]),
     ("chq_get_seglen", C.c_int, [_P]),
+    ("chq_autotune2", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, _D]),
+    ("chq_set_xvariant", C.c_int, [_P, C.c_int]),
+    ("chq_get_xvariant", C.c_int, [_P]),
     ("chq_history", C.c_int, [_P, _D, _P]),
     ("chq_history_record", C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int]),
     ("chq_history_drain", C.c_int, [_P, _D, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
@@ -103,6 +106,7 @@ SIGNATURES = [
     ("chq_batch_set_graph", C.c_int, [_P, C.c_int]),
     ("chq_batch_status", C.c_int, [_P, _D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("chq_batch_kernel_launches", C.c_longlong, [_P]),
+    ("chq_batch_autotune", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, _D]),
     ("chq_batch_stream", _P, [_P]),
     ("chq_server_create", C.c_int, [C.c_longlong, C.c_int, C.c_int, C.POINTER(_P)]),
     ("chq_server_submit", C.c_int, [_P, C.POINTER(chq_config), C.c_int, _D, C.c_int, C.POINTER(C.c_longlong)]),
@@ -114,12 +118,14 @@ SIGNATURES = [
     ("chq_server_destroy", C.c_int, [_P]),
     ("chq_server_set_lanes", C.c_int, [_P, C.c_int]),
     ("chq_server_set_solo_cells", C.c_int, [_P, C.c_longlong]),
+    ("chq_server_set_autotune", C.c_int, [_P, C.c_int]),
     ("chq_history_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       _P, _P, _P, _P, _D, _P]),
 ]
 
 TUNE_LENGTHS = (4, 8, 16, 32, 64)   # CHQ_TUNE_LENGTHS
 TUNE_NLEN = len(TUNE_LENGTHS)
+TUNE_NXVAR = 2                       # CHQ_TUNE_NXVAR
 
 PROFILE_KINDS = ("fluxes", "corner_emf", "update", "fofc_flag", "fofc_repair", "boundaries", "c2p_dt", "limiter",
                  "step_ctl", "diffusion", "sts")
@@ -326,12 +332,22 @@ class Mesh:
         return int(load_library().chq_sts_stages(self._h))
 
     def autotune(self) -> dict:
-        """Pick the y/z march length of the flux kernel by timing it on this mesh's state
-        (call after prime). Returns {"seglen": best, "ms": {length: ms per launch}}."""
-        best = C.c_int()
-        ms = np.zeros(TUNE_NLEN)
-        _check(load_library().chq_autotune(self._h, C.byref(best), _dptr(ms)))
-        return {"seglen": best.value, "ms": {L: float(t) for L, t in zip(TUNE_LENGTHS, ms)}}
+        """Pick the y/z march length and the x-sweep variant of the flux kernel by timing it on
+        this mesh's state (call after prime). Returns {"seglen": best length, "ms": {length: ms
+        per launch}, "xvar": best variant, "xvar_ms": {variant: ms per launch}}."""
+        best, bx = C.c_int(), C.c_int()
+        ms, msx = np.zeros(TUNE_NLEN), np.zeros(TUNE_NXVAR)
+        _check(load_library().chq_autotune2(self._h, C.byref(best), C.byref(bx), _dptr(ms), _dptr(msx)))
+        return {"seglen": best.value, "ms": {L: float(t) for L, t in zip(TUNE_LENGTHS, ms)},
+                "xvar": bx.value, "xvar_ms": {v: float(t) for v, t in enumerate(msx)}}
+
+    @property
+    def xvariant(self) -> int:
+        return int(load_library().chq_get_xvariant(self._h))
+
+    @xvariant.setter
+    def xvariant(self, v: int) -> None:
+        _check(load_library().chq_set_xvariant(self._h, int(v)))
 
     @property
     def seglen(self) -> int:
@@ -433,9 +449,10 @@ class Server:
     """Continuous-batching simulation server (chq_server_*)."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 1024, cycles_per_step: int = 4, lanes: int = 8,
-                 solo_cells: int = None):
+                 solo_cells: int = None, autotune: bool = True):
         h = _P()
         _check(load_library().chq_server_create(int(hbm_budget_bytes), max_active, cycles_per_step, C.byref(h)))
+        _check(load_library().chq_server_set_autotune(h, int(bool(autotune))))
         self._h = h
         _check(load_library().chq_server_set_lanes(h, int(lanes)))
         if solo_cells is not None:
@@ -507,6 +524,15 @@ class Batch:
 
     def kernel_launches(self) -> int:
         return int(load_library().chq_batch_kernel_launches(self._h))
+
+    def autotune(self) -> dict:
+        """The batch's march length and x-sweep variant, timed on the batched flux launch over
+        all members (cached per scheme, precision and size class)."""
+        best, bx = C.c_int(), C.c_int()
+        ms, msx = np.zeros(TUNE_NLEN), np.zeros(TUNE_NXVAR)
+        _check(load_library().chq_batch_autotune(self._h, C.byref(best), C.byref(bx), _dptr(ms), _dptr(msx)))
+        return {"seglen": best.value, "ms": {L: float(t) for L, t in zip(TUNE_LENGTHS, ms)},
+                "xvar": bx.value, "xvar_ms": {v: float(t) for v, t in enumerate(msx)}}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -46,6 +46,7 @@ template <class P> struct FluxArgs {
   long nwarp[3];       // warps per direction
   int nseg[3];         // segments along the sweep (x: XFaces-face segments)
   int nchunk;          // 32-wide i chunks for y/z sweeps (aligned to i = 0)
+  int xvar;            // x-sweep kernel variant (register cap, FluxMinBlocks); picked by the autotuner
   const int *skip;     // optional device flag: nonzero -> kernel returns immediately
 };
 
@@ -557,16 +558,20 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   }
 }
 
-// Resident 128-thread blocks per SM the flux kernel is compiled for (register cap). The
-// kernel is bound by FP64 / FP32 instruction latency, so more resident warps pay even with
-// some spilling to L1: measured best at 5 (FP64, 96 registers) and 10 (FP32, 48 registers).
+// Resident 128-thread blocks per SM the x-sweep kernel is compiled for (register cap), in two
+// variants that the autotuner chooses between per scheme, precision and mesh: V = 0 at 5
+// (FP64, 96 registers) / 10 (FP32, 48 registers) blocks, V = 1 at 6 / 12 blocks (more
+// resident warps to hide the FP64 / FP32 latency, fewer registers, some spilling to L1).
 #ifndef CHQ_FLUX_MINB_D
 #define CHQ_FLUX_MINB_D 5
 #endif
 #ifndef CHQ_FLUX_MINB_F
 #define CHQ_FLUX_MINB_F 10
 #endif
-template <class P> struct FluxMinBlocks { static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUX_MINB_D : CHQ_FLUX_MINB_F; };
+template <class P, int V = 0> struct FluxMinBlocks {
+  static constexpr int v = (sizeof(P) == 8) ? CHQ_FLUX_MINB_D + V : CHQ_FLUX_MINB_F + 2 * V;
+};
+constexpr int kFluxXVariants = 2;
 
 // Single-mesh launches split by sweep: the x-sweep kernel needs no shared window, so it keeps
 // the full L1 and the register cap above; the y/z kernel holds 8 + 8(2RE+1) shared columns
@@ -586,8 +591,8 @@ template <int R, class P> __host__ __device__ constexpr size_t flux_yz_smem() {
          kYzThreads * sizeof(P);
 }
 
-template <int R, int S, bool CHAR, class P>
-__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_x_kernel(const FluxArgs<P> A) {
+template <int R, int S, bool CHAR, class P, int V = 0>
+__global__ void __launch_bounds__(128, (FluxMinBlocks<P, V>::v)) flux_x_kernel(const FluxArgs<P> A) {
   if (A.skip && *A.skip) return;
   const int wid = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
   if (wid < (int)A.nwarp[0]) {
@@ -610,8 +615,8 @@ __global__ void __launch_bounds__(kYzThreads, FluxYzMinBlocks<P>::v) flux_yz_ker
 
 // batched forms: the blocks of many meshes in one launch per sweep kind (chq_batch); each
 // block copies its mesh's arguments to shared memory first
-template <int R, int S, bool CHAR, class P>
-__global__ void __launch_bounds__(128, FluxMinBlocks<P>::v) flux_x_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
+template <int R, int S, bool CHAR, class P, int V = 0>
+__global__ void __launch_bounds__(128, (FluxMinBlocks<P, V>::v)) flux_x_batched(const FluxArgs<P> *args, const BatchSlot *slots, int n) {
   __shared__ __align__(16) unsigned char sa[sizeof(FluxArgs<P>)];
   const int j = batch_job(slots, n, blockIdx.x);
   const FluxArgs<P> &A = stage_args(args, j, sa);

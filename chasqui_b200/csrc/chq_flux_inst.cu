@@ -38,7 +38,10 @@ static cudaError_t go(const FluxArgs<CHQ_P> &a, unsigned, cudaStream_t s) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  if (nx) flux_x_kernel<CHQ_R, S, C, CHQ_P><<<nx, 128, 0, s>>>(a);
+  if (nx) {
+    if (a.xvar) flux_x_kernel<CHQ_R, S, C, CHQ_P, 1><<<nx, 128, 0, s>>>(a);
+    else flux_x_kernel<CHQ_R, S, C, CHQ_P, 0><<<nx, 128, 0, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
@@ -57,7 +60,7 @@ cudaError_t launch_flux<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> &a, int rsolver, int
 
 template <int S, bool C>
 static cudaError_t gob(const FluxArgs<CHQ_P> *a, const BatchSlot *sx, const BatchSlot *syz, int n, unsigned nbx,
-                       unsigned nbyz, cudaStream_t s) {
+                       unsigned nbyz, int xvar, cudaStream_t s) {
   if (nbyz) {
     constexpr size_t smem = flux_yz_batched_smem<CHQ_R, CHQ_P>();
     static bool ready[64] = {};
@@ -67,19 +70,23 @@ static cudaError_t gob(const FluxArgs<CHQ_P> *a, const BatchSlot *sx, const Batc
     const cudaError_t e2 = cudaGetLastError();
     if (e2 != cudaSuccess) return e2;
   }
-  if (nbx) flux_x_batched<CHQ_R, S, C, CHQ_P><<<nbx, 128, 0, s>>>(a, sx, n);
+  if (nbx) {
+    if (xvar) flux_x_batched<CHQ_R, S, C, CHQ_P, 1><<<nbx, 128, 0, s>>>(a, sx, n);
+    else flux_x_batched<CHQ_R, S, C, CHQ_P, 0><<<nbx, 128, 0, s>>>(a, sx, n);
+  }
   return cudaGetLastError();
 }
 
 template <>
 cudaError_t launch_flux_batched<CHQ_P, CHQ_R>(const FluxArgs<CHQ_P> *a, const BatchSlot *sx, const BatchSlot *syz, int n,
-                                               int rsolver, int charac, unsigned nbx, unsigned nbyz, cudaStream_t s) {
+                                               int rsolver, int charac, unsigned nbx, unsigned nbyz, int xvar,
+                                               cudaStream_t s) {
   if (nbx == 0 && nbyz == 0) return cudaSuccess;
   const bool c = (charac != 0) && (CHQ_R != R_DC);
   switch (rsolver) {
-    case S_HLLE: return c ? gob<S_HLLE, true>(a, sx, syz, n, nbx, nbyz, s) : gob<S_HLLE, false>(a, sx, syz, n, nbx, nbyz, s);
-    case S_HLLD: return c ? gob<S_HLLD, true>(a, sx, syz, n, nbx, nbyz, s) : gob<S_HLLD, false>(a, sx, syz, n, nbx, nbyz, s);
-    case S_LHLLD: return c ? gob<S_LHLLD, true>(a, sx, syz, n, nbx, nbyz, s) : gob<S_LHLLD, false>(a, sx, syz, n, nbx, nbyz, s);
+    case S_HLLE: return c ? gob<S_HLLE, true>(a, sx, syz, n, nbx, nbyz, xvar, s) : gob<S_HLLE, false>(a, sx, syz, n, nbx, nbyz, xvar, s);
+    case S_HLLD: return c ? gob<S_HLLD, true>(a, sx, syz, n, nbx, nbyz, xvar, s) : gob<S_HLLD, false>(a, sx, syz, n, nbx, nbyz, xvar, s);
+    case S_LHLLD: return c ? gob<S_LHLLD, true>(a, sx, syz, n, nbx, nbyz, xvar, s) : gob<S_LHLLD, false>(a, sx, syz, n, nbx, nbyz, xvar, s);
     default: return cudaErrorInvalidValue;
   }
 }

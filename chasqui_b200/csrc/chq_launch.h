@@ -12,7 +12,8 @@ cudaError_t launch_flux(const FluxArgs<P> &a, int rsolver, int charac, unsigned 
 // x-sweep blocks and y/z-sweep blocks of many meshes, with one slot table each
 template <class P, int R>
 cudaError_t launch_flux_batched(const FluxArgs<P> *args, const BatchSlot *slots_x, const BatchSlot *slots_yz, int njobs,
-                                int rsolver, int charac, unsigned nblocks_x, unsigned nblocks_yz, cudaStream_t s);
+                                int rsolver, int charac, unsigned nblocks_x, unsigned nblocks_yz, int xvar,
+                                cudaStream_t s);
 
 // registers per thread of the instantiated y/z kernel (for the launch report)
 template <class P, int R>

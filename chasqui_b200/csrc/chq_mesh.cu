@@ -201,6 +201,7 @@ struct chq_mesh {
   int lo[3][3], hi[3][3], active[3];
   int act_lo[3][3], act_hi[3][3];
   int seglen;
+  int xvar = 0;   // x-sweep kernel variant (register cap), chq_autotune
   // RKL2 work arrays (cfg.sts only): Y0..Y2, M0, Mj on cells; their face-field twins
   double *sy[3] = {}, *sm0 = nullptr, *smj = nullptr;
   double *sb[3][3] = {}, *smb0[3] = {}, *smbj[3] = {};
@@ -344,6 +345,7 @@ FluxArgs<P> flux_args(chq_mesh *m, int cur, unsigned dirmask) {
   a.low_mach = m->cfg.low_mach;
   a.lhlld_phi = m->cfg.lhlld_phi;
   a.seglen = m->seglen;
+  a.xvar = m->xvar;
   a.nchunk = (m->g.ni + 1 + 31) / 32;
   // x: rows x segments of XFaces faces (29 for streaming PPM, else 31); y/z: i chunks x
   // outer x segments
@@ -1269,6 +1271,7 @@ int transfer(chq_mesh *m, const char *name, double *host, long n, bool up, cudaS
 struct chq_batch {
   std::vector<chq_mesh *> jobs;
   int mixed = 0, recon = 0, rsolver = 0, charac = 0, nstage = 0, fofc = 0, limiter = 0;
+  int xvar = 0;   // x-sweep kernel variant of the batched flux launch (chq_batch_autotune)
   cudaStream_t stream = nullptr;
   char *dev = nullptr;
   struct Kind {
@@ -1642,11 +1645,11 @@ cudaError_t batch_flux(const chq_batch *B, const FluxArgs<P> *args, cudaStream_t
   const unsigned nbx = (unsigned)B->k_flux.nblocks, nbyz = (unsigned)B->k_flux_yz.nblocks;
   const BatchSlot *sx = B->k_flux.slots, *syz = B->k_flux_yz.slots;
   switch (B->recon) {
-    case R_DC: return launch_flux_batched<P, R_DC>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
-    case R_PLM: return launch_flux_batched<P, R_PLM>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
-    case R_PPM: return launch_flux_batched<P, R_PPM>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
-    case R_PPMX: return launch_flux_batched<P, R_PPMX>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
-    case R_WENOZ: return launch_flux_batched<P, R_WENOZ>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, s);
+    case R_DC: return launch_flux_batched<P, R_DC>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, B->xvar, s);
+    case R_PLM: return launch_flux_batched<P, R_PLM>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, B->xvar, s);
+    case R_PPM: return launch_flux_batched<P, R_PPM>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, B->xvar, s);
+    case R_PPMX: return launch_flux_batched<P, R_PPMX>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, B->xvar, s);
+    case R_WENOZ: return launch_flux_batched<P, R_WENOZ>(args, sx, syz, n, B->rsolver, B->charac, nbx, nbyz, B->xvar, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -2893,6 +2896,21 @@ int chq_event_elapsed(chq_mesh *m, int a, int b, float *ms) {
 bool grav_on(const chq_mesh *m) { return m->cfg.gravity_uniform || m->cfg.gravity_point; }
 bool sts_on(const chq_mesh *m) { return m->diff && m->cfg.sts; }
 
+// Argument tables from the members' current settings, the batch's stream and its completion
+// event (members wait on it before work on their own streams).
+static int batch_setup(chq_batch *B) {
+  int rc = B->mixed ? batch_build<float>(B) : batch_build<double>(B);
+  if (rc == CHQ_OK) {
+    cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->done_evt, cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = cuda_fail(e, "batch stream");
+  }
+  if (rc != CHQ_OK) return rc;
+  // an event that has never been recorded counts as complete, so members can wait on it now
+  for (chq_mesh *m : B->jobs) m->batch_evt = B->done_evt;
+  return CHQ_OK;
+}
+
 int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   if (!meshes || n < 1 || !out) return fail(CHQ_ERR_ARG, "bad argument");
   *out = nullptr;
@@ -2925,19 +2943,12 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   B->cool = a->cfg.cooling ? 1 : 0;
   B->grav = grav_on(a) ? 1 : 0;
   B->sts = sts_on(a) ? 1 : 0;
-  int rc = B->mixed ? batch_build<float>(B) : batch_build<double>(B);
-  if (rc == CHQ_OK) {
-    cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->done_evt, cudaEventDisableTiming);
-    if (e != cudaSuccess) rc = cuda_fail(e, "batch stream");
-  }
+  const int rc = batch_setup(B);
   if (rc != CHQ_OK) {
     batch_free(B);
     delete B;
     return rc;
   }
-  // an event that has never been recorded counts as complete, so members can wait on it now
-  for (chq_mesh *m : B->jobs) m->batch_evt = B->done_evt;
   *out = B;
   return CHQ_OK;
 }
@@ -3023,67 +3034,227 @@ int chq_set_seglen(chq_mesh *m, int seglen) {
 
 int chq_get_seglen(const chq_mesh *m) { return m ? m->seglen : 0; }
 
-int chq_autotune(chq_mesh *m, int *seglen, double ms[CHQ_TUNE_NLEN]) {
-  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
-  drop_cycle_graph(m);   // the captured cycle holds the old march length
-  static std::mutex mu;
-  static std::map<std::vector<int>, int> cache;
-  const std::vector<int> key = {m->mixed, m->cfg.recon, m->cfg.rsolver, m->cfg.characteristic,
-                                m->g.nx1, m->g.nx2, m->g.nx3};
+int chq_set_xvariant(chq_mesh *m, int xvar) {
+  if (!m || xvar < 0 || xvar >= CHQ_TUNE_NXVAR) return fail(CHQ_ERR_ARG, "x-sweep variant out of range");
+  if (xvar != m->xvar) drop_cycle_graph(m);
+  m->xvar = xvar;
+  return CHQ_OK;
+}
+
+int chq_get_xvariant(const chq_mesh *m) { return m ? m->xvar : -1; }
+
+}  // extern "C"
+
+namespace {
+
+// Device time of `reps` launches of `launch` after one warm-up launch, on stream s.
+template <class F>
+int time_launches(cudaStream_t s, int reps, F launch, double *ms) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CHQ_CUDA(cudaEventCreate(&e0));
+  cudaError_t e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(e, "autotune timing");
+  }
+  int rc = launch();
+  if (rc == CHQ_OK) e = cudaEventRecord(e0, s);
+  for (int r = 0; r < reps && rc == CHQ_OK && e == cudaSuccess; ++r) rc = launch();
+  if (rc == CHQ_OK && e == cudaSuccess) e = cudaEventRecord(e1, s);
+  float t = 0.f;
+  if (rc == CHQ_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
+  if (rc == CHQ_OK && e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != CHQ_OK) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "autotune timing");
+  *ms = t / reps;
+  return CHQ_OK;
+}
+
+// Two-knob search shared by meshes and batches: the y/z march length over CHQ_TUNE_LENGTHS
+// (x-sweep variant 0), then the x-sweep variants at the best length (the knobs act on
+// different kernels). set(len, xvar) applies a candidate, run(&ms) times the flux launch.
+template <class Set, class Run>
+int tune_two_knobs(Set set, Run run, int nxvar, int *best_len, int *best_xvar, double ms_len[CHQ_TUNE_NLEN],
+                   double ms_xvar[CHQ_TUNE_NXVAR]) {
   const int cand[CHQ_TUNE_NLEN] = CHQ_TUNE_LENGTHS;
+  double best = 1e300;
+  *best_len = cand[0];
+  *best_xvar = 0;
+  for (int q = 0; q < CHQ_TUNE_NLEN; ++q) {
+    double t = 0.0;
+    int rc = set(cand[q], 0);
+    if (rc == CHQ_OK) rc = run(&t);
+    if (rc != CHQ_OK) return rc;
+    if (ms_len) ms_len[q] = t;
+    if (t < best) {
+      best = t;
+      *best_len = cand[q];
+    }
+  }
+  if (ms_xvar) {
+    ms_xvar[0] = best;
+    for (int v = nxvar; v < CHQ_TUNE_NXVAR; ++v) ms_xvar[v] = -1.0;
+  }
+  for (int v = 1; v < nxvar; ++v) {
+    double t = 0.0;
+    int rc = set(*best_len, v);
+    if (rc == CHQ_OK) rc = run(&t);
+    if (rc != CHQ_OK) return rc;
+    if (ms_xvar) ms_xvar[v] = t;
+    if (t < best) {
+      best = t;
+      *best_xvar = v;
+    }
+  }
+  return set(*best_len, *best_xvar);
+}
+
+std::mutex g_tune_mu;
+std::map<std::vector<long>, std::pair<int, int>> g_tune_cache;   // key -> (march length, x variant)
+
+// x-sweep variants the tuner may pick. The FP64 form is compiled without multiply-add
+// contraction, so both builds compute bit for bit the same fluxes; in the mixed form the
+// compiler may contract the FP32 arithmetic differently in the two builds, which would make a
+// job's rounding depend on the tuning (and a server job differ from the same job run alone),
+// so the mixed form keeps variant 0.
+int tune_xvariants(int mixed) { return mixed ? 1 : CHQ_TUNE_NXVAR; }
+
+// batches of this many cells or more keep their members' launch settings untimed
+constexpr long kBatchTuneMaxCells = 1L << 23;
+
+}  // namespace
+
+extern "C" {
+
+int chq_autotune2(chq_mesh *m, int *seglen, int *xvar, double ms_len[CHQ_TUNE_NLEN],
+                  double ms_xvar[CHQ_TUNE_NXVAR]) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  drop_cycle_graph(m);   // the captured cycle holds the old settings
+  // per process: scheme, precision and mesh shape
+  const std::vector<long> key = {0, m->mixed, m->cfg.recon, m->cfg.rsolver, m->cfg.characteristic,
+                                 m->g.nx1, m->g.nx2, m->g.nx3};
   {
-    std::lock_guard<std::mutex> lk(mu);
-    const auto it = cache.find(key);
-    if (it != cache.end()) {
-      m->seglen = it->second;
-      if (seglen) *seglen = it->second;
-      if (ms)
-        for (int q = 0; q < CHQ_TUNE_NLEN; ++q) ms[q] = -1.0;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      m->seglen = it->second.first;
+      m->xvar = it->second.second;
+      if (seglen) *seglen = m->seglen;
+      if (xvar) *xvar = m->xvar;
+      if (ms_len)
+        for (int q = 0; q < CHQ_TUNE_NLEN; ++q) ms_len[q] = -1.0;
+      if (ms_xvar)
+        for (int q = 0; q < CHQ_TUNE_NXVAR; ++q) ms_xvar[q] = -1.0;
       return CHQ_OK;
     }
   }
   cudaStream_t s = S(m, nullptr);
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  CHQ_CUDA(cudaEventCreate(&e0));
-  CHQ_CUDA(cudaEventCreate(&e1));
-  const int keep = m->seglen;
-  int best = keep;
-  double best_ms = 1e300;
-  int rc = CHQ_OK;
-  for (int q = 0; q < CHQ_TUNE_NLEN && rc == CHQ_OK; ++q) {
-    m->seglen = cand[q];
-    const int reps = 3;
-    rc = do_fluxes(m, 0, 7u, nullptr, s);   // warm-up (fluxes are scratch: the state is unchanged)
-    if (rc == CHQ_OK) cudaEventRecord(e0, s);
-    for (int r = 0; r < reps && rc == CHQ_OK; ++r) rc = do_fluxes(m, 0, 7u, nullptr, s);
-    if (rc != CHQ_OK) break;
-    cudaEventRecord(e1, s);
-    float t = 0.f;
-    cudaError_t err = cudaEventSynchronize(e1);
-    if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
-    if (err != cudaSuccess) {
-      rc = cuda_fail(err, "autotune timing");
-      break;
-    }
-    const double per = t / reps;
-    if (ms) ms[q] = per;
-    if (per < best_ms) {
-      best_ms = per;
-      best = cand[q];
-    }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  const int keep_len = m->seglen, keep_x = m->xvar;
+  int bl = keep_len, bx = keep_x;
+  // fluxes are scratch: timing them leaves the state unchanged
+  const int rc = tune_two_knobs(
+      [&](int len, int v) {
+        m->seglen = len;
+        m->xvar = v;
+        return CHQ_OK;
+      },
+      [&](double *t) { return time_launches(s, 3, [&] { return do_fluxes(m, 0, 7u, nullptr, s); }, t); },
+      tune_xvariants(m->mixed), &bl, &bx, ms_len, ms_xvar);
   if (rc != CHQ_OK) {
-    m->seglen = keep;
+    m->seglen = keep_len;
+    m->xvar = keep_x;
     return rc;
   }
-  m->seglen = best;
   {
-    std::lock_guard<std::mutex> lk(mu);
-    cache[key] = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = {bl, bx};
   }
-  if (seglen) *seglen = best;
+  if (seglen) *seglen = bl;
+  if (xvar) *xvar = bx;
+  return CHQ_OK;
+}
+
+int chq_autotune(chq_mesh *m, int *seglen, double ms[CHQ_TUNE_NLEN]) {
+  return chq_autotune2(m, seglen, nullptr, ms, nullptr);
+}
+
+int chq_batch_autotune(chq_batch *B, int *seglen, int *xvar, double ms_len[CHQ_TUNE_NLEN],
+                       double ms_xvar[CHQ_TUNE_NXVAR]) {
+  if (!B || B->jobs.empty()) return fail(CHQ_ERR_ARG, "null or empty batch");
+  // per process: scheme, precision, and the batch's size class (log2 of its cells and of its
+  // member count), so that lanes of similar load share one measurement
+  long cells = 0;
+  for (const chq_mesh *m : B->jobs) cells += (long)m->g.nx1 * m->g.nx2 * m->g.nx3;
+  const auto lg = [](long v) {
+    int b = 0;
+    while (v > 1) { v >>= 1; ++b; }
+    return (long)b;
+  };
+  const std::vector<long> key = {1, B->mixed, B->recon, B->rsolver, B->charac, lg(cells), lg((long)B->jobs.size())};
+  int bl = B->jobs[0]->seglen, bx = B->xvar;
+  bool cached = false;
+  if (cells >= kBatchTuneMaxCells) {
+    // the members' own settings already fill the device: no timing (it would cost more than
+    // it could gain over a short run); report them
+    if (ms_len)
+      for (int q = 0; q < CHQ_TUNE_NLEN; ++q) ms_len[q] = -1.0;
+    if (ms_xvar)
+      for (int q = 0; q < CHQ_TUNE_NXVAR; ++q) ms_xvar[q] = -1.0;
+    if (seglen) *seglen = bl;
+    if (xvar) *xvar = bx;
+    return CHQ_OK;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      bl = it->second.first;
+      bx = it->second.second;
+      cached = true;
+    }
+  }
+  // a new march length changes the flux launch geometry: rebuild the tables for it
+  auto set = [&](int len, int v) -> int {
+    bool same = (B->xvar == v);
+    for (const chq_mesh *m : B->jobs) same = same && (m->seglen == len);
+    if (same && B->dev) return CHQ_OK;
+    batch_free(B);
+    for (chq_mesh *m : B->jobs) {
+      if (m->seglen != len) drop_cycle_graph(m);
+      m->seglen = len;
+      m->xvar = v;
+    }
+    B->xvar = v;
+    return batch_setup(B);
+  };
+  if (cached) {
+    if (ms_len)
+      for (int q = 0; q < CHQ_TUNE_NLEN; ++q) ms_len[q] = -1.0;
+    if (ms_xvar)
+      for (int q = 0; q < CHQ_TUNE_NXVAR; ++q) ms_xvar[q] = -1.0;
+  } else {
+    // members' own streams may still hold work (uploads, prime): order after them
+    for (chq_mesh *m : B->jobs) CHQ_CUDA(cudaStreamSynchronize(m->stream));
+    const int rc = tune_two_knobs(
+        set,
+        [&](double *t) {
+          return time_launches(B->stream, 3, [&]() -> int {
+            const cudaError_t e = B->mixed ? batch_flux<float>(B, (const FluxArgs<float> *)B->a_flux[0], B->stream)
+                                           : batch_flux<double>(B, (const FluxArgs<double> *)B->a_flux[0], B->stream);
+            return (e == cudaSuccess) ? CHQ_OK : cuda_fail(e, "batched flux launch");
+          }, t);
+        },
+        tune_xvariants(B->mixed), &bl, &bx, ms_len, ms_xvar);
+    if (rc != CHQ_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = {bl, bx};
+  }
+  const int rc = set(bl, bx);
+  if (rc != CHQ_OK) return rc;
+  if (seglen) *seglen = bl;
+  if (xvar) *xvar = bx;
   return CHQ_OK;
 }
 

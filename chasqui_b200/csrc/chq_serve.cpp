@@ -106,6 +106,7 @@ struct chq_server {
   long long budget = 0, used = 0;
   int max_active = 0, cycles_per_step = 1, lanes = 8;
   long long solo_cells = 0;   // jobs of at least this many cells run unbatched
+  int autotune = 1;           // tune each new lane's batch (chq_batch_autotune)
   long long next_id = 1;
   std::map<long long, Job *> jobs;
   std::vector<Job *> queue;
@@ -318,8 +319,12 @@ int rebuild(chq_server *S) {
     if (g.members.empty()) continue;
     std::vector<chq_mesh *> ms;
     for (Job *j : g.members) ms.push_back(j->mesh);
-    const int rc = chq_batch_create(ms.data(), (int)ms.size(), &g.batch);
+    int rc = chq_batch_create(ms.data(), (int)ms.size(), &g.batch);
     if (rc) return rc;
+    if (S->autotune) {
+      rc = chq_batch_autotune(g.batch, nullptr, nullptr, nullptr, nullptr);
+      if (rc) return rc;
+    }
     chq_batch_set_graph(g.batch, 1);
   }
   return CHQ_OK;
@@ -443,6 +448,12 @@ int chq_server_set_solo_cells(chq_server *S, long long cells) {
   // at 2^15 cells ended in a device fault whose cause is not known
   if (cells < kSoloCells) return err(CHQ_ERR_ARG, "the solo threshold must be at least 2^21 cells");
   S->solo_cells = cells;
+  return CHQ_OK;
+}
+
+int chq_server_set_autotune(chq_server *S, int enable) {
+  if (!S) return err(CHQ_ERR_ARG, "null server");
+  S->autotune = (enable != 0);
   return CHQ_OK;
 }
 

@@ -217,20 +217,37 @@ CHQ_API int chq_profile(chq_mesh *m, int enable);
 
 /* ---- flux-kernel autotuning (no reference counterpart: the reference has one fixed
  * Kokkos range policy) ---------------------------------------------------------------------
- * March length = faces each thread of the y/z sweeps carries its cell states across. The
- * default is the longest of 16, 8, 4 that keeps a full device of y/z threads busy (16 from
- * about 128^3 up, 4 for small meshes). chq_autotune times the flux kernel of this mesh's scheme on its current
- * state (call it after chq_prime) for every candidate in CHQ_TUNE_LENGTHS, keeps the fastest
- * on the mesh, and returns it with the per-candidate ms per launch (ms may be NULL). The
- * choice is cached for the process per (precision, reconstruction, Riemann solver,
- * characteristic flag, nx1, nx2, nx3); a later mesh with the same key takes it without
- * timing (ms then holds -1). Synchronises the mesh stream. Results are bitwise independent
- * of the length. */
+ * Two knobs of the face-flux launch, neither of which changes any result bit:
+ *  - march length = faces each thread of the y/z sweeps carries its cell states across
+ *    (CHQ_TUNE_LENGTHS). The default is the longest of 16, 8, 4 that keeps a full device of
+ *    y/z threads busy (16 from about 128^3 up, 4 for small meshes);
+ *  - x-sweep variant = the register cap the x-sweep kernel is compiled for (0: 5 resident
+ *    128-thread blocks per SM in FP64 / 10 in FP32; 1: 6 / 12, more resident warps, fewer
+ *    registers). Default 0. The tuner varies it in the FP64 form only: there both builds
+ *    compute the same bits, while in the mixed form the compiler may contract the FP32
+ *    arithmetic of the two builds differently (chq_set_xvariant still selects it there).
+ * chq_autotune2 times the flux launch of this mesh's scheme on its current state (call it
+ * after chq_prime): every march length with variant 0, then every variant at the best length;
+ * it keeps the fastest pair on the mesh and returns it with the ms per launch of each
+ * candidate (the arrays may be NULL). The choice is cached for the process per (precision,
+ * reconstruction, Riemann solver, characteristic flag, nx1, nx2, nx3); a later mesh with the
+ * same key takes it without timing (the arrays then hold -1). Synchronises the mesh stream.
+ * chq_autotune is the same search reporting the march length only.
+ * chq_batch_autotune does the same for a batch: it times the batched flux launch over all its
+ * members (their march lengths and the batch's x variant change together; the batch's tables
+ * are rebuilt for each candidate) and caches per (precision, scheme, log2 of the batch's
+ * cells, log2 of its member count); a batch of 2^23 cells or more fills the device with its
+ * members' own settings and is returned untimed (the arrays hold -1). */
 #define CHQ_TUNE_NLEN 5
 #define CHQ_TUNE_LENGTHS {4, 8, 16, 32, 64}
+#define CHQ_TUNE_NXVAR 2
 CHQ_API int chq_autotune(chq_mesh *m, int *seglen, double ms[CHQ_TUNE_NLEN]);
+CHQ_API int chq_autotune2(chq_mesh *m, int *seglen, int *xvar, double ms_len[CHQ_TUNE_NLEN],
+                          double ms_xvar[CHQ_TUNE_NXVAR]);
 CHQ_API int chq_set_seglen(chq_mesh *m, int seglen);
 CHQ_API int chq_get_seglen(const chq_mesh *m);
+CHQ_API int chq_set_xvariant(chq_mesh *m, int xvar);
+CHQ_API int chq_get_xvariant(const chq_mesh *m);
 /* Synchronises; totals in ms and launch counts per kind since the last reset. */
 CHQ_API int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launches[CHQ_NPROF], int reset);
 
@@ -257,6 +274,9 @@ CHQ_API int chq_batch_cycles(chq_batch *b, int n, void *stream);
 CHQ_API int chq_batch_set_graph(chq_batch *b, int enable);
 /* Synchronises; per member time, cycle count and done flag (arrays of length n, any NULL). */
 CHQ_API int chq_batch_status(chq_batch *b, double *t, int *cycle, int *done);
+/* see "flux-kernel autotuning" above; call after the members are primed */
+CHQ_API int chq_batch_autotune(chq_batch *b, int *seglen, int *xvar, double ms_len[CHQ_TUNE_NLEN],
+                               double ms_xvar[CHQ_TUNE_NXVAR]);
 CHQ_API long long chq_batch_kernel_launches(const chq_batch *b);
 /* the batch's own stream (cudaStream_t) */
 CHQ_API void *chq_batch_stream(chq_batch *b);
@@ -298,6 +318,9 @@ CHQ_API int chq_server_set_lanes(chq_server *s, int lanes);
 /* jobs of at least `cells` cells run unbatched on their own streams (default and minimum
  * 2^21; smaller values return CHQ_ERR_ARG); takes effect for newly admitted jobs */
 CHQ_API int chq_server_set_solo_cells(chq_server *s, long long cells);
+/* tune every new lane's batch with chq_batch_autotune (1, the default) or keep the members'
+ * default launch settings (0); takes effect for batches built afterwards */
+CHQ_API int chq_server_set_autotune(chq_server *s, int enable);
 
 /* ---- history sums without any device allocation --------------------------------------------
  * No counterpart in the reference. For callers that cannot allocate device memory: an
