@@ -160,7 +160,10 @@ template <class P> struct UpdateArgs {
   const double *beta_dt_dev; // device beta*dt of this stage (StepCtl::beta_dt[s])
   double idx1, idx2, idx3;
   const int *done;
-  const int *need;           // run only when *need != 0 (FOFC re-run); null = always
+  const int *need;           // run only when *need > need_min (FOFC re-run); null = always
+  int need_min;
+  const int *list;           // flagged cells of the stage (update_rerun_listed_kernel)
+  int cap;                   // list capacity
 };
 
 // new face fields; curl of the edge EMFs (src/physics.hpp:327-347)
@@ -186,16 +189,10 @@ template <class P> CHQ_D double new_b3(const UpdateArgs<P> &A, long l, double g0
 
 // GRAV: compile the gravity epilogue (a separate instantiation keeps the plain update's
 // register count, and with it its occupancy, unchanged)
-template <class P, bool GRAV = false> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by, int bz) {
-  if (A.done && *A.done) return;
-  if (A.need && *A.need == 0) return;
+// The update of one point (k, j, i) of the face/edge frame, is <= i <= ie+1 (and so on).
+template <class P, bool GRAV = false> CHQ_D void update_point(const UpdateArgs<P> &A, int k, int j, int i, double bdt) {
   const Geom &g = A.g;
-  const int i = g.is + bx * blockDim.x + threadIdx.x;
-  const int j = g.js + by * blockDim.y + threadIdx.y;
-  const int k = g.ks + bz;
-  if (i > g.ie + 1 || j > g.je + 1 || k > g.ke + 1) return;
   const double g0 = A.g0, g1 = A.g1;
-  const double bdt = A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt;
   const long l = g.idx(k, j, i);
   const long vs = g.vstride;
   const bool cell = (i <= g.ie && j <= g.je && k <= g.ke);
@@ -216,7 +213,7 @@ template <class P, bool GRAV = false> CHQ_D void update_body(const UpdateArgs<P>
       if (gr.point) {
         const double dx = (g.x1min + (i - g.is + 0.5) * g.dx1) - gr.x0;
         const double dy = g.two_d ? (g.x2min + (j - g.js + 0.5) * g.dx2) - gr.y0 : 0.0;
-        const double dz = g.three_d ? (g.x3min + (k - g.ks + 0.5) * g.dx3) - gr.z0 : 0.0;
+        const double dz = g.three_d ? (g.x3min + (k - g.ks + g.koff + 0.5) * g.dx3) - gr.z0 : 0.0;
         const double r2 = dx * dx + dy * dy + dz * dz + gr.rsoft * gr.rsoft;
         const double f = -gr.gm / (r2 * sqrt(r2));
         a1 += f * dx;
@@ -249,8 +246,55 @@ template <class P, bool GRAV = false> CHQ_D void update_body(const UpdateArgs<P>
   }
 }
 
+template <class P, bool GRAV = false> CHQ_D void update_body(const UpdateArgs<P> &A, int bx, int by, int bz) {
+  if (A.done && *A.done) return;
+  if (A.need && *A.need <= A.need_min) return;
+  const Geom &g = A.g;
+  const int i = g.is + bx * blockDim.x + threadIdx.x;
+  const int j = g.js + by * blockDim.y + threadIdx.y;
+  const int k = g.ks + bz;
+  if (i > g.ie + 1 || j > g.je + 1 || k > g.ke + 1) return;
+  update_point<P, GRAV>(A, k, j, i, A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt);
+}
+
 template <class P, bool GRAV> __global__ void __launch_bounds__(256) update_kernel(const UpdateArgs<P> A) {
   update_body<P, GRAV>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// FOFC re-run of the update in a stage whose b-weight is zero and whose output is the
+// b-state (the first stage of RK2, RK3 and SSPRK(4,3): out = u1 = ub, g1 = 0; src/main.cpp:68-91
+// re-runs Update over every cell). There the re-run computes g0 ua + 0 ub - bdt div with ub
+// the first pass's output: 0 ub is a zero, and the sum equals the first pass's value wherever
+// the divergence and the curl are unchanged (a zero's sign can only matter when ua is -0, and
+// then the first pass's output carries the sign the re-run reproduces). Only points whose
+// fluxes or edge EMFs were repaired change: the listed cells and their face neighbours, and
+// the faces next to the listed cells' edges, all inside the 3x3x3 points around each listed
+// cell. A point shared by two listed cells is recomputed twice with equal results. A cell
+// whose first-pass state was not finite keeps it (the full re-run would give NaN there too,
+// or for an infinite state NaN instead of the infinity). Without a usable list (count above
+// the capacity) this kernel does nothing and update_kernel with need_min = cap re-runs every
+// point.
+template <class P, bool GRAV> __global__ void __launch_bounds__(256) update_rerun_listed_kernel(const UpdateArgs<P> A) {
+  if (A.done && *A.done) return;
+  const int nb = *A.need;
+  if (nb <= 0 || nb > A.cap) return;
+  const Geom &g = A.g;
+  const double bdt = A.beta_dt_dev ? *A.beta_dt_dev : A.beta_dt;
+  const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
+  {
+    const int rj = g.two_d ? 3 : 1, rk = g.three_d ? 3 : 1, per = 3 * rj * rk;
+    const int sj = (int)g.sj, sk = (int)g.sk;
+    for (int it = tid; it < per * nb; it += nth) {
+      const int q = it / per, p = it - per * q;
+      const int c = A.list[q];
+      const int kc = c / sk, r = c - kc * sk, jc = r / sj, ic = r - jc * sj;
+      const int i = ic + p % 3 - 1;
+      const int j = jc + (p / 3) % rj - (rj >> 1);
+      const int k = kc + p / (3 * rj) - (rk >> 1);
+      if (i < g.is || i > g.ie + 1 || j < g.js || j > g.je + 1 || k < g.ks || k > g.ke + 1) continue;
+      update_point<P, GRAV>(A, k, j, i, bdt);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------------------

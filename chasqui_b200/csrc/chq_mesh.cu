@@ -489,6 +489,32 @@ int do_update(chq_mesh *m, int out, double g0, double g1, double bdt, const doub
   return CHQ_OK;
 }
 
+// FOFC re-run of the update (need = the device count of flagged cells). In a stage with
+// g1 = 0 whose output is the b-state only the points around the listed cells change
+// (update_rerun_listed_kernel); every other stage re-runs the whole update, as the reference.
+template <class P>
+int do_update_rerun(chq_mesh *m, int out, double g0, double g1, double bdt, const double *bdt_dev, const int *done,
+                    const int *need, cudaStream_t s) {
+  if (!(g1 == 0.0 && out == 1) || m->bad_cap <= 0) return do_update<P>(m, out, g0, g1, bdt, bdt_dev, done, need, s);
+  UpdateArgs<P> a = update_args<P>(m, out, g0, g1, bdt, bdt_dev, done, need);
+  a.list = m->bad_list;
+  a.cap = m->bad_cap;
+  const Geom &g = m->g;
+  const int per = 3 * (g.two_d ? 3 : 1) * (g.three_d ? 3 : 1);
+  const dim3 grid = repair_grid((long)per * m->bad_cap, kRepairBlocks).grid;
+  m->nlaunch += 2;
+  if (a.grav.on) update_rerun_listed_kernel<P, true><<<grid, 256, 0, s>>>(a);
+  else update_rerun_listed_kernel<P, false><<<grid, 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  // list overflow (count above the capacity): the whole update, as in the other stages
+  a.need_min = m->bad_cap;
+  const Launch3 L = update_grid(m);
+  if (a.grav.on) update_kernel<P, true><<<L.grid, L.block, 0, s>>>(a);
+  else update_kernel<P, false><<<L.grid, L.block, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
 FlagArgs flag_args(chq_mesh *m, int buf, int *nbad_dev, const int *done) {
   const Geom &g = m->g;
   FlagArgs a{};
@@ -908,7 +934,7 @@ int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, c
     else rc = DISPATCH_P(m, do_corner_rerun)(m, done, nbad, s);
     if (rc) return rc;
     if (dstage && (rc = DISPATCH_P(m, do_res_emf)(m, bc1, bc2, bc3, done, nbad, s))) return rc;
-    if ((rc = DISPATCH_P(m, do_update)(m, out, g0, g1, bdt, bdt_dev, done, nbad, s))) return rc;
+    if ((rc = DISPATCH_P(m, do_update_rerun)(m, out, g0, g1, bdt, bdt_dev, done, nbad, s))) return rc;
   }
   Prof p(m, PK_BC, s);
   return do_bc(m, out, done, s);
@@ -2943,6 +2969,7 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   B->cool = a->cfg.cooling ? 1 : 0;
   B->grav = grav_on(a) ? 1 : 0;
   B->sts = sts_on(a) ? 1 : 0;
+  B->xvar = a->xvar;   // the first member's x-sweep variant (chq_set_xvariant), as chq_batch_autotune sets it
   const int rc = batch_setup(B);
   if (rc != CHQ_OK) {
     batch_free(B);

@@ -166,6 +166,43 @@ CHQ_HD void side_dstar_flux(const MState<T> &S, T bn, T e, T pt, T s, T ds, T sm
   }
 }
 
+// Single-star (single) or double-star flux of the side `left` selects. The operands of the
+// two sides are picked value by value, then one evaluation runs with exactly the expression
+// sequence of side_star_flux / side_dstar_flux, so the result is bitwise the flux of that
+// side. The left side's double-star energy is E*_L - sqrt(D*_L) (v*_L.B*_L - v**.B**) sgn(bn),
+// the right side's E*_R + (the mirror term); x - t and x + (-t) are the same IEEE operation.
+template <bool LHLLD, class T>
+CHQ_HD void side_region_flux(bool left, bool single, const MState<T> &L, const MState<T> &R, T bn, T el, T er, T ptl,
+                             T ptr, T sl, T sr, T dls, T drs, T sm, T vls, T vrs, T wls, T wrs, T byls, T byrs, T bzls,
+                             T bzrs, T els, T ers, T pts, T sls, T srs, T sqdl, T sqdr, T vdotb_ls, T vdotb_rs, T sg,
+                             T vss, T wss, T byss, T bzss, T vdotb_ss, T f[NFLX]) {
+  const T ds = left ? dls : drs, vs = left ? vls : vrs, ws = left ? wls : wrs;
+  const T bys = left ? byls : byrs, bzs = left ? bzls : bzrs, es = left ? els : ers;
+  if constexpr (LHLLD) {
+    if (single) {
+      star_flux(ds, sm, vs, ws, es, bys, bzs, bn, pts, f);
+    } else {
+      const T t = (left ? sqdl : sqdr) * (((left ? vdotb_ls : vdotb_rs) - vdotb_ss) * sg);
+      const T ess = es + (left ? -t : t);
+      star_flux(ds, sm, vss, wss, ess, byss, bzss, bn, pts, f);
+    }
+  } else {
+    const MState<T> S{left ? L.d : R.d, left ? L.u : R.u, left ? L.v : R.v, left ? L.w : R.w,
+                      left ? L.p : R.p, left ? L.by : R.by, left ? L.bz : R.bz};
+    const T e = left ? el : er, pt = left ? ptl : ptr, s = left ? sl : sr;
+    side_star_flux<false>(S, bn, e, pt, s, ds, sm, vs, ws, bys, bzs, es, pts, f);
+    if (!single) {
+      const T t = (left ? sqdl : sqdr) * (((left ? vdotb_ls : vdotb_rs) - vdotb_ss) * sg);
+      const T ess = es + (left ? -t : t);
+      const T ss = left ? sls : srs;
+      const T us[NFLX] = {ds, ds * sm, ds * vs, ds * ws, es, bys, bzs};
+      const T uss[NFLX] = {ds, ds * sm, ds * vss, ds * wss, ess, byss, bzss};
+#pragma unroll
+      for (int n = 0; n < NFLX; ++n) f[n] = f[n] + ss * (uss[n] - us[n]);
+    }
+  }
+}
+
 template <bool LHLLD, class T>
 CHQ_HD void hlld(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T f[NFLX], T theta, T phi) {
   // speeds and the scalars of both sides first; flux vectors only for the selected region
@@ -222,53 +259,43 @@ CHQ_HD void hlld(const MState<T> &L, const MState<T> &R, T bn, T gamma, T gm1, T
   const T sls = sm - divz(abn, sqdl);
   const T srs = sm + divz(abn, sqdr);
 
-  // strict inequalities: with S*_L = S*_R = 0 both sides are averaged below
-  if (sls > T(0)) {
-    side_star_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, f);
-    return;
-  }
-  if (srs < T(0)) {
-    side_star_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, f);
-    return;
-  }
-  // bn ~ 0: the double-star region collapses onto the contact
+  // Region of the face (strict inequalities: with S*_L = S*_R = 0 both sides are averaged):
+  //   S*_L > 0           single-star flux of the left side
+  //   S*_R < 0           single-star flux of the right side
+  //   bn ~ 0             the double-star region collapses onto the contact: single-star flux
+  //                      of the side the contact moves away from
+  //   otherwise          double-star flux of that side
+  // and both sides averaged when the contact speed is exactly zero (or not a number). The
+  // side's operands are selected first and its flux is evaluated once, so the lanes of a
+  // warp whose contacts move either way run one flux evaluation instead of one per side.
   const T bnsmall = T(1e-12) * (ptl + ptr);
-  if (bnsq <= bnsmall) {
-    if (sm > T(0)) {
-      side_star_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, f);
-    } else if (sm < T(0)) {
-      side_star_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, f);
-    } else {
-      T fa[NFLX], fb[NFLX];
-      side_star_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, fa);
-      side_star_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, fb);
-#pragma unroll
-      for (int n = 0; n < NFLX; ++n) f[n] = T(0.5) * (fa[n] + fb[n]);
-    }
-    return;
-  }
+  const bool star_l = sls > T(0);
+  const bool star_r = !star_l && (srs < T(0));
+  const bool single = star_l || star_r || (bnsq <= bnsmall);
+  const bool pos = sm > T(0), neg = sm < T(0);
+  const bool both = !star_l && !star_r && !pos && !neg;
+  const bool left = star_l || (!star_r && (pos || both));
   // double-star states (MK05 eqs. 59-63)
-  const T sg = sgn(bn);
-  const T inv = T(1) / (sqdl + sqdr);
-  const T vss = ((sqdl * vls + sqdr * vrs) + (byrs - byls) * sg) * inv;
-  const T wss = ((sqdl * wls + sqdr * wrs) + (bzrs - bzls) * sg) * inv;
-  const T byss = ((sqdl * byrs + sqdr * byls) + (sqdl * sqdr) * ((vrs - vls) * sg)) * inv;
-  const T bzss = ((sqdl * bzrs + sqdr * bzls) + (sqdl * sqdr) * ((wrs - wls) * sg)) * inv;
-  const T vdotb_ss = (sm * bn + vss * byss) + wss * bzss;
-  if (sm > T(0)) {
-    const T elss = els - sqdl * ((vdotb_ls - vdotb_ss) * sg);
-    side_dstar_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, sls, vss, wss, byss, bzss, elss, f);
-  } else if (sm < T(0)) {
-    const T erss = ers + sqdr * ((vdotb_rs - vdotb_ss) * sg);
-    side_dstar_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, srs, vss, wss, byss, bzss, erss, f);
-  } else {
-    const T elss = els - sqdl * ((vdotb_ls - vdotb_ss) * sg);
-    const T erss = ers + sqdr * ((vdotb_rs - vdotb_ss) * sg);
-    T fa[NFLX], fb[NFLX];
-    side_dstar_flux<LHLLD>(L, bn, el, ptl, sl, dls, sm, vls, wls, byls, bzls, els, pts, sls, vss, wss, byss, bzss, elss, fa);
-    side_dstar_flux<LHLLD>(R, bn, er, ptr, sr, drs, sm, vrs, wrs, byrs, bzrs, ers, pts, srs, vss, wss, byss, bzss, erss, fb);
+  T sg = T(0), vss = T(0), wss = T(0), byss = T(0), bzss = T(0), vdotb_ss = T(0);
+  if (!single) {
+    sg = sgn(bn);
+    const T inv = T(1) / (sqdl + sqdr);
+    vss = ((sqdl * vls + sqdr * vrs) + (byrs - byls) * sg) * inv;
+    wss = ((sqdl * wls + sqdr * wrs) + (bzrs - bzls) * sg) * inv;
+    byss = ((sqdl * byrs + sqdr * byls) + (sqdl * sqdr) * ((vrs - vls) * sg)) * inv;
+    bzss = ((sqdl * bzrs + sqdr * bzls) + (sqdl * sqdr) * ((wrs - wls) * sg)) * inv;
+    vdotb_ss = (sm * bn + vss * byss) + wss * bzss;
+  }
+  side_region_flux<LHLLD>(left, single, L, R, bn, el, er, ptl, ptr, sl, sr, dls, drs, sm, vls, vrs, wls, wrs, byls,
+                          byrs, bzls, bzrs, els, ers, pts, sls, srs, sqdl, sqdr, vdotb_ls, vdotb_rs, sg, vss, wss,
+                          byss, bzss, vdotb_ss, f);
+  if (both) {
+    T fb[NFLX];
+    side_region_flux<LHLLD>(false, single, L, R, bn, el, er, ptl, ptr, sl, sr, dls, drs, sm, vls, vrs, wls, wrs,
+                            byls, byrs, bzls, bzrs, els, ers, pts, sls, srs, sqdl, sqdr, vdotb_ls, vdotb_rs, sg, vss,
+                            wss, byss, bzss, vdotb_ss, fb);
 #pragma unroll
-    for (int n = 0; n < NFLX; ++n) f[n] = T(0.5) * (fa[n] + fb[n]);
+    for (int n = 0; n < NFLX; ++n) f[n] = T(0.5) * (f[n] + fb[n]);
   }
 }
 
