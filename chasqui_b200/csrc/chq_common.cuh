@@ -35,6 +35,9 @@ struct Geom {
   int two_d, three_d;
   double x1min, x2min, x3min, x1max, x2max, x3max;
   double dx1, dx2, dx3;
+  // global index of this mesh's first active plane minus ks: 0 for a whole mesh, the slab's
+  // first plane for one z slab of a decomposed mesh (coordinates and seeded noise use it)
+  int koff;
   // device frame strides (elements)
   long sj;        // row pitch
   long sk;        // plane stride = (nj+1) * sj

@@ -2008,6 +2008,7 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   g.dx1 = (c.x1max - c.x1min) / c.nx1;
   g.dx2 = (c.x2max - c.x2min) / c.nx2;
   g.dx3 = (c.x3max - c.x3min) / c.nx3;
+  g.koff = 0;
   g.sj = (long)align_up((size_t)g.ni + 1, 32);
   g.sk = (long)(g.nj + 1) * g.sj;
   g.vstride = (long)align_up((size_t)(g.nk + 1) * g.sk, 64);

@@ -32,10 +32,10 @@ struct PgenArgs {
 
 CHQ_HD double pg_x1v(const Geom &g, int i) { return g.x1min + (i - g.is + 0.5) * g.dx1; }
 CHQ_HD double pg_x2v(const Geom &g, int j) { return g.x2min + (j - g.js + 0.5) * g.dx2; }
-CHQ_HD double pg_x3v(const Geom &g, int k) { return g.x3min + (k - g.ks + 0.5) * g.dx3; }
+CHQ_HD double pg_x3v(const Geom &g, int k) { return g.x3min + (k - g.ks + g.koff + 0.5) * g.dx3; }
 CHQ_HD double pg_x1f(const Geom &g, int i) { return g.x1min + (i - g.is) * g.dx1; }
 CHQ_HD double pg_x2f(const Geom &g, int j) { return g.x2min + (j - g.js) * g.dx2; }
-CHQ_HD double pg_x3f(const Geom &g, int k) { return g.x3min + (k - g.ks) * g.dx3; }
+CHQ_HD double pg_x3f(const Geom &g, int k) { return g.x3min + (k - g.ks + g.koff) * g.dx3; }
 
 // splitmix64 of (seed, index): uniform double in [0, 1) from the top 53 bits
 CHQ_HD double pg_uniform(unsigned long long seed, unsigned long long idx) {
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(256) pgen_cells_kernel(const PgenArgs a) {
     const bool active = (i >= g.is && i <= g.ie && j >= g.js && j <= g.je && k >= g.ks && k <= g.ke);
     if (amp != 0.0 && active) {
       const unsigned long long idx =
-          ((unsigned long long)(k - g.ks) * g.nx2 + (unsigned long long)(j - g.js)) * g.nx1 + (unsigned long long)(i - g.is);
+          ((unsigned long long)(k - g.ks + g.koff) * g.nx2 + (unsigned long long)(j - g.js)) * g.nx1 + (unsigned long long)(i - g.is);
       const unsigned long long seed = (unsigned long long)a.prm[6];
       d = 1.0 + amp * (2.0 * pg_uniform(seed, idx) - 1.0);
     }

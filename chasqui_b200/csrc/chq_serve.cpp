@@ -93,6 +93,10 @@ struct Group {
   bool dirty = false;
   long long cells = 0;
   std::vector<chq_mesh *> retired;   // finished members' meshes, freed after their batch is dropped
+  // launch settings of the lane, timed by chq_batch_autotune when the lane is first built and
+  // given to the members of every later rebuild (no timing then)
+  bool tuned = false;
+  int seglen = 0, xvar = 0;
 };
 
 int err(int code, const std::string &m) {
@@ -318,12 +322,19 @@ int rebuild(chq_server *S) {
     g.dirty = false;
     if (g.members.empty()) continue;
     std::vector<chq_mesh *> ms;
-    for (Job *j : g.members) ms.push_back(j->mesh);
-    int rc = chq_batch_create(ms.data(), (int)ms.size(), &g.batch);
+    int rc = CHQ_OK;
+    for (Job *j : g.members) {
+      ms.push_back(j->mesh);
+      if (S->autotune && g.tuned) {
+        if ((rc = chq_set_seglen(j->mesh, g.seglen)) || (rc = chq_set_xvariant(j->mesh, g.xvar))) return rc;
+      }
+    }
+    rc = chq_batch_create(ms.data(), (int)ms.size(), &g.batch);
     if (rc) return rc;
-    if (S->autotune) {
-      rc = chq_batch_autotune(g.batch, nullptr, nullptr, nullptr, nullptr);
+    if (S->autotune && !g.tuned) {
+      rc = chq_batch_autotune(g.batch, &g.seglen, &g.xvar, nullptr, nullptr);
       if (rc) return rc;
+      g.tuned = true;
     }
     chq_batch_set_graph(g.batch, 1);
   }

@@ -237,7 +237,8 @@ CHQ_API int chq_profile(chq_mesh *m, int enable);
  * members (their march lengths and the batch's x variant change together; the batch's tables
  * are rebuilt for each candidate) and caches per (precision, scheme, log2 of the batch's
  * cells, log2 of its member count); a batch of 2^23 cells or more fills the device with its
- * members' own settings and is returned untimed (the arrays hold -1). */
+ * members' own settings and is returned untimed (the arrays hold -1). A batch starts with its
+ * members' march lengths and its first member's x variant. */
 #define CHQ_TUNE_NLEN 5
 #define CHQ_TUNE_LENGTHS {4, 8, 16, 32, 64}
 #define CHQ_TUNE_NXVAR 2
@@ -319,7 +320,9 @@ CHQ_API int chq_server_set_lanes(chq_server *s, int lanes);
  * 2^21; smaller values return CHQ_ERR_ARG); takes effect for newly admitted jobs */
 CHQ_API int chq_server_set_solo_cells(chq_server *s, long long cells);
 /* tune every new lane's batch with chq_batch_autotune (1, the default) or keep the members'
- * default launch settings (0); takes effect for batches built afterwards */
+ * default launch settings (0); takes effect for batches built afterwards. A lane is timed once,
+ * when it is first built; its later rebuilds (members admitted or finished) give the new
+ * members the lane's tuned march length and x variant without timing. */
 CHQ_API int chq_server_set_autotune(chq_server *s, int enable);
 
 /* ---- history sums without any device allocation --------------------------------------------
