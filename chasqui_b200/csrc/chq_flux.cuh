@@ -260,12 +260,12 @@ template <int RE, class P> struct WindowStencil {
 
 // ---------------------------------------------------------------------------------------
 // Face work: Riemann solve of the face `lf` (between cells lf - stride and lf).
+// b_n: the face-normal field of the face (a sweep that prefetched it passes it in).
 template <int S, class P>
-CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, int lf, const P wl[8], const P wr[8]) {
+CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, int lf, const P wl[8], const P wr[8], const P b_n) {
   const P gamma = P(A.eos.gamma), gm1 = P(A.eos.gm1);
   MState<P> L{wl[0], wl[1], wl[2], wl[3], wl[4], wl[5], wl[6]};
   MState<P> R{wr[0], wr[1], wr[2], wr[3], wr[4], wr[5], wr[6]};
-  const P b_n = P(V.bn[lf]);
   if (A.low_mach) {
     // Thornber et al. (2008) blend of the normal velocities (src/physics.hpp:170-178)
     const P cl = fast_speed(L, b_n, gamma), cr = fast_speed(R, b_n, gamma);
@@ -314,6 +314,10 @@ CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, int lf, const P 
   V.out[5][lf] = (f[FD] > P(0)) ? f[FD] * sl : (f[FD] < P(0)) ? f[FD] * sr : P(0.5) * (f[FD] * (sl + sr));
   V.out[6][lf] = -f[FBY];
   V.out[7][lf] = f[FBZ];
+}
+template <int S, class P>
+CHQ_D void face_flux(const FluxArgs<P> &A, const DirView<P> &V, int lf, const P wl[8], const P wr[8]) {
+  face_flux<S, P>(A, V, lf, wl, wr, P(V.bn[lf]));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -397,7 +401,10 @@ CHQ_D void sweep_x_ppm(const FluxArgs<P> &A, int wid) {
 // the unlimited interface value F_{c-1/2} computed at the previous cell; the velocity adds
 // u_{c-1} and the pressure p_{c-2}, p_{c-1} (flattening). A cell then evaluates one slope
 // (s_{c+1}) and one interface value (F_{c+1/2}) per quantity instead of three and two, with
-// the reference's operands (bitwise the same limited states as the per-cell form).
+// the reference's operands (bitwise the same limited states as the per-cell form). In FP64
+// the face-normal field of the next face is copied asynchronously one cell ahead as well,
+// into one of two slots per thread (alternating, so a copy never lands in the slot being
+// read), instead of a load at the Riemann solve.
 struct PpmWin {
   static constexpr int nslot = 43;
   enum : int { Q0 = 0, Q1 = 1, Q2 = 2, S = 3, F = 4, X1 = 5, X2 = 6 };
@@ -426,6 +433,8 @@ CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   int lc = (d == 1) ? A.g.idx32(A.lo[1][0] + outer, f0 - 1, i) : A.g.idx32(f0 - 1, A.lo[2][1] + outer, i);
   const int t = threadIdx.x;
   P *col = win + t;
+  constexpr bool PFB = (sizeof(P) == 8);
+  double *bnw = reinterpret_cast<double *>(win + PpmWin::nslot * kYzThreads) + t;
 #define CHQ_SLOT(n, k) col[(PpmWin::off(n) + PpmWin::k) * kYzThreads]
   // cell f0-1: its slope, its left interface value and the window, from direct loads
 #pragma unroll
@@ -451,6 +460,11 @@ CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   for (int f = f0 - 1; f <= f1; ++f, lc += st) {
     cp_async_wait_all();
     const bool pre = (f < f1);
+    P bnv = P(0);
+    if constexpr (PFB) {
+      if (f >= f0) bnv = P(bnw[(f & 1) * kYzThreads]);
+      if (pre) cp_async_elem(bnw + ((f + 1) & 1) * kYzThreads, V.bn + lc + st);
+    }
     P aL[8], aR[8], qc[8], p5[5], um1 = P(0), up1 = P(0);
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
@@ -487,7 +501,10 @@ CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
     finish_states<R_PPM, P>(A, aL, aR, qc, p5, um1, up1);
 #pragma unroll
     for (int n = 0; n < 8; ++n) park[n * kYzThreads + t] = aR[n];
-    if (f >= f0) face_flux<S, P>(A, V, lc, wl, aL);
+    if (f >= f0) {
+      if constexpr (PFB) face_flux<S, P>(A, V, lc, wl, aL, bnv);
+      else face_flux<S, P>(A, V, lc, wl, aL);
+    }
 #pragma unroll
     for (int n = 0; n < 8; ++n) wl[n] = park[n * kYzThreads + t];
   }
@@ -586,9 +603,10 @@ template <class P> struct FluxYzMinBlocks { static constexpr int v = (sizeof(P) 
 
 template <int R, class P> __host__ __device__ constexpr size_t flux_yz_smem() {
   // park (8) + window: streaming PPM 43 slots (the characteristic PPM form uses 40 of them),
-  // otherwise 8 quantities x (2 reach + 1)
+  // otherwise 8 quantities x (2 reach + 1); streaming PPM in FP64 adds two face-field slots
   return (size_t)(8 + ((R == R_PPM) ? PpmWin::nslot : (Reach<R>::v > 0) ? 8 * (2 * Reach<R>::v + 1) : 0)) *
-         kYzThreads * sizeof(P);
+             kYzThreads * sizeof(P) +
+         ((R == R_PPM && sizeof(P) == 8) ? 2 * kYzThreads * sizeof(double) : 0);
 }
 
 template <int R, int S, bool CHAR, class P, int V = 0>
