@@ -244,9 +244,56 @@ def config_rates(steps: int = 5, warmup: int = 3) -> dict:
                 r["rkl2_stages_per_cycle"] = m.sts_stages() / (warmup + steps)
             out[name + ("_mixed" if prec else "_fp64")] = r
             m.close()
+    # the decomposed path on one device: the 512^3 blast as two z slabs with in-process halos
+    out["blast3d_512_2slabs_one_gpu_fp64"] = slab_run(512, 2, steps, warmup)
     out["ot2d_256_hst_every_cycle_fp64"] = history_rates()
     out["rkl2_batch_64x_ot2d_64_fp64"] = rkl2_batch_rates()
     return out
+
+
+def slab_run(n: int, nslab: int, steps: int, warmup: int, dist=None, rank: int = 0, local: bool = True) -> dict:
+    """The headline blast as z slabs (chasqui_b200/slabs.py): with local=True all nslab slabs
+    on this GPU (in-process halo exchange: the cost of the decomposed stage on one device);
+    otherwise this rank's slab of nslab ranks with NCCL messages between GPUs. CUDA events on
+    the slabs' stream around `steps` cycles; the slowest rank's time."""
+    import torch
+    from chasqui_b200.slabs import DistExchange, LocalExchange, SlabMesh, SlabRun
+    stream = torch.cuda.Stream()
+    mine = range(nslab) if local else [rank]
+    slabs = [SlabMesh(blast_config(n, 0), nslab, r) for r in mine]
+    for s in slabs:
+        s.init_problem("blast", BLAST_PARAMS)
+    if local:
+        ex = LocalExchange(slabs, stream)
+    else:
+        # the halo planes and step-control words live on the GPUs: an NCCL group beside the
+        # gloo group of the timings, created collectively by a first all-reduce
+        import datetime
+        torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+        group = dist.new_group(backend="nccl", timeout=datetime.timedelta(seconds=120))
+        dist.all_reduce(torch.zeros(1, device="cuda"), group=group)
+        ex = DistExchange(slabs[0], stream, group=group)
+    run = SlabRun(slabs, ex, stream)
+    run.prime(0.0)
+    run.cycles(warmup)
+    run.synchronize()
+    l0 = sum(s.kernel_launches() for s in slabs)
+    barrier(dist)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run.cycles(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = dist_max(dist, e0.elapsed_time(e1))
+    launches = sum(s.kernel_launches() for s in slabs) - l0
+    ck = slabs[0].clock()
+    fofc = slabs[0].counters()[0]
+    for s in slabs:
+        s.close()
+    return {"value": float(n) ** 3 * steps / (ms / 1e3), "ms_per_step": ms / steps, "slabs": nslab,
+            "cycle": ck["cycle"], "fofc_corrections": fofc, "gpu_launches": launches,
+            "how": ("all slabs on one GPU, halo planes packed and unpacked in-process" if local else
+                    "one slab per rank and GPU, halo planes as NCCL messages to the ring neighbours")}
 
 
 def rkl2_batch_rates(jobs: int = 64, n: int = 64, cycles: int = 20) -> dict:
@@ -748,6 +795,8 @@ def main(argv=None):
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--serving-study", action="store_true",
                     help="only the serving configuration at its own size range (see serving_study)")
+    ap.add_argument("--slabs", action="store_true",
+                    help="only the headline blast decomposed into one z slab per rank (strong scaling)")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     rank, local = env_int("RANK", 0), env_int("LOCAL_RANK", 0)
@@ -758,6 +807,17 @@ def main(argv=None):
     dist = dist_init()
     world = env_int("WORLD_SIZE", 1)
     set_device(local)
+    if args.slabs:
+        r = slab_run(args.n, world, args.steps, args.warmup, dist, rank, local=False)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                              "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic", "config": dict(workload_config(args.n, world), parallelism=f"z slabs x{world}"),
+                              "slabs": r}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     if args.serving_study:
         res = serving_study(args, dist, rank, world)
         if rank == 0:

@@ -121,6 +121,16 @@ SIGNATURES = [
     ("chq_server_set_autotune", C.c_int, [_P, C.c_int]),
     ("chq_history_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       _P, _P, _P, _P, _D, _P]),
+    ("chq_slab_create", C.c_int, [C.POINTER(chq_config), C.c_int, C.c_int, C.POINTER(_P)]),
+    ("chq_slab_info", C.c_int, [_P, C.POINTER(C.c_int)]),
+    ("chq_slab_halo_bytes", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
+    ("chq_slab_pack", C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P, _P]),
+    ("chq_slab_unpack", C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P, _P]),
+    ("chq_slab_ctl", C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    ("chq_slab_prime", C.c_int, [_P, C.c_double, C.c_int, _P]),
+    ("chq_slab_begin", C.c_int, [_P, _P]),
+    ("chq_slab_stage", C.c_int, [_P, C.c_int, C.c_int, _P]),
+    ("chq_slab_end", C.c_int, [_P, _P]),
 ]
 
 TUNE_LENGTHS = (4, 8, 16, 32, 64)   # CHQ_TUNE_LENGTHS
@@ -184,13 +194,16 @@ class Mesh:
         lib = load_library()
         self.cfg = cfg if cfg is not None else make_config(**kw)
         h = _P()
-        _check(lib.chq_mesh_create(C.byref(self.cfg), C.byref(h)))
+        _check(self._create(lib, h))
         self._h = h
         d = (C.c_int * 10)()
         _check(lib.chq_mesh_dims(h, d))
         (self.nx1, self.nx2, self.nx3, self.ng, self.ni, self.nj, self.nk, self.nstage,
          two, three) = list(d)
         self.two_d, self.three_d = bool(two), bool(three)
+
+    def _create(self, lib, h) -> int:
+        return lib.chq_mesh_create(C.byref(self.cfg), C.byref(h))
 
     @classmethod
     def from_params(cls, pin: Params, **extra) -> "Mesh":

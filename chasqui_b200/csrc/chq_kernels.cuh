@@ -415,6 +415,7 @@ template <class P> struct RepairArgs {
   DiffArgs<P> diff;
   const int *list;          // flagged cells (linear indices) of this stage, or null
   int cap;                  // list capacity
+  int kext[2];              // z slab: the ghost plane below / above holds the neighbouring slab's flags
 };
 
 template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k, int j, int i) {
@@ -422,8 +423,9 @@ template <int DIR, class P> CHQ_D void repair_face(const RepairArgs<P> &A, int k
   constexpr int IVU = IVX + DIR, IVV = IVX + (DIR + 1) % 3, IVW = IVX + (DIR + 2) % 3;
   constexpr int IBT1 = (DIR + 1) % 3, IBT2 = (DIR + 2) % 3;
   const int kL = k - (DIR == 2), jL = j - (DIR == 1), iL = i - (DIR == 0);
+  // cells of the mesh (with a z slab's neighbouring planes, which are cells of the whole mesh)
   auto inside = [&](int kk, int jj, int ii) {
-    return (ii >= g.is && ii <= g.ie && jj >= g.js && jj <= g.je && kk >= g.ks && kk <= g.ke);
+    return (ii >= g.is && ii <= g.ie && jj >= g.js && jj <= g.je && kk >= g.ks - A.kext[0] && kk <= g.ke + A.kext[1]);
   };
   const long l = g.idx(k, j, i), lL = g.idx(kL, jL, iL);
   const bool fr = inside(k, j, i) && A.flag[l];
@@ -632,6 +634,7 @@ struct BcArgs {
   double *u, *b1, *b2, *b3;
   int bc;
   const int *done;
+  int zside;   // z sweep: bit 0 fills the lower ghosts, bit 1 the upper ones (a z slab's peer sides get halos instead)
 };
 
 template <int DIR> CHQ_D void bc_body(const BcArgs &A, int bx) {
@@ -706,26 +709,52 @@ template <int DIR> CHQ_D void bc_body(const BcArgs &A, int bx) {
     const int srcl = (A.bc == 0) ? kl + g.nx3 : (A.bc == 1) ? g.ks : 2 * g.ks - 1 - kl;
     const int srcr = (A.bc == 0) ? kr - g.nx3 : (A.bc == 1) ? g.ke : 2 * g.ke + 1 - kr;
     const long lkl = g.idx(kl, j, i), lkr = g.idx(kr, j, i), lsl = g.idx(srcl, j, i), lsr = g.idx(srcr, j, i);
+    const bool lo = (A.zside & 1) != 0, hi = (A.zside & 2) != 0;
     if (j < g.nj && i < g.ni) {
 #pragma unroll
       for (int n = 0; n < NVAR; ++n) {
         const double f = (n == IM3) ? sgn : 1.0;
-        A.u[n * vs + lkl] = f * A.u[n * vs + lsl];
-        A.u[n * vs + lkr] = f * A.u[n * vs + lsr];
+        if (lo) A.u[n * vs + lkl] = f * A.u[n * vs + lsl];
+        if (hi) A.u[n * vs + lkr] = f * A.u[n * vs + lsr];
       }
     }
-    A.b1[lkl] = A.b1[lsl]; A.b1[lkr] = A.b1[lsr];
-    A.b2[lkl] = A.b2[lsl]; A.b2[lkr] = A.b2[lsr];
+    if (lo) { A.b1[lkl] = A.b1[lsl]; A.b2[lkl] = A.b2[lsl]; }
+    if (hi) { A.b1[lkr] = A.b1[lsr]; A.b2[lkr] = A.b2[lsr]; }
     const int fl = gh, fr = g.ke + 2 + gh;
     const long lfl = g.idx(fl, j, i), lfr = g.idx(fr, j, i);
-    if (A.bc == 0) { A.b3[lfl] = A.b3[g.idx(fl + g.nx3, j, i)]; A.b3[lfr] = A.b3[g.idx(fr - g.nx3, j, i)]; }
-    else if (A.bc == 1) { A.b3[lfl] = A.b3[g.idx(g.ks, j, i)]; A.b3[lfr] = A.b3[g.idx(g.ke + 1, j, i)]; }
-    else { A.b3[lfl] = -A.b3[g.idx(2 * g.ks - fl, j, i)]; A.b3[lfr] = -A.b3[g.idx(2 * (g.ke + 1) - fr, j, i)]; }
-    if (A.bc == 0 && gh == 0) A.b3[g.idx(g.ke + 1, j, i)] = A.b3[g.idx(g.ks, j, i)];
+    if (A.bc == 0) {
+      if (lo) A.b3[lfl] = A.b3[g.idx(fl + g.nx3, j, i)];
+      if (hi) A.b3[lfr] = A.b3[g.idx(fr - g.nx3, j, i)];
+    } else if (A.bc == 1) {
+      if (lo) A.b3[lfl] = A.b3[g.idx(g.ks, j, i)];
+      if (hi) A.b3[lfr] = A.b3[g.idx(g.ke + 1, j, i)];
+    } else {
+      if (lo) A.b3[lfl] = -A.b3[g.idx(2 * g.ks - fl, j, i)];
+      if (hi) A.b3[lfr] = -A.b3[g.idx(2 * (g.ke + 1) - fr, j, i)];
+    }
+    if (A.bc == 0 && gh == 0 && lo && hi) A.b3[g.idx(g.ke + 1, j, i)] = A.b3[g.idx(g.ks, j, i)];
   }
 }
 
 template <int DIR> __global__ void __launch_bounds__(256) bc_kernel(const BcArgs A) { bc_body<DIR>(A, blockIdx.x); }
+
+// Halo exchange of z slabs (chq_slab_pack / chq_slab_unpack): contiguous spans of 8-byte
+// words copied between a slab's planes and a packed buffer, one grid row (blockIdx.y) per span.
+constexpr int kHaloSpans = 12;
+struct HaloArgs {
+  unsigned long long *dst[kHaloSpans];
+  const unsigned long long *src[kHaloSpans];
+  long words[kHaloSpans];
+  int nspan;
+};
+__global__ void __launch_bounds__(256) halo_copy_kernel(const HaloArgs A) {
+  const int q = (int)blockIdx.y;
+  if (q >= A.nspan) return;
+  unsigned long long *d = A.dst[q];
+  const unsigned long long *src = A.src[q];
+  const long n = A.words[q];
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) d[t] = src[t];
+}
 
 // ---------------------------------------------------------------------------------------
 // K5

@@ -202,6 +202,13 @@ struct chq_mesh {
   int act_lo[3][3], act_hi[3][3];
   int seglen;
   int xvar = 0;   // x-sweep kernel variant (register cap), chq_autotune
+  // z slab of a decomposed mesh (chq_slab_create): the lower / upper z side borders another
+  // slab (its ghosts come from chq_slab_unpack, not from the boundary kernel); slab geometry
+  int zpeer[2] = {0, 0};
+  int slab_rank = 0, slab_count = 1;
+  // the FOFC repair reads the flags of the ghost plane below / above: only across an internal
+  // slab boundary (at the periodic wrap the whole mesh's ghost cells are never flagged cells)
+  int fofc_ext[2] = {0, 0};
   // RKL2 work arrays (cfg.sts only): Y0..Y2, M0, Mj on cells; their face-field twins
   double *sy[3] = {}, *sm0 = nullptr, *smj = nullptr;
   double *sb[3][3] = {}, *smb0[3] = {}, *smbj[3] = {};
@@ -567,6 +574,8 @@ RepairArgs<P> repair_args(chq_mesh *m, int cur, unsigned dirmask, const int *don
   a.need = need;
   a.list = m->bad_list;
   a.cap = m->bad_cap;
+  a.kext[0] = m->fofc_ext[0];
+  a.kext[1] = m->fofc_ext[1];
   return a;
 }
 
@@ -633,6 +642,7 @@ BcArgs bc_args(chq_mesh *m, int buf, const int *done, int dir) {
   a.b1 = m->bf[buf][0]; a.b2 = m->bf[buf][1]; a.b3 = m->bf[buf][2];
   a.done = done;
   a.bc = (dir == 0) ? m->cfg.bc1 : (dir == 1) ? m->cfg.bc2 : m->cfg.bc3;
+  a.zside = 3;
   return a;
 }
 
@@ -663,7 +673,9 @@ int do_bc_ptr(chq_mesh *m, double *u, double *b1, double *b2, double *b3, const 
     bc_kernel<1><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
     CHQ_CUDA(cudaGetLastError());
   }
-  if (g.three_d) {
+  // a z slab's peer sides receive halos from the neighbouring slabs instead (chq_slab_unpack)
+  a.zside = (m->zpeer[0] ? 0 : 1) | (m->zpeer[1] ? 0 : 2);
+  if (g.three_d && a.zside) {
     a.bc = m->cfg.bc3;
     n = (long)g.ng * (g.nj + 1) * (g.ni + 1);
     m->nlaunch += 1;
@@ -890,8 +902,10 @@ int do_repair_d(chq_mesh *m, int cur, bool with_diff, const int *done, const int
 // One RK stage (src/main.cpp:46-93) with all decisions on the device. With explicit
 // diffusion (diffusion.sts off) the diffusive fluxes join the hyperbolic ones before the
 // limiter and eta J joins the corner EMFs before the update, also in the FOFC re-run.
-int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, const double *bdt_dev,
-              const int *done, cudaStream_t s) {
+// First part: fluxes through the update and the FOFC flags (the FOFC count is complete
+// when it ends; a z slab adds the other slabs' counts before the second part).
+int run_stage_a(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, const double *bdt_dev,
+                const int *done, cudaStream_t s) {
   int rc;
   const bool dstage = m->diff && !m->cfg.sts;
   const double *bc1 = m->bf[cur][0], *bc2 = m->bf[cur][1], *bc3 = m->bf[cur][2];
@@ -920,11 +934,20 @@ int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, c
     if ((rc = DISPATCH_P(m, do_update)(m, out, g0, g1, bdt, bdt_dev, done, nullptr, s))) return rc;
   }
   if (m->cfg.fofc) {
+    Prof p(m, PK_FLAG, s);
+    if ((rc = do_flag(m, out, &m->ctl->nbad, done, s))) return rc;
+  }
+  return CHQ_OK;
+}
+
+// Second part: the FOFC repair and re-runs when cells were flagged, then the ghost fill.
+int run_stage_b(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, const double *bdt_dev,
+                const int *done, cudaStream_t s) {
+  int rc;
+  const bool dstage = m->diff && !m->cfg.sts;
+  const double *bc1 = m->bf[cur][0], *bc2 = m->bf[cur][1], *bc3 = m->bf[cur][2];
+  if (m->cfg.fofc) {
     int *nbad = &m->ctl->nbad;
-    {
-      Prof p(m, PK_FLAG, s);
-      if ((rc = do_flag(m, out, nbad, done, s))) return rc;
-    }
     Prof p(m, PK_REPAIR, s);
     if (m->mixed) rc = do_repair_d<float>(m, cur, dstage, done, nbad, s);
     else rc = do_repair_d<double>(m, cur, dstage, done, nbad, s);
@@ -938,6 +961,12 @@ int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, c
   }
   Prof p(m, PK_BC, s);
   return do_bc(m, out, done, s);
+}
+
+int run_stage(chq_mesh *m, int cur, int out, double g0, double g1, double bdt, const double *bdt_dev,
+              const int *done, cudaStream_t s) {
+  const int rc = run_stage_a(m, cur, out, g0, g1, bdt, bdt_dev, done, s);
+  return rc ? rc : run_stage_b(m, cur, out, g0, g1, bdt, bdt_dev, done, s);
 }
 
 // ---- RKL2 super-time-stepping (src/sts.hpp) ---------------------------------------------
@@ -1970,10 +1999,21 @@ void chq_config_defaults(chq_config *c) {
   c->cool_alpha = 1.0;
 }
 
-int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
+}  // extern "C"
+
+namespace {
+// A whole mesh (nslab = 1) or z slab `rank` of `nslab` equal slabs of the mesh cfg describes:
+// the slab holds nx3 / nslab active planes, keeps the whole mesh's x3 extent, cell width and
+// coordinates (Geom::koff), and marks the z sides that border another slab.
+int mesh_create_impl(const chq_config *cfg, int nslab, int rank, chq_mesh **out) {
   if (!cfg || !out) return fail(CHQ_ERR_ARG, "null argument");
   *out = nullptr;
-  const chq_config &c = *cfg;
+  chq_config cl = *cfg;
+  if (nslab > 1) {
+    if (cfg->nx3 < 2 || cfg->nx3 % nslab != 0) return fail(CHQ_ERR_ARG, "z slabs: nx3 must be a multiple of the slab count");
+    cl.nx3 = cfg->nx3 / nslab;
+  }
+  const chq_config &c = cl;
   if (c.nx1 < 1 || c.nx2 < 1 || c.nx3 < 1) return fail(CHQ_ERR_ARG, "nx must be >= 1");
   if (c.nx2 == 1 && c.nx3 > 1) return fail(CHQ_ERR_ARG, "nx3 > 1 requires nx2 > 1");
   if (c.recon < 0 || c.recon > 4) return fail(CHQ_ERR_ARG, "unknown reconstruction");
@@ -1988,6 +2028,10 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   const int ng = (c.nghost > 0) ? c.nghost : ng_min;
   if (ng < ng_min) return fail(CHQ_ERR_ARG, "nghost too small for the reconstruction method");
   if (c.nu < 0 || c.kappa < 0 || c.eta < 0) return fail(CHQ_ERR_ARG, "diffusion coefficients must be >= 0");
+  if (nslab > 1) {
+    if (c.nx3 < ng) return fail(CHQ_ERR_ARG, "z slabs: each slab needs at least nghost planes");
+    if (c.sts || c.cooling) return fail(CHQ_ERR_ARG, "z slabs: RKL2 super-time-stepping and cooling are not supported");
+  }
 
   chq_mesh *m = new chq_mesh;
   cudaGetDevice(&m->device);
@@ -2009,6 +2053,17 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   g.dx2 = (c.x2max - c.x2min) / c.nx2;
   g.dx3 = (c.x3max - c.x3min) / c.nx3;
   g.koff = 0;
+  if (nslab > 1) {
+    // the whole mesh's cell width and the global index of this slab's first plane
+    g.dx3 = (c.x3max - c.x3min) / cfg->nx3;
+    g.koff = rank * c.nx3;
+    m->slab_rank = rank;
+    m->slab_count = nslab;
+    m->zpeer[0] = (rank > 0 || c.bc3 == CHQ_BC_PERIODIC) ? 1 : 0;
+    m->zpeer[1] = (rank < nslab - 1 || c.bc3 == CHQ_BC_PERIODIC) ? 1 : 0;
+    m->fofc_ext[0] = (rank > 0) ? 1 : 0;
+    m->fofc_ext[1] = (rank < nslab - 1) ? 1 : 0;
+  }
   g.sj = (long)align_up((size_t)g.ni + 1, 32);
   g.sk = (long)(g.nj + 1) * g.sj;
   g.vstride = (long)align_up((size_t)(g.nk + 1) * g.sk, 64);
@@ -2083,6 +2138,9 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   m->bad_list = (int *)p; p += align_up(kBadCap * sizeof(int), 256);
   m->bad_cap = (int)kBadCap;
   if (const char *cap = std::getenv("CHQ_FOFC_LIST_CAP")) m->bad_cap = std::max(0, std::min(std::atoi(cap), (int)kBadCap));
+  // a slab's FOFC repair also reads the flags of the neighbouring slabs' boundary planes,
+  // which are not in its own cell list: slabs repair by scanning every face
+  if (nslab > 1) m->bad_cap = 0;
   m->ctl = (StepCtl *)p; p += ctl_bytes;
   m->hst_part = (double *)p;
   m->hst_out = m->hst_part + (size_t)m->hst_blocks * 10;
@@ -2130,6 +2188,16 @@ int chq_mesh_create(const chq_config *cfg, chq_mesh **out) {
   }
   *out = m;
   return CHQ_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int chq_mesh_create(const chq_config *cfg, chq_mesh **out) { return mesh_create_impl(cfg, 1, 0, out); }
+
+int chq_slab_create(const chq_config *cfg, int nslab, int rank, chq_mesh **out) {
+  if (nslab < 1 || rank < 0 || rank >= nslab) return fail(CHQ_ERR_ARG, "z slabs: rank out of range");
+  return mesh_create_impl(cfg, nslab, rank, out);
 }
 
 int chq_mesh_destroy(chq_mesh *m) {
@@ -2451,6 +2519,7 @@ int chq_limit_fluxes(chq_mesh *m, int dir, double beta_dt, long *count, void *st
 
 int chq_stage(chq_mesh *m, int cur, int out, double g0, double g1, double beta_dt, void *stream) {
   if (!m || (cur != 0 && cur != 1) || (out != 0 && out != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  if (m->slab_count > 1) return fail(CHQ_ERR_ARG, "a z slab steps through chq_slab_stage");
   cudaStream_t s = S(m, stream);
   CHQ_CUDA(cudaMemsetAsync(&m->ctl->nbad, 0, sizeof(int), s));
   return run_stage(m, cur, out, g0, g1, beta_dt, nullptr, nullptr, s);
@@ -2458,6 +2527,7 @@ int chq_stage(chq_mesh *m, int cur, int out, double g0, double g1, double beta_d
 
 int chq_prime(chq_mesh *m, double t, void *stream) {
   if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  if (m->slab_count > 1) return fail(CHQ_ERR_ARG, "a z slab is primed through chq_slab_prime");
   cudaStream_t s = S(m, stream);
   ctl_prime_kernel<<<1, 1, 0, s>>>(m->ctl, t);
   CHQ_CUDA(cudaGetLastError());
@@ -2594,6 +2664,7 @@ extern "C" {
 // captured one's.
 int chq_cycles(chq_mesh *m, int n, void *stream) {
   if (!m || n < 0) return fail(CHQ_ERR_ARG, "bad argument");
+  if (m->slab_count > 1) return fail(CHQ_ERR_ARG, "a z slab steps through chq_slab_begin / chq_slab_stage / chq_slab_end");
   cudaStream_t s = S(m, stream);
   const bool graphable = !(m->cfg.sts && m->diff) && !m->prof && (stream == nullptr || s == m->stream);
   if (!graphable || n == 0) return plain_cycles(m, n, s);
@@ -2945,6 +3016,7 @@ int chq_batch_create(chq_mesh *const *meshes, int n, chq_batch **out) {
   for (int j = 0; j < n; ++j) {
     const chq_mesh *m = meshes[j];
     if (!m) return fail(CHQ_ERR_ARG, "null mesh in batch");
+    if (m->slab_count > 1) return fail(CHQ_ERR_ARG, "a z slab cannot be a batch member");
     if (m->mixed != a->mixed || m->cfg.recon != a->cfg.recon || m->cfg.rsolver != a->cfg.rsolver ||
         m->cfg.characteristic != a->cfg.characteristic || m->nstage != a->nstage || m->cfg.fofc != a->cfg.fofc ||
         m->cfg.flux_limiter != a->cfg.flux_limiter)
@@ -3310,6 +3382,203 @@ int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launches[CHQ_N
     if (launches) launches[k] = m->prof_n[k];
     if (reset) { m->prof_ms[k] = 0; m->prof_n[k] = 0; }
   }
+  return CHQ_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// z slabs of one decomposed mesh (single-job multi-GPU domain decomposition). Each slab runs
+// the stage of a whole mesh on its own planes; between the parts below the caller moves data
+// between slabs (chq_slab_pack / chq_slab_unpack, and reductions of the step-control words
+// chq_slab_ctl returns). Every part is asynchronous on `stream` (NULL = the mesh stream).
+namespace {
+
+int slab_check(chq_mesh *m) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  if (m->hrec) return fail(CHQ_ERR_ARG, "z slabs: device history recording is not supported");
+  return CHQ_OK;
+}
+
+// spans of the halo message `what` for `side` (0: lower, 1: upper): pack = the planes the
+// neighbour on that side needs, unpack = this slab's ghost planes that the neighbour on that
+// side fills.
+//   what 0: the state of buffer `buf` (the nghost planes the neighbour's ghosts hold);
+//   what 1: the FOFC message of a stage whose output is buffer `buf`: the flags, b1 and b2 of
+//           the boundary plane. The repair of the transverse faces on the ghost plane reads
+//           the face-normal field of the stage's current state, which in a stage whose output
+//           overwrites it (src/main.cpp:68-91) is the first update's output there.
+int halo_spans(chq_mesh *m, int what, int buf, int side, bool pack, HaloArgs &a, long &words) {
+  const Geom &g = m->g;
+  const long sk = g.sk, vs = g.vstride, ng = g.ng;
+  a = HaloArgs{};
+  words = 0;
+  auto add = [&](void *base, long first_plane, long nplanes, size_t esize) {
+    a.src[a.nspan] = nullptr;
+    a.dst[a.nspan] = reinterpret_cast<unsigned long long *>(static_cast<char *>(base) + (size_t)first_plane * sk * esize);
+    a.words[a.nspan] = nplanes * sk * (long)esize / 8;
+    words += a.words[a.nspan];
+    ++a.nspan;
+  };
+  if ((what != 0 && what != 1) || (buf != 0 && buf != 1)) return fail(CHQ_ERR_ARG, "z slabs: unknown halo message");
+  if (what == 1) {
+    // the boundary plane (pack) or the ghost plane next to it (unpack)
+    const long k = pack ? (side == 0 ? g.ks : g.ke) : (side == 0 ? g.ks - 1 : g.ke + 1);
+    add(m->flag, k, 1, sizeof(int));
+    add(m->bf[buf][0], k, 1, sizeof(double));
+    add(m->bf[buf][1], k, 1, sizeof(double));
+    return CHQ_OK;
+  }
+  // cell planes of u (6 components), b1, b2; face planes of b3
+  long kc, kf, nf;
+  if (pack) {
+    kc = (side == 0) ? g.ks : g.ke + 1 - ng;
+    kf = kc;
+    nf = (side == 0) ? ng + 1 : ng;   // the lower neighbour also takes the shared face
+  } else {
+    kc = (side == 0) ? 0 : g.ke + 1;
+    kf = kc;
+    nf = (side == 0) ? ng : ng + 1;
+  }
+  for (int n = 0; n < NVAR; ++n) add(m->u[buf] + n * vs, kc, ng, sizeof(double));
+  add(m->bf[buf][0], kc, ng, sizeof(double));
+  add(m->bf[buf][1], kc, ng, sizeof(double));
+  add(m->bf[buf][2], kf, nf, sizeof(double));
+  return CHQ_OK;
+}
+
+int halo_copy(chq_mesh *m, int what, int buf, int side, bool pack, void *dev, cudaStream_t s) {
+  if (side != 0 && side != 1) return fail(CHQ_ERR_ARG, "z slabs: side must be 0 or 1");
+  if (!m->zpeer[side]) return fail(CHQ_ERR_ARG, "z slabs: no neighbouring slab on that side");
+  // the FOFC message crosses internal slab boundaries only: at the periodic wrap the whole
+  // mesh's repair sees ghost cells (never flagged) and the stage-start ghost fields
+  if (what == 1 && !m->fofc_ext[side]) return CHQ_OK;
+  if (!dev || (reinterpret_cast<uintptr_t>(dev) & 7)) return fail(CHQ_ERR_ARG, "z slabs: buffer must be 8-byte aligned");
+  HaloArgs a;
+  long words = 0;
+  if (int rc = halo_spans(m, what, buf, side, pack, a, words)) return rc;
+  // the packed buffer holds the spans back to back
+  unsigned long long *b = static_cast<unsigned long long *>(dev);
+  long maxw = 0;
+  for (int q = 0; q < a.nspan; ++q) {
+    if (pack) {
+      a.src[q] = a.dst[q];
+      a.dst[q] = b;
+    } else {
+      a.src[q] = b;
+    }
+    b += a.words[q];
+    maxw = std::max(maxw, a.words[q]);
+  }
+  const dim3 grid((unsigned)std::max(1L, std::min(64L, (maxw + 255) / 256)), (unsigned)a.nspan);
+  m->nlaunch += 1;
+  halo_copy_kernel<<<grid, 256, 0, s>>>(a);
+  CHQ_CUDA(cudaGetLastError());
+  return CHQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int chq_slab_info(const chq_mesh *m, int info[5]) {
+  if (!m || !info) return fail(CHQ_ERR_ARG, "null argument");
+  // info[2], info[3]: the side borders another slab (periodic wrap included)
+  info[0] = m->slab_rank;
+  info[1] = m->slab_count;
+  info[2] = m->zpeer[0];
+  info[3] = m->zpeer[1];
+  info[4] = m->g.koff;
+  return CHQ_OK;
+}
+
+int chq_slab_halo_bytes(chq_mesh *m, int what, int side, long long *bytes) {
+  if (!m || !bytes || (side != 0 && side != 1)) return fail(CHQ_ERR_ARG, "bad argument");
+  HaloArgs a;
+  long words = 0;
+  if (int rc = halo_spans(m, what, 0, side, true, a, words)) return rc;
+  *bytes = (long long)words * 8;
+  return CHQ_OK;
+}
+
+int chq_slab_pack(chq_mesh *m, int what, int buf, int side, void *dev, void *stream) {
+  if (int rc = slab_check(m)) return rc;
+  return halo_copy(m, what, buf, side, true, dev, S(m, stream));
+}
+
+int chq_slab_unpack(chq_mesh *m, int what, int buf, int side, const void *dev, void *stream) {
+  if (int rc = slab_check(m)) return rc;
+  return halo_copy(m, what, buf, side, false, const_cast<void *>(dev), S(m, stream));
+}
+
+int chq_slab_ctl(chq_mesh *m, int **nbad, unsigned long long **mdt_bits, unsigned long long **rho_bits) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  if (nbad) *nbad = &m->ctl->nbad;
+  if (mdt_bits) *mdt_bits = &m->ctl->mdt_bits;
+  if (rho_bits) *rho_bits = &m->ctl->rho_bits;
+  return CHQ_OK;
+}
+
+int chq_slab_prime(chq_mesh *m, double t, int part, void *stream) {
+  if (int rc = slab_check(m)) return rc;
+  cudaStream_t s = S(m, stream);
+  int rc = CHQ_OK;
+  if (part == 0) {
+    ctl_prime_kernel<<<1, 1, 0, s>>>(m->ctl, t);
+    CHQ_CUDA(cudaGetLastError());
+    m->nlaunch += 1;
+    return do_bc(m, 0, nullptr, s);
+  }
+  if (part == 1) {
+    if ((rc = DISPATCH_P(m, do_c2p)(m, 0, 1, &m->ctl->mdt_bits, m->ctl, nullptr, s))) return rc;
+    if (m->diff && (rc = DISPATCH_P(m, do_rho_min)(m, nullptr, s))) return rc;
+    return CHQ_OK;
+  }
+  if (part == 2) {
+    ctl_take_dt_kernel<<<1, 1, 0, s>>>(m->ctl);
+    CHQ_CUDA(cudaGetLastError());
+    m->nlaunch += 1;
+    return CHQ_OK;
+  }
+  return fail(CHQ_ERR_ARG, "z slabs: prime part must be 0, 1 or 2");
+}
+
+int chq_slab_begin(chq_mesh *m, void *stream) {
+  if (int rc = slab_check(m)) return rc;
+  cudaStream_t s = S(m, stream);
+  ctl_begin_kernel<<<1, 1, 0, s>>>(m->ctl, 0);
+  CHQ_CUDA(cudaGetLastError());
+  m->nlaunch += 1;
+  return CHQ_OK;
+}
+
+int chq_slab_stage(chq_mesh *m, int stage, int part, void *stream) {
+  if (int rc = slab_check(m)) return rc;
+  if (stage < 1 || stage > m->nstage) return fail(CHQ_ERR_ARG, "z slabs: stage out of range");
+  cudaStream_t s = S(m, stream);
+  double g0, g1, beta;
+  int cur, out;
+  stage_table(m->nstage, stage, g0, g1, beta, cur, out);
+  const int *done = &m->ctl->done;
+  const double *bdt = &m->ctl->beta_dt[stage - 1];
+  if (part == 0) return run_stage_a(m, cur, out, g0, g1, 0.0, bdt, done, s);
+  if (part == 1) return run_stage_b(m, cur, out, g0, g1, 0.0, bdt, done, s);
+  if (part == 2) {
+    const bool last = (stage == m->nstage);
+    int rc = last ? DISPATCH_P(m, do_c2p_end)(m, done, s)
+                  : DISPATCH_P(m, do_c2p)(m, out, 0, &m->ctl->mdt_bits, m->ctl, done, s);
+    if (!rc && last && m->diff) rc = DISPATCH_P(m, do_rho_min)(m, done, s);
+    return rc;
+  }
+  return fail(CHQ_ERR_ARG, "z slabs: stage part must be 0, 1 or 2");
+}
+
+int chq_slab_end(chq_mesh *m, void *stream) {
+  if (int rc = slab_check(m)) return rc;
+  cudaStream_t s = S(m, stream);
+  ctl_end_kernel<<<1, 1, 0, s>>>(m->ctl);
+  CHQ_CUDA(cudaGetLastError());
+  m->nlaunch += 1;
   return CHQ_OK;
 }
 

@@ -325,6 +325,50 @@ CHQ_API int chq_server_set_solo_cells(chq_server *s, long long cells);
  * members the lane's tuned march length and x variant without timing. */
 CHQ_API int chq_server_set_autotune(chq_server *s, int enable);
 
+/* ---- z slabs: one mesh decomposed over several GPUs ------------------------------------------
+ * No counterpart in the reference, whose mesh is one block on one device (src/mesh.hpp;
+ * README.md:163 and :175 list domain decomposition as future work). A mesh of nx3 planes is
+ * cut into nslab slabs of nx3 / nslab planes along z, one per rank and device; each slab
+ * runs the same stage kernels on its own planes with the whole mesh's cell widths and
+ * coordinates, and its z ghost planes on a side that borders another slab come from that
+ * slab (periodic z: every side). The results are bitwise those of the whole mesh.
+ * chq_slab_create: slab `rank` of `nslab` of the mesh cfg describes (3-D, nx3 a multiple of
+ * nslab, at least nghost planes per slab, no RKL2 or cooling). A slab steps only through
+ * the calls below: chq_prime, chq_stage, chq_cycles and batches reject it. Its FOFC repair
+ * scans every face (it reads the neighbouring slabs' flags, which its cell list lacks).
+ * Order of one cycle on every slab, `x` marking where the caller moves data between slabs:
+ *   chq_slab_begin
+ *   for stage s = 1..nstage:
+ *     chq_slab_stage(s, 0)   fluxes .. update, FOFC flags
+ *     x  nbad = sum over slabs of nbad; FOFC message (what 1) of the stage's output buffer
+ *        out (1 for stages before the last, 0 for the last): pack(1, out, side) -> the
+ *        neighbour's unpack(1, out, other side). It carries the boundary plane's flags and
+ *        face fields (the repair of a face next to another slab reads both) and crosses
+ *        internal slab boundaries only (at the periodic wrap, between the last and the
+ *        first slab, the whole mesh's repair sees ghost cells: there pack and unpack of
+ *        what 1 do nothing and the message need not be sent)
+ *     chq_slab_stage(s, 1)   FOFC repair and re-runs, x/y ghosts, physical z sides
+ *     x  state planes of buffer out (what 0) exchanged the same way
+ *     chq_slab_stage(s, 2)   con2prim (dt and density minima at the last stage)
+ *   x  mdt_bits (and rho_bits with explicit diffusion) = minimum over slabs
+ *   chq_slab_end
+ * and to prime: chq_slab_prime(t, 0); x state planes of buffer 0; chq_slab_prime(t, 1);
+ * x minima; chq_slab_prime(t, 2). The step-control words live in device memory
+ * (chq_slab_ctl: int nbad; mdt_bits and rho_bits, non-negative doubles as 64-bit integers,
+ * so an integer minimum is the double minimum). A message for `side` packs the planes the
+ * neighbour on that side needs; chq_slab_halo_bytes gives its size (8-byte aligned device
+ * buffers). info = rank, nslab, lower side is a slab, upper side is a slab, first plane. */
+CHQ_API int chq_slab_create(const chq_config *cfg, int nslab, int rank, chq_mesh **out);
+CHQ_API int chq_slab_info(const chq_mesh *m, int info[5]);
+CHQ_API int chq_slab_halo_bytes(chq_mesh *m, int what, int side, long long *bytes);
+CHQ_API int chq_slab_pack(chq_mesh *m, int what, int buf, int side, void *dev, void *stream);
+CHQ_API int chq_slab_unpack(chq_mesh *m, int what, int buf, int side, const void *dev, void *stream);
+CHQ_API int chq_slab_ctl(chq_mesh *m, int **nbad, unsigned long long **mdt_bits, unsigned long long **rho_bits);
+CHQ_API int chq_slab_prime(chq_mesh *m, double t, int part, void *stream);
+CHQ_API int chq_slab_begin(chq_mesh *m, void *stream);
+CHQ_API int chq_slab_stage(chq_mesh *m, int stage, int part, void *stream);
+CHQ_API int chq_slab_end(chq_mesh *m, void *stream);
+
 /* ---- history sums without any device allocation --------------------------------------------
  * No counterpart in the reference. For callers that cannot allocate device memory: an
  * application whose memory belongs to its own pool or framework allocator (for example a
