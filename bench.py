@@ -184,6 +184,7 @@ def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, pro
     default_len = mesh.seglen
     tune = mesh.autotune()
     tune["default"] = default_len
+    tune["yz"] = mesh.autotune_yz()   # y/z staging: cp.async (0) or TMA (1), FP64 streaming PPM
     mesh.cycles(warmup)
     mesh.clock()
     l0 = mesh.kernel_launches()
@@ -389,7 +390,12 @@ def tune_summary(tune):
     d = tune.get("default", 16)
     out = {"default_seglen": d, "seglen": tune["seglen"], "flux_ms_per_launch": {str(k): v for k, v in ms.items()},
            "xvar": tune.get("xvar", 0), "flux_ms_per_xvar": {str(k): v for k, v in tune.get("xvar_ms", {}).items()}}
-    best = min([t for t in list(ms.values()) + list(tune.get("xvar_ms", {}).values()) if t > 0], default=-1)
+    yz = tune.get("yz")
+    if yz:
+        out["yz_staging"] = {"chosen": "tma" if yz["yzvar"] == 1 else "cp.async",
+                             "flux_ms_per_launch": {"cp.async": yz["ms"][0], "tma": yz["ms"][1]}}
+    best = min([t for t in list(ms.values()) + list(tune.get("xvar_ms", {}).values()) +
+                (list(yz["ms"].values()) if yz else []) if t > 0], default=-1)
     if ms.get(d, -1) > 0 and best > 0:
         out["speedup_vs_default"] = ms[d] / best
     return out
@@ -724,6 +730,8 @@ def serving_study(args, dist, rank, world) -> dict:
         for r in args.srv_rates.split(","):
             out.append(serving(args.srv_jobs, float(r), prec, 77, t_end=(0.05, 0.5), nmax2=1024, nmax3=192, cps=8,
                                dist=dist, rank=rank, world=world, one_at_a_time=True))
+            if rank == 0:   # each leg as it completes (a long study may be cut short)
+                print(json.dumps({"serving_leg": out[-1]}), file=sys.stderr, flush=True)
     return {"serving_study": out}
 
 

@@ -84,6 +84,9 @@ SIGNATURES = [
     ("chq_autotune2", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, _D]),
     ("chq_set_xvariant", C.c_int, [_P, C.c_int]),
     ("chq_get_xvariant", C.c_int, [_P]),
+    ("chq_set_yzvariant", C.c_int, [_P, C.c_int]),
+    ("chq_get_yzvariant", C.c_int, [_P]),
+    ("chq_autotune_yz", C.c_int, [_P, C.POINTER(C.c_int), _D]),
     ("chq_history", C.c_int, [_P, _D, _P]),
     ("chq_history_record", C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int]),
     ("chq_history_drain", C.c_int, [_P, _D, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
@@ -361,6 +364,22 @@ class Mesh:
     @xvariant.setter
     def xvariant(self, v: int) -> None:
         _check(load_library().chq_set_xvariant(self._h, int(v)))
+
+    @property
+    def yzvariant(self) -> int:
+        return int(load_library().chq_get_yzvariant(self._h))
+
+    @yzvariant.setter
+    def yzvariant(self, v: int) -> None:
+        _check(load_library().chq_set_yzvariant(self._h, int(v)))
+
+    def autotune_yz(self) -> dict:
+        """Time the y/z staging variants (cp.async, TMA) of the FP64 streaming-PPM flux launch
+        on this mesh's state and keep the faster: {"yzvar": chosen, "ms": {0: ms, 1: ms}}."""
+        v = C.c_int()
+        ms = np.zeros(2)
+        _check(load_library().chq_autotune_yz(self._h, C.byref(v), _dptr(ms)))
+        return {"yzvar": v.value, "ms": {0: float(ms[0]), 1: float(ms[1])}}
 
     @property
     def seglen(self) -> int:

@@ -19,6 +19,7 @@
 //             unlimited interface value to the next cell). z warps come first, then y.
 // The batched forms (flux_x_batched, flux_yz_batched) run the same sweeps for many meshes.
 #pragma once
+#include <cuda.h>   // CUtensorMap (the TMA descriptor type; no driver call is made from here)
 #include "chq_common.cuh"
 #include "chq_recon.cuh"
 #include "chq_riemann.cuh"
@@ -48,6 +49,16 @@ template <class P> struct FluxArgs {
   int nchunk;          // 32-wide i chunks for y/z sweeps (aligned to i = 0)
   int xvar;            // x-sweep kernel variant (register cap, FluxMinBlocks); picked by the autotuner
   const int *skip;     // optional device flag: nonzero -> kernel returns immediately
+  int yzvar;           // y/z staging of the FP64 streaming-PPM march: 0 cp.async, 1 TMA (autotuner)
+  const void *yzmaps;  // host copy of the two tensor maps of the TMA staging (YzMaps), or null
+  int *err;            // device error word: a TMA wait that gave up sets it (and its warp stops)
+};
+
+// Tensor maps of the TMA staging: the primitives w (6 components) and the centred field bcc
+// (3 components) of one mesh as 4-D tensors (i over the row pitch, j, k, component), boxes of
+// one 32-cell row segment of one component.
+struct YzMaps {
+  CUtensorMap w, b;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -232,6 +243,42 @@ CHQ_D void cp_async_elem(float *dst, const float *src) {
 CHQ_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 CHQ_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Tensor-memory-access (TMA) staging: an mbarrier in shared memory counts the bytes the
+// bulk tensor copies deliver (complete_tx); threads wait on its phase parity.
+CHQ_D unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+CHQ_D void mbar_init(unsigned long long *mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(mb)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+CHQ_D void mbar_expect_tx(unsigned long long *mb, unsigned bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_addr(mb)),
+               "r"(bytes)
+               : "memory");
+}
+// bounded wait for the phase of the given parity; false when the limit ran out
+CHQ_D bool mbar_wait(unsigned long long *mb, unsigned parity) {
+  const unsigned a = smem_addr(mb);
+  for (int it = 0; it < (1 << 24); ++it) {
+    unsigned ok = 0;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(a), "r"(parity)
+                 : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+// generic-proxy accesses of shared memory before the async-proxy writes that follow
+CHQ_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// one box of a 4-D tensor map (no multicast) into shared memory, completing on mb
+CHQ_D void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, unsigned long long *mb) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(mb))
+      : "memory");
+}
+
 // Threads per block of the y/z kernels (the stride of their shared-memory columns).
 #ifndef CHQ_FLUXYZ_THREADS
 #define CHQ_FLUXYZ_THREADS 128
@@ -413,8 +460,14 @@ struct PpmWin {
   }
 };
 
-template <int S, class P>
-CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
+// TMA (FP64 only, maps and mbar given): instead of one cp.async per quantity and thread, one
+// lane of the warp issues, one cell ahead, eight bulk tensor copies of the next cell's 32-wide
+// row of each quantity straight into the warp's rows of the window's q_{c+2} slots; the warp
+// waits on its mbarrier's phase. Same slots, same values: the states are bitwise those of the
+// cp.async form.
+template <int S, class P, bool TMA = false>
+CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win, const YzMaps *maps = nullptr,
+                        unsigned long long *mbar = nullptr) {
   const int lane = threadIdx.x & 31;
   const int nseg = A.nseg[d];
   const int nchunk = A.nchunk;
@@ -423,7 +476,14 @@ CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   const int seg = (int)(rest % nseg);
   const int outer = (int)(rest / nseg);
   const int i = 32 * chunk + lane;
-  if (i < A.lo[d][2] || i > A.hi[d][2]) return;
+  const bool act = !(i < A.lo[d][2] || i > A.hi[d][2]);
+  unsigned mask = 0xffffffffu;
+  bool leader = false;
+  if constexpr (TMA) {
+    mask = __ballot_sync(0xffffffffu, act);
+    leader = act && (lane == __ffs(mask) - 1);
+  }
+  if (!act) return;
   const int sweep_lo = (d == 1) ? A.lo[1][1] : A.lo[2][0];
   const int sweep_hi = (d == 1) ? A.hi[1][1] : A.hi[2][0];
   const int f0 = sweep_lo + A.seglen * seg;
@@ -435,6 +495,27 @@ CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   P *col = win + t;
   constexpr bool PFB = (sizeof(P) == 8);
   double *bnw = reinterpret_cast<double *>(win + PpmWin::nslot * kYzThreads) + t;
+  // TMA staging: this warp's mbarrier, its rows of the q_{c+2} slots, the tensor coordinates
+  unsigned long long *mb = TMA ? mbar + (t >> 5) : nullptr;
+  unsigned phase = 0;
+  const int outer_idx = (d == 1) ? A.lo[1][0] + outer : A.lo[2][1] + outer;
+  auto issue = [&](int pos) {   // the rows of the cell at sweep position pos, all 8 quantities
+    mbar_expect_tx(mb, 8u * 32u * (unsigned)sizeof(P));
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      // component of quantity n in w (0, 1, 2, 3, 4, 7) or bcc (5, 6), as dir_view orders them
+      const int comp = (n == 0) ? IDN : (n == 1) ? IVX + d : (n == 2) ? IVX + (d + 1) % 3 : (n == 3) ? IVX + (d + 2) % 3
+                     : (n == 4) ? IPR : (n == 5) ? (d + 1) % 3 : (n == 6) ? (d + 2) % 3 : IENT;
+      const CUtensorMap *map = (n == 5 || n == 6) ? &maps->b : &maps->w;
+      P *row = win + (PpmWin::off(n) + PpmWin::Q2) * kYzThreads + (t & ~31);
+      if (d == 1) tma_load_4d(row, map, 32 * chunk, pos, outer_idx, comp, mb);
+      else tma_load_4d(row, map, 32 * chunk, outer_idx, pos, comp, mb);
+    }
+  };
+  if constexpr (TMA) {
+    if (leader) mbar_init(mb, 1);
+    __syncwarp(mask);
+  }
 #define CHQ_SLOT(n, k) col[(PpmWin::off(n) + PpmWin::k) * kYzThreads]
   // cell f0-1: its slope, its left interface value and the window, from direct loads
 #pragma unroll
@@ -451,14 +532,26 @@ CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
       CHQ_SLOT(4, X1) = qm2;
       CHQ_SLOT(4, X2) = qm1;
     }
-    cp_async_elem(&CHQ_SLOT(n, Q2), src + 2 * st);
+    if constexpr (!TMA) cp_async_elem(&CHQ_SLOT(n, Q2), src + 2 * st);
   }
   cp_async_commit();
+  if constexpr (TMA) {
+    if (leader) issue(f0 + 1);
+  }
   P wl[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) wl[n] = P(0);
   for (int f = f0 - 1; f <= f1; ++f, lc += st) {
     cp_async_wait_all();
+    if constexpr (TMA) {
+      // q_{c+2} rows of this cell: the warp gives up together if the copies never land
+      const bool ok = __all_sync(mask, mbar_wait(mb, phase & 1u));
+      ++phase;
+      if (!ok) {
+        if (leader && A.err) atomicExch(A.err, 3);
+        return;
+      }
+    }
     const bool pre = (f < f1);
     P bnv = P(0);
     if constexpr (PFB) {
@@ -495,9 +588,20 @@ CHQ_D void sweep_yz_ppm(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
       CHQ_SLOT(n, Q1) = q2;
       CHQ_SLOT(n, S) = sp;
       CHQ_SLOT(n, F) = fp;
-      if (pre) cp_async_elem(&CHQ_SLOT(n, Q2), V.src[n] + lc + 3 * st);
+      if constexpr (!TMA) {
+        if (pre) cp_async_elem(&CHQ_SLOT(n, Q2), V.src[n] + lc + 3 * st);
+      }
     }
     cp_async_commit();
+    if constexpr (TMA) {
+      if (pre) {
+        __syncwarp(mask);   // every lane has read its q_{c+2} slots before the copies overwrite them
+        if (leader) {
+          fence_proxy_async();
+          issue(f + 3);
+        }
+      }
+    }
     finish_states<R_PPM, P>(A, aL, aR, qc, p5, um1, up1);
 #pragma unroll
     for (int n = 0; n < 8; ++n) park[n * kYzThreads + t] = aR[n];
@@ -629,6 +733,24 @@ __global__ void __launch_bounds__(kYzThreads, FluxYzMinBlocks<P>::v) flux_yz_ker
   const int nz = (int)A.nwarp[2], nyz = (int)(A.nwarp[2] + A.nwarp[1]);
   if (wid < nz) sweep_yz<R, S, CHAR, true, P>(A, 2, wid, park, win);
   else if (wid < nyz) sweep_yz<R, S, CHAR, true, P>(A, 1, wid - nz, park, win);
+}
+
+// The FP64 streaming-PPM y/z kernel with TMA staging (FluxArgs::yzvar = 1): dynamic shared
+// memory of flux_yz_kernel plus one mbarrier per warp; the tensor maps are kernel parameters.
+constexpr size_t flux_yz_tma_smem() { return flux_yz_smem<R_PPM, double>() + (kYzThreads / 32) * sizeof(unsigned long long); }
+
+template <int S>
+__global__ void __launch_bounds__(kYzThreads, FluxYzMinBlocks<double>::v)
+    flux_yz_tma_kernel(const __grid_constant__ FluxArgs<double> A, const __grid_constant__ YzMaps maps) {
+  extern __shared__ __align__(128) unsigned char flux_tma_dsm[];
+  double *park = reinterpret_cast<double *>(flux_tma_dsm);
+  double *win = park + 8 * kYzThreads;
+  unsigned long long *mbar = reinterpret_cast<unsigned long long *>(flux_tma_dsm + flux_yz_smem<R_PPM, double>());
+  if (A.skip && *A.skip) return;
+  const int wid = (int)blockIdx.x * (kYzThreads / 32) + (int)(threadIdx.x >> 5);
+  const int nz = (int)A.nwarp[2], nyz = (int)(A.nwarp[2] + A.nwarp[1]);
+  if (wid < nz) sweep_yz_ppm<S, double, true>(A, 2, wid, park, win, &maps, mbar);
+  else if (wid < nyz) sweep_yz_ppm<S, double, true>(A, 1, wid - nz, park, win, &maps, mbar);
 }
 
 // batched forms: the blocks of many meshes in one launch per sweep kind (chq_batch); each

@@ -1,5 +1,6 @@
 // chasqui_b200 — instantiation unit of the face-flux kernel for one (precision, scheme).
 // Compiled once per pair with -DCHQ_P=<double|float> -DCHQ_R=<0..4>.
+#include <cstring>
 #include "chq_launch.h"
 
 #ifndef CHQ_P
@@ -29,7 +30,23 @@ template <int S, bool C>
 static cudaError_t go(const FluxArgs<CHQ_P> &a, unsigned, cudaStream_t s) {
   constexpr int wpb = kYzThreads / 32;
   const unsigned nyz = (unsigned)((a.nwarp[1] + a.nwarp[2] + wpb - 1) / wpb), nx = (unsigned)((a.nwarp[0] + 3) / 4);
-  if (nyz) {
+  bool yz_done = false;
+  if constexpr (CHQ_R == R_PPM && !C && sizeof(CHQ_P) == 8) {
+    // TMA staging of the streaming-PPM march (picked by the autotuner; FP64 only)
+    if (nyz && a.yzvar == 1 && a.yzmaps) {
+      constexpr size_t smem = flux_yz_tma_smem();
+      static bool ready_tma[64] = {};
+      const cudaError_t ea = allow_smem(flux_yz_tma_kernel<S>, smem, ready_tma);
+      if (ea != cudaSuccess) return ea;
+      YzMaps maps;
+      std::memcpy(&maps, a.yzmaps, sizeof(maps));
+      flux_yz_tma_kernel<S><<<nyz, kYzThreads, smem, s>>>(a, maps);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      yz_done = true;
+    }
+  }
+  if (nyz && !yz_done) {
     constexpr size_t smem = flux_yz_smem<CHQ_R, CHQ_P>();
     static bool ready[64] = {};
     const cudaError_t ea = allow_smem(flux_yz_kernel<CHQ_R, S, C, CHQ_P>, smem, ready);

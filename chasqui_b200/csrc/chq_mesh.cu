@@ -5,6 +5,7 @@
 // reference's Stage() (src/main.cpp:46-93) with the host synchronisations removed: the
 // time step, the FOFC decision and all counters live in a device StepCtl.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -202,6 +203,11 @@ struct chq_mesh {
   int act_lo[3][3], act_hi[3][3];
   int seglen;
   int xvar = 0;   // x-sweep kernel variant (register cap), chq_autotune
+  // y/z staging of the FP64 streaming-PPM march: 0 cp.async, 1 TMA (chq_autotune_yz); the
+  // tensor maps over w and bcc are encoded at creation when the driver offers the encoder
+  int yzvar = 0;
+  bool tma_ok = false;
+  YzMaps tmaps;
   // z slab of a decomposed mesh (chq_slab_create): the lower / upper z side borders another
   // slab (its ghosts come from chq_slab_unpack, not from the boundary kernel); slab geometry
   int zpeer[2] = {0, 0};
@@ -353,6 +359,9 @@ FluxArgs<P> flux_args(chq_mesh *m, int cur, unsigned dirmask) {
   a.lhlld_phi = m->cfg.lhlld_phi;
   a.seglen = m->seglen;
   a.xvar = m->xvar;
+  a.yzvar = m->tma_ok ? m->yzvar : 0;
+  a.yzmaps = m->tma_ok ? &m->tmaps : nullptr;
+  a.err = &m->ctl->err;
   a.nchunk = (m->g.ni + 1 + 31) / 32;
   // x: rows x segments of XFaces faces (29 for streaming PPM, else 31); y/z: i chunks x
   // outer x segments
@@ -2002,6 +2011,53 @@ void chq_config_defaults(chq_config *c) {
 }  // extern "C"
 
 namespace {
+// The driver's tensor-map encoder, looked up once through the runtime (no -lcuda link).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tensor maps of the FP64 y/z TMA staging over this mesh's own w (6 components) and bcc (3):
+// 4-D (i over the row pitch, j, k, component), box = one 32-cell row segment of one component.
+// The base addresses are 256-byte aligned, strides are multiples of 256 bytes and every box
+// starts at i = 32 * chunk (256 bytes), which the bulk tensor copy requires (16 bytes).
+bool encode_yz_maps(chq_mesh *m) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const Geom &g = m->g;
+  const cuuint64_t stride[3] = {(cuuint64_t)g.sj * 8, (cuuint64_t)g.sk * 8, (cuuint64_t)g.vstride * 8};
+  const cuuint32_t box[4] = {32, 1, 1, 1}, estr[4] = {1, 1, 1, 1};
+  const cuuint64_t dw[4] = {(cuuint64_t)g.sj, (cuuint64_t)g.nj + 1, (cuuint64_t)g.nk + 1, 6};
+  const cuuint64_t db[4] = {(cuuint64_t)g.sj, (cuuint64_t)g.nj + 1, (cuuint64_t)g.nk + 1, 3};
+  CUresult r = enc(&m->tmaps.w, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, m->w, dw, stride, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r == CUDA_SUCCESS)
+    r = enc(&m->tmaps.b, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, m->bcc, db, stride, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+// the TMA staging variant exists for FP64 streaming PPM (no characteristic projection)
+bool yz_tma_applies(const chq_mesh *m) {
+  return m->tma_ok && !m->mixed && m->cfg.recon == R_PPM && !m->cfg.characteristic;
+}
+
+namespace {
 // A whole mesh (nslab = 1) or z slab `rank` of `nslab` equal slabs of the mesh cfg describes:
 // the slab holds nx3 / nslab active planes, keeps the whole mesh's x3 extent, cell width and
 // coordinates (Geom::koff), and marks the z sides that border another slab.
@@ -2186,6 +2242,7 @@ int mesh_create_impl(const chq_config *cfg, int nslab, int rank, chq_mesh **out)
     chq_mesh_destroy(m);
     return cuda_fail(e, "mesh initialisation");
   }
+  if (!m->mixed && g.two_d) m->tma_ok = encode_yz_maps(m);
   *out = m;
   return CHQ_OK;
 }
@@ -3143,6 +3200,17 @@ int chq_set_xvariant(chq_mesh *m, int xvar) {
 
 int chq_get_xvariant(const chq_mesh *m) { return m ? m->xvar : -1; }
 
+int chq_set_yzvariant(chq_mesh *m, int yzvar) {
+  if (!m || yzvar < 0 || yzvar > 1) return fail(CHQ_ERR_ARG, "y/z staging variant out of range");
+  if (yzvar == 1 && !yz_tma_applies(m))
+    return fail(CHQ_ERR_ARG, "TMA staging applies to 3-D FP64 meshes with PPM without characteristic projection");
+  if (yzvar != m->yzvar) drop_cycle_graph(m);
+  m->yzvar = yzvar;
+  return CHQ_OK;
+}
+
+int chq_get_yzvariant(const chq_mesh *m) { return m ? m->yzvar : -1; }
+
 }  // extern "C"
 
 namespace {
@@ -3278,6 +3346,38 @@ int chq_autotune2(chq_mesh *m, int *seglen, int *xvar, double ms_len[CHQ_TUNE_NL
 
 int chq_autotune(chq_mesh *m, int *seglen, double ms[CHQ_TUNE_NLEN]) {
   return chq_autotune2(m, seglen, nullptr, ms, nullptr);
+}
+
+int chq_autotune_yz(chq_mesh *m, int *yzvar, double ms[2]) {
+  if (!m) return fail(CHQ_ERR_ARG, "null mesh");
+  if (ms) ms[0] = ms[1] = -1.0;
+  if (!yz_tma_applies(m)) {
+    if (yzvar) *yzvar = m->yzvar;
+    return CHQ_OK;
+  }
+  drop_cycle_graph(m);
+  cudaStream_t s = S(m, nullptr);
+  double t[2] = {0.0, 0.0};
+  const int keep = m->yzvar;
+  for (int v = 0; v < 2; ++v) {
+    m->yzvar = v;
+    const int rc = time_launches(s, 3, [&] { return do_fluxes(m, 0, 7u, nullptr, s); }, &t[v]);
+    if (rc != CHQ_OK) {
+      m->yzvar = keep;
+      return rc;
+    }
+  }
+  // a TMA wait that gave up marks the step control: keep the cp.async form then
+  StepCtl h;
+  CHQ_CUDA(cudaMemcpyAsync(&h, m->ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CHQ_CUDA(cudaStreamSynchronize(s));
+  m->yzvar = (h.err == 0 && t[1] < t[0]) ? 1 : 0;
+  if (ms) {
+    ms[0] = t[0];
+    ms[1] = t[1];
+  }
+  if (yzvar) *yzvar = m->yzvar;
+  return CHQ_OK;
 }
 
 int chq_batch_autotune(chq_batch *B, int *seglen, int *xvar, double ms_len[CHQ_TUNE_NLEN],

@@ -249,6 +249,15 @@ CHQ_API int chq_set_seglen(chq_mesh *m, int seglen);
 CHQ_API int chq_get_seglen(const chq_mesh *m);
 CHQ_API int chq_set_xvariant(chq_mesh *m, int xvar);
 CHQ_API int chq_get_xvariant(const chq_mesh *m);
+/* y/z staging of the FP64 streaming-PPM march (2-D and 3-D meshes, PPM without characteristic
+ * projection): 0 (default) copies each thread's next stencil values with cp.async, 1 lets one
+ * lane per warp fetch the next cell's 32-cell rows with bulk tensor copies (TMA) over the
+ * mesh's own arrays. Same results bit for bit. chq_autotune_yz times both on the mesh's state
+ * (call after chq_prime and chq_autotune2) and keeps the faster (ms[v] = ms per flux launch
+ * of variant v; -1 where the variant does not apply). No counterpart in the reference. */
+CHQ_API int chq_set_yzvariant(chq_mesh *m, int yzvar);
+CHQ_API int chq_get_yzvariant(const chq_mesh *m);
+CHQ_API int chq_autotune_yz(chq_mesh *m, int *yzvar, double ms[2]);
 /* Synchronises; totals in ms and launch counts per kind since the last reset. */
 CHQ_API int chq_profile_read(chq_mesh *m, double ms[CHQ_NPROF], long long launches[CHQ_NPROF], int reset);
 

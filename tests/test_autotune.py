@@ -93,3 +93,42 @@ def test_batch_autotune_keeps_members_bitwise_equal_to_solo_runs():
         for f in FIELDS:
             assert np.array_equal(m.get(f), a.get(f)), (j, f)
     b.close()
+
+
+@pytest.mark.parametrize("text,ov", [(cases.blast(20), []), (cases.ot(48), []),
+                                     (cases.blast(16), ["problem.pres_in=1e4", "problem.pres_out=1e-3",
+                                                        "time.cfl=0.5"])],
+                         ids=["blast3d_ppm", "ot2d_ppm", "blast3d_strong_fofc"])
+def test_tma_staging_gives_the_same_bits(text, ov):
+    """chq_set_yzvariant(1): the FP64 streaming-PPM march fetches its stencil rows with bulk
+    tensor copies instead of per-thread cp.async; same slots, same values, same results"""
+    out = {}
+    for v, L in ((0, 16), (1, 16), (1, 4), (1, 64)):
+        ref, mesh = make_pair(text, ov)
+        copy_state(ref, mesh, FIELDS)
+        mesh.seglen = L
+        mesh.yzvariant = v
+        assert mesh.yzvariant == v
+        mesh.prime(0.0)
+        mesh.cycles(6)
+        out[(v, L)] = {f: mesh.get(f) for f in FIELDS}
+        ref.close()
+    for k in ((1, 16), (1, 4), (1, 64)):
+        for f in FIELDS:
+            assert np.array_equal(out[k][f], out[(0, 16)][f]), (k, f)
+
+
+def test_tma_staging_is_tuned_and_limited_to_fp64_ppm():
+    ref, mesh = make_pair(cases.blast(24), [])
+    copy_state(ref, mesh, FIELDS)
+    mesh.prime(0.0)
+    r = mesh.autotune_yz()
+    assert r["ms"][0] > 0 and r["ms"][1] > 0
+    assert mesh.yzvariant == r["yzvar"] == (1 if r["ms"][1] < r["ms"][0] else 0)
+    from chasqui_b200 import ChqError
+    for ov, prec in ((["mhd.reconstruct=wenoz"], "fp64"), ([], "mixed"), (["mhd.characteristic=true"], "fp64")):
+        _, other = make_pair(cases.blast(16), ov, precision=prec)
+        with pytest.raises(ChqError):
+            other.yzvariant = 1
+        assert other.autotune_yz()["ms"] == {0: -1.0, 1: -1.0}
+    ref.close()
