@@ -527,6 +527,10 @@ template <class P> struct LimitArgs {
   long nface[3];
   long long *count;
   const int *done;
+  // limited faces counted per direction only for k in [kcount[d][0], kcount[d][1]]: a z slab
+  // also limits the transverse faces of the ghost plane next to another slab (their mass
+  // fluxes steer that plane's edge EMFs), which the neighbouring slab owns and counts
+  int kcount[3][2];
 };
 
 template <class P> CHQ_D void cell_flux6(const MState<P> &s, P bn, P sent, P gm1, P gamma, P fc[6], P uc[6], P &cf) {
@@ -616,6 +620,7 @@ template <class P> CHQ_D void limit_body(const LimitArgs<P> &A, int bx) {
       if (d == 0) lim = limit_face<0, P>(A, k, j, i, bdt);
       else if (d == 1) lim = limit_face<1, P>(A, k, j, i, bdt);
       else lim = limit_face<2, P>(A, k, j, i, bdt);
+      if (k < A.kcount[d][0] || k > A.kcount[d][1]) lim = 0;
       t = -1;
     } else if (t >= 0) {
       t -= (int)A.nface[d];

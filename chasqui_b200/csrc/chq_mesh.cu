@@ -623,6 +623,16 @@ LimitArgs<P> limit_args(chq_mesh *m, unsigned dirmask, double bdt, const double 
   for (int d = 0; d < 3; ++d) {
     a.flx[d] = as<P>(m->flx[d]);
     for (int q = 0; q < 3; ++q) { a.lo[d][q] = m->act_lo[d][q]; a.hi[d][q] = m->act_hi[d][q]; }
+    a.kcount[d][0] = a.lo[d][0];
+    a.kcount[d][1] = a.hi[d][0];
+    if (d < 2) {
+      // across an internal slab boundary the transverse faces of the ghost plane are active
+      // faces of the whole mesh
+      a.lo[d][0] -= m->fofc_ext[0];
+      a.hi[d][0] += m->fofc_ext[1];
+    } else if (m->fofc_ext[1]) {
+      a.kcount[d][1] -= 1;   // the face shared with the upper slab is counted there
+    }
     const bool on = m->active[d] && ((dirmask >> d) & 1);
     a.nface[d] = on ? (long)(a.hi[d][0] - a.lo[d][0] + 1) * (a.hi[d][1] - a.lo[d][1] + 1) * (a.hi[d][2] - a.lo[d][2] + 1) : 0;
     tot += a.nface[d];

@@ -145,3 +145,10 @@ def test_slab_rejects_whole_mesh_stepping():
     with pytest.raises(ChqError):
         s.cycles(1)
     s.close()
+
+
+@pytest.mark.parametrize("integrator", [1, 2, 4])
+def test_other_integrators_and_the_limiter(integrator):
+    """rk1, rk2 and SSPRK(4,3): other stage tables and output buffers; the positivity limiter
+    on (per-slab counts, no exchange needed)"""
+    _compare(_cfg(24, integrator=integrator, cfl=0.3 if integrator < 4 else 0.5, flux_limiter=1), 3, STRONG, 5)
