@@ -384,11 +384,12 @@ CHQ_D void sweep_x(const FluxArgs<P> &A, int wid) {
 #pragma unroll
   for (int n = 0; n < 8; ++n) { aL[n] = P(0); aR[n] = P(0); }
   const int lc = A.g.idx32(k, j, c);
+  const P bnf = have ? P(ldg(V.bn + lc)) : P(0);   // loaded before the reconstruction
   if (have) cell_states<R, CHAR, P>(A, V, lc, aL, aR);
   P wl[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) wl[n] = __shfl_up_sync(0xffffffffu, aR[n], 1);
-  if (have && lane > 0) face_flux<S, P>(A, V, lc, wl, aL);
+  if (have && lane > 0) face_flux<S, P>(A, V, lc, wl, aL, bnf);
 }
 
 // Faces per x-sweep warp: 31 in the per-cell form (lane 0 contributes only its right state),
@@ -420,6 +421,7 @@ CHQ_D void sweep_x_ppm(const FluxArgs<P> &A, int wid) {
             cp2 = min(c + 2, last);
   const int base = A.g.idx32(k, j, 0);
   const DirView<P> V = dir_view(A, 0);
+  const P bnf = P(ldg(V.bn + base + c0));   // this lane's face-normal field, loaded before the reconstruction
   P aL[8], aR[8], qc[8], p5[5], um1 = P(0), up1 = P(0);
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
@@ -440,7 +442,7 @@ CHQ_D void sweep_x_ppm(const FluxArgs<P> &A, int wid) {
   P wl[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) wl[n] = __shfl_up_sync(0xffffffffu, aR[n], 1);
-  if (lane >= 2 && lane <= 30 && c <= A.hi[0][2]) face_flux<S, P>(A, V, base + c, wl, aL);
+  if (lane >= 2 && lane <= 30 && c <= A.hi[0][2]) face_flux<S, P>(A, V, base + c, wl, aL, bnf);
 }
 
 // Streaming PPM along a y/z march. Each thread's shared-memory column keeps, per quantity,
@@ -651,6 +653,10 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   constexpr int RE = Reach<R>::v;
   constexpr bool use_win = WIN && (RE > 0);
   P *col = use_win ? win + t : nullptr;
+  // FP64: the next face's normal field copied one cell ahead into two alternating slots
+  // after the window (as in the streaming-PPM march)
+  constexpr bool PFB = use_win && (sizeof(P) == 8);
+  double *bnw = PFB ? reinterpret_cast<double *>(win + 8 * (2 * RE + 1) * kYzThreads) + t : nullptr;
   if constexpr (use_win) {
     // window of cell f0-1: q[c-RE .. c+RE-1] now, q[c+RE] asynchronously
 #pragma unroll
@@ -664,8 +670,13 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
   }
   for (int f = f0 - 1; f <= f1; ++f, lc += V.st) {
     P aL[8], aR[8];
+    P bnv = P(0);
     if constexpr (use_win) {
       cp_async_wait_all();
+      if constexpr (PFB) {
+        if (f >= f0) bnv = P(bnw[(f & 1) * kYzThreads]);
+        if (f < f1) cp_async_elem(bnw + ((f + 1) & 1) * kYzThreads, V.bn + lc + V.st);
+      }
       cell_states_from<R, CHAR, P>(A, V, lc, aL, aR, WindowStencil<RE, P>{col, V, lc, f < f1});
       cp_async_commit();
     } else {
@@ -673,7 +684,10 @@ CHQ_D void sweep_yz(const FluxArgs<P> &A, int d, int wid, P *park, P *win) {
     }
 #pragma unroll
     for (int n = 0; n < 8; ++n) park[n * kYzThreads + t] = aR[n];
-    if (f >= f0) face_flux<S, P>(A, V, lc, wl, aL);
+    if (f >= f0) {
+      if constexpr (PFB) face_flux<S, P>(A, V, lc, wl, aL, bnv);
+      else face_flux<S, P>(A, V, lc, wl, aL);
+    }
 #pragma unroll
     for (int n = 0; n < 8; ++n) wl[n] = park[n * kYzThreads + t];
   }
@@ -707,10 +721,10 @@ template <class P> struct FluxYzMinBlocks { static constexpr int v = (sizeof(P) 
 
 template <int R, class P> __host__ __device__ constexpr size_t flux_yz_smem() {
   // park (8) + window: streaming PPM 43 slots (the characteristic PPM form uses 40 of them),
-  // otherwise 8 quantities x (2 reach + 1); streaming PPM in FP64 adds two face-field slots
+  // otherwise 8 quantities x (2 reach + 1); in FP64 every windowed march adds two face-field slots
   return (size_t)(8 + ((R == R_PPM) ? PpmWin::nslot : (Reach<R>::v > 0) ? 8 * (2 * Reach<R>::v + 1) : 0)) *
              kYzThreads * sizeof(P) +
-         ((R == R_PPM && sizeof(P) == 8) ? 2 * kYzThreads * sizeof(double) : 0);
+         ((Reach<R>::v > 0 && sizeof(P) == 8) ? 2 * kYzThreads * sizeof(double) : 0);
 }
 
 template <int R, int S, bool CHAR, class P, int V = 0>
