@@ -121,6 +121,7 @@ SIGNATURES = [
     ("chq_server_destroy", C.c_int, [_P]),
     ("chq_server_set_lanes", C.c_int, [_P, C.c_int]),
     ("chq_server_set_solo_cells", C.c_int, [_P, C.c_longlong]),
+    ("chq_server_set_solo_slots", C.c_int, [_P, C.c_int]),
     ("chq_server_set_autotune", C.c_int, [_P, C.c_int]),
     ("chq_history_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       _P, _P, _P, _P, _D, _P]),
@@ -481,7 +482,7 @@ class Server:
     """Continuous-batching simulation server (chq_server_*)."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 1024, cycles_per_step: int = 4, lanes: int = 8,
-                 solo_cells: int = None, autotune: bool = True):
+                 solo_cells: int = None, autotune: bool = False, solo_slots: int = None):
         h = _P()
         _check(load_library().chq_server_create(int(hbm_budget_bytes), max_active, cycles_per_step, C.byref(h)))
         _check(load_library().chq_server_set_autotune(h, int(bool(autotune))))
@@ -489,6 +490,8 @@ class Server:
         _check(load_library().chq_server_set_lanes(h, int(lanes)))
         if solo_cells is not None:
             _check(load_library().chq_server_set_solo_cells(h, int(solo_cells)))
+        if solo_slots is not None:
+            _check(load_library().chq_server_set_solo_slots(h, int(solo_slots)))
 
     def submit(self, cfg: chq_config, problem: str, params) -> int:
         a = np.ascontiguousarray(params, dtype=np.float64)

@@ -261,6 +261,40 @@ struct chq_mesh {
 
 namespace {
 
+// Mesh slabs and batch tables come from one stream-ordered memory pool per device. cudaFree
+// waits for the whole device, so a server that retired a job while others ran stalled them
+// all; a pool free is ordered on one stream only, and up to kPoolKeepBytes of freed blocks
+// stay in the pool for the next job's mesh (beyond that the pool returns memory to the
+// device at the next synchronisation).
+const uint64_t kPoolKeepBytes = 16ull << 30;
+
+cudaMemPool_t device_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = kPoolKeepBytes;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
+// stream-ordered allocation from the device's pool (the device's default pool if the
+// library's own could not be created)
+cudaError_t pool_alloc(void **ptr, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t p = device_pool();
+  return p ? cudaMallocFromPoolAsync(ptr, bytes, p, s) : cudaMallocAsync(ptr, bytes, s);
+}
+
 const int kHstBlocks = 1184;   // 8 blocks per SM on 148 SMs
 const size_t kBadCap = 1 << 16;            // flagged cells listed per stage
 const long kRepairBlocks = 1184;           // repair grid of one mesh
@@ -1652,7 +1686,8 @@ int batch_build(chq_batch *B) {
     o_sts_copy0 = push_vec(h, copy0);
   }
   const size_t o_status = h.push(std::vector<double>(3 * n + 1).data(), (3 * n + 1) * sizeof(double));
-  cudaError_t e = cudaMalloc(&B->dev, h.b.size());
+  // allocated and uploaded on the legacy default stream, which then completes both
+  cudaError_t e = pool_alloc(reinterpret_cast<void **>(&B->dev), h.b.size(), cudaStreamLegacy);
   if (e != cudaSuccess) return fail(CHQ_ERR_NOMEM, std::string("batch tables: ") + cudaGetErrorString(e));
   e = cudaMemcpy(B->dev, h.b.data(), h.b.size(), cudaMemcpyHostToDevice);
   // from pageable memory cudaMemcpy may return before the transfer has landed, and the
@@ -1975,7 +2010,7 @@ void batch_free(chq_batch *B) {
   B->done_evt = nullptr;
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
-  if (B->dev) cudaFree(B->dev);
+  if (B->dev) cudaFreeAsync(B->dev, cudaStreamLegacy);   // the batch's stream has drained
   if (B->sts_skip) cudaFree(B->sts_skip);
   if (B->sts_dyn) cudaFree(B->sts_dyn);
   B->sts_skip = nullptr;
@@ -2184,8 +2219,10 @@ int mesh_create_impl(const chq_config *cfg, int nslab, int rank, chq_mesh **out)
   m->hst_blocks = kHstBlocks;
   const size_t ctl_bytes = align_up(sizeof(StepCtl), 256);
   m->slab_bytes = slab_size(nel, m->psize, c.sts != 0);
-  cudaError_t e = cudaMalloc(&m->slab, m->slab_bytes);
+  cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = pool_alloc(reinterpret_cast<void **>(&m->slab), m->slab_bytes, m->stream);
   if (e != cudaSuccess) {
+    if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
     return fail(CHQ_ERR_NOMEM, std::string("device allocation of the mesh failed: ") + cudaGetErrorString(e));
   }
@@ -2221,8 +2258,7 @@ int mesh_create_impl(const chq_config *cfg, int nslab, int rank, chq_mesh **out)
     for (int d = 0; d < 3; ++d) { m->smbj[d] = (double *)p; p += dbytes; }
   }
   m->diff = (c.nu > 0 || c.kappa > 0 || c.eta > 0);
-  e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMemsetAsync(m->slab, 0, m->slab_bytes, m->stream);
+  e = cudaMemsetAsync(m->slab, 0, m->slab_bytes, m->stream);
   if (e == cudaSuccess) {
     StepCtl h{};
     h.tlim = c.tlim;
@@ -2297,7 +2333,9 @@ int chq_mesh_destroy(chq_mesh *m) {
   for (auto &p : m->pending) { m->pool.push_back(p.b); m->pool.push_back(p.e); }
   for (cudaEvent_t e : m->pool) cudaEventDestroy(e);
   for (cudaEvent_t e : m->slots) if (e) cudaEventDestroy(e);
-  if (m->slab) cudaFree(m->slab);
+  // every stream that used the slab has drained (above): return it to the pool in the mesh
+  // stream's order, without waiting for the rest of the device
+  if (m->slab) cudaFreeAsync(m->slab, m->stream);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   return CHQ_OK;

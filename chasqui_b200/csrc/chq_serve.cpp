@@ -15,7 +15,10 @@
 // Jobs of 2^21 cells or more (chq_server_set_solo_cells raises the threshold) are not
 // batched: each runs "solo" on its own mesh stream (replaying a CUDA graph of one cycle, except with RKL2) and the
 // server polls an event behind its chunk instead of waiting for it, so a large job never holds
-// up the lanes (or another large job). Diffusion (explicit or RKL2), cooling and gravity
+// up the lanes (or another large job). At most `solo_slots` solo jobs run at once (default 2,
+// chq_server_set_solo_slots): each fills the device alone, and more of them at once only
+// share it less efficiently; the others wait in the queue while smaller jobs behind them are
+// admitted into the lanes. Diffusion (explicit or RKL2), cooling and gravity
 // batch with jobs that have the same terms switched on.
 // Each job keeps its own dt and clock on the device, so its result is the same alone and in
 // any mix. Times are seconds on the server's steady clock.
@@ -110,7 +113,8 @@ struct chq_server {
   long long budget = 0, used = 0;
   int max_active = 0, cycles_per_step = 1, lanes = 8;
   long long solo_cells = 0;   // jobs of at least this many cells run unbatched
-  int autotune = 1;           // tune each new lane's batch (chq_batch_autotune)
+  int solo_slots = 2;         // solo jobs running at once
+  int autotune = 0;           // tune each new lane's batch (chq_batch_autotune); off by default
   long long next_id = 1;
   std::map<long long, Job *> jobs;
   std::vector<Job *> queue;
@@ -263,8 +267,10 @@ void admit(chq_server *S) {
   std::vector<Job *> still;
   int active = (int)S->solo.size();
   for (auto &kv : S->groups) active += (int)kv.second.members.size();
+  int solo_running = (int)S->solo.size();
   for (Job *j : S->queue) {
-    if (active >= S->max_active || S->used + j->bytes > S->budget) {
+    if (active >= S->max_active || S->used + j->bytes > S->budget ||
+        (j->cells >= S->solo_cells && solo_running >= S->solo_slots)) {
       still.push_back(j);
       continue;
     }
@@ -288,6 +294,7 @@ void admit(chq_server *S) {
       j->solo = true;
       S->solo.push_back(j);
       ++active;
+      ++solo_running;
       continue;
     }
     int lane = 0;
@@ -459,6 +466,12 @@ int chq_server_set_solo_cells(chq_server *S, long long cells) {
   // at 2^15 cells ended in a device fault whose cause is not known
   if (cells < kSoloCells) return err(CHQ_ERR_ARG, "the solo threshold must be at least 2^21 cells");
   S->solo_cells = cells;
+  return CHQ_OK;
+}
+
+int chq_server_set_solo_slots(chq_server *S, int slots) {
+  if (!S || slots < 1 || slots > 1024) return err(CHQ_ERR_ARG, "solo slots must be in [1, 1024]");
+  S->solo_slots = slots;
   return CHQ_OK;
 }
 

@@ -328,10 +328,14 @@ CHQ_API int chq_server_set_lanes(chq_server *s, int lanes);
 /* jobs of at least `cells` cells run unbatched on their own streams (default and minimum
  * 2^21; smaller values return CHQ_ERR_ARG); takes effect for newly admitted jobs */
 CHQ_API int chq_server_set_solo_cells(chq_server *s, long long cells);
-/* tune every new lane's batch with chq_batch_autotune (1, the default) or keep the members'
- * default launch settings (0); takes effect for batches built afterwards. A lane is timed once,
- * when it is first built; its later rebuilds (members admitted or finished) give the new
- * members the lane's tuned march length and x variant without timing. */
+/* solo jobs (those above the solo threshold) running at once, default 2: each fills the
+ * device alone; the others wait in the queue while smaller jobs are admitted into the lanes */
+CHQ_API int chq_server_set_solo_slots(chq_server *s, int slots);
+/* tune every new lane's batch with chq_batch_autotune (1) or keep the members' default launch
+ * settings (0, the default: on the ensemble and serving mixes the timing of the candidates
+ * cost more than the tuned settings gained); takes effect for batches built afterwards. A lane
+ * is timed once, when it is first built; its later rebuilds (members admitted or finished)
+ * give the new members the lane's tuned march length and x variant without timing. */
 CHQ_API int chq_server_set_autotune(chq_server *s, int enable);
 
 /* ---- z slabs: one mesh decomposed over several GPUs ------------------------------------------

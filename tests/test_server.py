@@ -66,8 +66,9 @@ def run_all(srv, max_steps=5000):
     raise AssertionError("server did not drain")
 
 
-def test_results_equal_solo_runs_in_any_mix():
-    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=3)
+@pytest.mark.parametrize("autotune", [False, True], ids=["default_settings", "tuned_lanes"])
+def test_results_equal_solo_runs_in_any_mix(autotune):
+    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=3, autotune=autotune)
     ids = [srv.submit(f(), p, prm) for f, p, prm in JOBS]
     run_all(srv)
     for jid, (f, p, prm) in zip(ids, JOBS):
@@ -79,9 +80,11 @@ def test_results_equal_solo_runs_in_any_mix():
         assert st["t_done"] >= st["t_start"] >= st["t_submit"]
 
 
-def test_large_jobs_run_solo_beside_batched_lanes():
+@pytest.mark.parametrize("slots", [None, 1])
+def test_large_jobs_run_solo_beside_batched_lanes(slots):
     """Jobs of 2^21 cells or more run on their own streams (polled, never waited for) while
-    small jobs step in batched lanes; every result equals the job run alone."""
+    small jobs step in batched lanes; at most `slots` of them at once (default 2: the third
+    waits in the queue); every result equals the job run alone."""
     jobs = [
         (lambda: ot_cfg(2048, 4), "orszag_tang", [-1.0]),
         (lambda: blast_cfg(128, 5, precision=1), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 3.0]),
@@ -90,7 +93,7 @@ def test_large_jobs_run_solo_beside_batched_lanes():
         (lambda: ot_cfg(32, 12), "orszag_tang", [-1.0]),
         (lambda: blast_cfg(16, 9, precision=1), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 7.0]),
     ]
-    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=2)
+    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=2, solo_slots=slots)
     ids = [srv.submit(f(), p, prm) for f, p, prm in jobs]
     run_all(srv)
     total = 0
