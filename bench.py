@@ -174,17 +174,26 @@ def l1_per_field(a: dict, b: dict) -> tuple[dict, dict]:
     return rel, mean
 
 
-def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, profile_cycles=2, keep_state=False):
+def run_form(n, precision, steps, warmup, dist, device, sample_clocks=False, profile_cycles=2, keep_state=False,
+             pin=None):
     from chasqui_b200 import Mesh
     mesh = Mesh(blast_config(n, precision))
     mesh.init_problem("blast", BLAST_PARAMS)
     mesh.prime(0.0)
     # flux-kernel march length picked by the library's autotuner on this state (the default
-    # is 16; the per-length launch times are reported beside the choice)
+    # is 16; the per-length launch times are reported beside the choice). `pin` =
+    # (march length, x variant, y/z staging) skips the tuner and sets those, so that a run
+    # under a profiler, whose serialised replays distort the tuner's timings, launches the
+    # kernels a plain run picked.
     default_len = mesh.seglen
-    tune = mesh.autotune()
-    tune["default"] = default_len
-    tune["yz"] = mesh.autotune_yz()   # y/z staging: cp.async (0) or TMA (1), FP64 streaming PPM
+    if pin is not None:
+        mesh.seglen, mesh.xvariant, mesh.yzvariant = pin
+        tune = {"ms": {}, "seglen": mesh.seglen, "xvar": mesh.xvariant, "default": default_len, "pinned": True,
+                "yz": {"yzvar": mesh.yzvariant, "ms": {0: -1.0, 1: -1.0}}}
+    else:
+        tune = mesh.autotune()
+        tune["default"] = default_len
+        tune["yz"] = mesh.autotune_yz()   # y/z staging: cp.async (0) or TMA (1), FP64 streaming PPM
     mesh.cycles(warmup)
     mesh.clock()
     l0 = mesh.kernel_launches()
@@ -398,6 +407,8 @@ def tune_summary(tune):
                 (list(yz["ms"].values()) if yz else []) if t > 0], default=-1)
     if ms.get(d, -1) > 0 and best > 0:
         out["speedup_vs_default"] = ms[d] / best
+    if tune.get("pinned"):
+        out["pinned"] = True
     return out
 
 
@@ -804,6 +815,9 @@ def main(argv=None):
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--serving-study", action="store_true",
                     help="only the serving configuration at its own size range (see serving_study)")
+    ap.add_argument("--flux-settings", default=None, metavar="SEGLEN,XVAR,YZ",
+                    help="set the FP64 headline's flux launch settings (march length, x variant, y/z "
+                         "staging 0 = cp.async / 1 = TMA) instead of autotuning them")
     ap.add_argument("--slabs", action="store_true",
                     help="only the headline blast decomposed into one z slab per rank (strong scaling)")
     args = ap.parse_args(argv)
@@ -837,8 +851,11 @@ def main(argv=None):
     n = args.n
     hbm, peak_kind = peaks()
 
+    pin = tuple(int(v) for v in args.flux_settings.split(",")) if args.flux_settings else None
+    if pin is not None and len(pin) != 3:
+        raise SystemExit("--flux-settings wants SEGLEN,XVAR,YZ")
     mesh, r64 = run_form(n, 0, args.steps, args.warmup, dist, local, sample_clocks=True,
-                         keep_state=not args.no_mixed)
+                         keep_state=not args.no_mixed, pin=pin)
     zones = float(n) ** 3
     value = world * zones * args.steps / (r64["ms_max"] / 1e3)
     ms_step = r64["ms_max"] / args.steps
