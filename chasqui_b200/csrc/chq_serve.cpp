@@ -15,19 +15,24 @@
 // Jobs of 2^21 cells or more (chq_server_set_solo_cells raises the threshold) are not
 // batched: each runs "solo" on its own mesh stream (replaying a CUDA graph of one cycle, except with RKL2) and the
 // server polls an event behind its chunk instead of waiting for it, so a large job never holds
-// up the lanes (or another large job). At most `solo_slots` solo jobs run at once (default 2,
-// chq_server_set_solo_slots): each fills the device alone, and more of them at once only
-// share it less efficiently; the others wait in the queue while smaller jobs behind them are
-// admitted into the lanes. Diffusion (explicit or RKL2), cooling and gravity
+// up the lanes (or another large job). At most `solo_slots` solo jobs run at once (default 1,
+// chq_server_set_solo_slots): each fills the device alone, and two of them at once share it
+// less efficiently (the 40 solo-sized jobs of the 256-job ensemble draw: 15.4 s with two at
+// once, 13.2 s with one, as fast as running them one after another); the others wait in the
+// queue while smaller jobs behind them are admitted into the lanes. No chunk is queued past a
+// job's end where that is known (cycles_left), and a finished solo job's events and pinned
+// clock slots go to the next one. Diffusion (explicit or RKL2), cooling and gravity
 // batch with jobs that have the same terms switched on.
 // Each job keeps its own dt and clock on the device, so its result is the same alone and in
 // any mix. Times are seconds on the server's steady clock.
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <algorithm>
 #include <map>
 #include <string>
 #include <tuple>
+#include <utility>
 #include <vector>
 #include <cuda_runtime.h>
 #include "chq.h"
@@ -61,6 +66,7 @@ struct Job {
   // recorded, which the server polls, so a solo job never waits for the rest of the server
   bool solo = false;
   int head = 0, nfly = 0;             // oldest chunk in flight, chunks in flight
+  long long queued = 0;               // cycles queued since the job was primed
   cudaEvent_t ev[2] = {nullptr, nullptr};
   void *clk[2] = {nullptr, nullptr};  // pinned clock copies
 };
@@ -107,19 +113,39 @@ int err(int code, const std::string &m) {
   return code;
 }
 
+// Cycles a job still needs beyond its first `from` cycles, or -1 when that is not known yet.
+// A cycle limit (time.nlim) gives the exact count. An end time gives an estimate from the
+// job's clock: the mean step so far carries it to tlim, with 5 % and one cycle to spare for
+// a shrinking step. Cycles queued past a job's end return at once on the device, but each
+// still launches every kernel of a cycle over the job's whole grid: this count keeps the
+// server from queueing them.
+long long cycles_left(const Job *j, long long from) {
+  long long need = (j->cfg.nlim >= 0) ? (long long)j->cfg.nlim : -1;
+  if (j->cycle > 0 && j->t > 0 && j->t < j->cfg.tlim) {
+    const double mean = j->t / j->cycle;
+    const double more = std::ceil(1.05 * (j->cfg.tlim - j->t) / mean) + 1.0;
+    const long long est = j->cycle + (long long)std::min(more, 1e9);
+    need = (need < 0) ? est : std::min(need, est);
+  }
+  return (need < 0) ? -1 : need - from;
+}
+
 }  // namespace
 
 struct chq_server {
   long long budget = 0, used = 0;
   int max_active = 0, cycles_per_step = 1, lanes = 8;
   long long solo_cells = 0;   // jobs of at least this many cells run unbatched
-  int solo_slots = 2;         // solo jobs running at once
+  int solo_slots = 1;         // solo jobs running at once
   int autotune = 0;           // tune each new lane's batch (chq_batch_autotune); off by default
   long long next_id = 1;
   std::map<long long, Job *> jobs;
   std::vector<Job *> queue;
   std::map<ClassKey, Group> groups;
   std::vector<Job *> solo;   // running solo jobs
+  // events and pinned clock copies of finished solo jobs, handed to the next solo jobs:
+  // freeing pinned memory synchronises the device, and pinning it costs milliseconds
+  std::vector<std::pair<cudaEvent_t, void *>> spare;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   long long zone_updates = 0;
   double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
@@ -193,7 +219,15 @@ int retire_solo(chq_server *S, bool block) {
     for (double v : j->hist) finite = finite && (v == v) && (v - v == 0.0);
     chq_mesh_destroy(j->mesh);
     j->mesh = nullptr;
-    free_solo(j);
+    // every chunk of the job has finished (chq_history waited for its stream)
+    for (int q = 0; q < 2; ++q) {
+      if (j->ev[q] && j->clk[q]) {
+        S->spare.emplace_back(j->ev[q], j->clk[q]);
+        j->ev[q] = nullptr;
+        j->clk[q] = nullptr;
+      }
+    }
+    free_solo(j);   // a half-made slot, if any
     j->nfly = 0;
     S->used -= j->bytes;
     j->state = finite ? CHQ_JOB_DONE : CHQ_JOB_FAILED;
@@ -242,19 +276,33 @@ int retire_solo(chq_server *S, bool block) {
   return CHQ_OK;
 }
 
-// keep two chunks of cycles_per_step cycles queued on every solo job's stream
+// keep two chunks of cycles_per_step cycles queued on every solo job's stream, none past the
+// job's end where that is known (the last chunk is shortened to it)
 int launch_solo(chq_server *S) {
   for (Job *j : S->solo) {
     while (j->nfly < 2) {
+      long long n = S->cycles_per_step;
+      const long long left = cycles_left(j, j->queued);
+      if (left >= 0) {
+        if (left <= 0 && j->nfly > 0) break;
+        // an end-time estimate fell short with nothing in flight: a short chunk more
+        n = std::min(n, std::max(left, 2LL));
+      }
       const int slot = (j->head + j->nfly) & 1;
+      if (!j->ev[slot] && !S->spare.empty()) {
+        j->ev[slot] = S->spare.back().first;
+        j->clk[slot] = S->spare.back().second;
+        S->spare.pop_back();
+      }
       if (!j->ev[slot]) {
         cudaError_t e = cudaEventCreateWithFlags(&j->ev[slot], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaHostAlloc(&j->clk[slot], chq::clock_bytes(), cudaHostAllocDefault);
         if (e != cudaSuccess) return err(CHQ_ERR_CUDA, std::string("solo job: ") + cudaGetErrorString(e));
       }
-      int rc = chq_cycles(j->mesh, S->cycles_per_step, nullptr);
+      int rc = chq_cycles(j->mesh, (int)n, nullptr);
       if (!rc) rc = chq::clock_enqueue(j->mesh, j->clk[slot]);
       if (rc) return rc;
+      j->queued += n;
       const cudaError_t e = cudaEventRecord(j->ev[slot], chq::mesh_stream(j->mesh));
       if (e != cudaSuccess) return err(CHQ_ERR_CUDA, std::string("solo job: ") + cudaGetErrorString(e));
       ++j->nfly;
@@ -410,6 +458,14 @@ int chq_server_step(chq_server *S) {
     if (!g.batch) continue;
     long long n = S->cycles_per_step;
     if (g.cells > 0) n = std::min<long long>(4LL * S->cycles_per_step, (S->cycles_per_step * heaviest + g.cells - 1) / g.cells);
+    // no cycles past the last member's end where every member's end is known (the members'
+    // clocks were read at this step: the lane has nothing in flight)
+    long long most = 0;
+    for (const Job *j : g.members) {
+      const long long left = cycles_left(j, j->cycle);
+      most = (left < 0 || most < 0) ? -1 : std::max(most, left);
+    }
+    if (most >= 0) n = std::min(n, std::max(most, 1LL));
     rc = chq_batch_cycles(g.batch, (int)std::max(1LL, n), nullptr);
     if (rc) return rc;
     active += (int)g.members.size();
@@ -491,6 +547,10 @@ int chq_server_destroy(chq_server *S) {
     if (kv.second->mesh) chq_mesh_destroy(kv.second->mesh);   // synchronises its stream first
     free_solo(kv.second);
     delete kv.second;
+  }
+  for (auto &sp : S->spare) {
+    cudaEventDestroy(sp.first);
+    if (sp.second) cudaFreeHost(sp.second);
   }
   delete S;
   return CHQ_OK;

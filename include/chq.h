@@ -328,7 +328,7 @@ CHQ_API int chq_server_set_lanes(chq_server *s, int lanes);
 /* jobs of at least `cells` cells run unbatched on their own streams (default and minimum
  * 2^21; smaller values return CHQ_ERR_ARG); takes effect for newly admitted jobs */
 CHQ_API int chq_server_set_solo_cells(chq_server *s, long long cells);
-/* solo jobs (those above the solo threshold) running at once, default 2: each fills the
+/* solo jobs (those above the solo threshold) running at once, default 1: each fills the
  * device alone; the others wait in the queue while smaller jobs are admitted into the lanes */
 CHQ_API int chq_server_set_solo_slots(chq_server *s, int slots);
 /* tune every new lane's batch with chq_batch_autotune (1) or keep the members' default launch

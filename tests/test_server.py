@@ -49,12 +49,12 @@ def solo_history(cfg, problem, params):
     m.prime(0.0)
     if cfg.precision == 1 and cfg.nx1 * cfg.nx2 * cfg.nx3 < SOLO_CELLS:
         b = Batch([m], graph=True)
-        while not b.status()[0]["done"] and b.status()[0]["cycle"] < cfg.nlim:
+        while not b.status()[0]["done"] and (cfg.nlim < 0 or b.status()[0]["cycle"] < cfg.nlim):
             b.cycles(4)
         cyc = b.status()[0]["cycle"]
         b.close()
         return m.history(), cyc
-    while not m.clock()["cycle"] >= cfg.nlim and m.clock()["t"] < cfg.tlim:
+    while (cfg.nlim < 0 or m.clock()["cycle"] < cfg.nlim) and m.clock()["t"] < cfg.tlim:
         m.cycles(4)
     return m.history(), m.clock()["cycle"]
 
@@ -80,11 +80,11 @@ def test_results_equal_solo_runs_in_any_mix(autotune):
         assert st["t_done"] >= st["t_start"] >= st["t_submit"]
 
 
-@pytest.mark.parametrize("slots", [None, 1])
+@pytest.mark.parametrize("slots", [None, 2])
 def test_large_jobs_run_solo_beside_batched_lanes(slots):
     """Jobs of 2^21 cells or more run on their own streams (polled, never waited for) while
-    small jobs step in batched lanes; at most `slots` of them at once (default 2: the third
-    waits in the queue); every result equals the job run alone."""
+    small jobs step in batched lanes; at most `slots` of them at once (default 1: the others
+    wait in the queue); every result equals the job run alone."""
     jobs = [
         (lambda: ot_cfg(2048, 4), "orszag_tang", [-1.0]),
         (lambda: blast_cfg(128, 5, precision=1), "blast", [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 3.0]),
@@ -106,6 +106,32 @@ def test_large_jobs_run_solo_beside_batched_lanes(slots):
         total += f().nlim * f().nx1 * f().nx2 * f().nx3
     s = srv.stats()
     assert s["zone_updates"] == total and s["active"] == 0 and s["used_bytes"] == 0
+
+
+def test_time_limited_jobs_end_at_their_end_time():
+    """Jobs with an end time and no cycle limit. The server sizes their last chunks from the
+    mean step so far instead of a cycle count; where that estimate falls short it runs a
+    short chunk more. Every job ends on the cycle the job run alone ends on, with its result."""
+    box = dict(x1min=-.5, x1max=.5, x2min=-.5, x2max=.5, x3min=-.5, x3max=.5)
+    jobs = [
+        (lambda: make_config(nx1=32, nx2=32, nx3=1, cfl=0.4, tlim=0.05, nlim=-1), "orszag_tang", [-1.0]),
+        (lambda: make_config(nx1=16, nx2=16, nx3=16, cfl=0.3, tlim=0.02, nlim=-1, **box), "blast",
+         [10.0, 0.1, 0.1, 1.0, 45.0, 1e-3, 7.0]),
+        (lambda: make_config(nx1=24, nx2=24, nx3=1, cfl=0.4, tlim=0.03, nlim=-1, precision=1), "orszag_tang", [0.5]),
+        (lambda: make_config(nx1=1536, nx2=1536, nx3=1, cfl=0.4, tlim=0.002, nlim=-1), "orszag_tang", [-1.0]),
+    ]
+    srv = Server(hbm_budget_bytes=40 << 30, cycles_per_step=3)
+    ids = [srv.submit(f(), p, prm) for f, p, prm in jobs]
+    run_all(srv)
+    total = 0
+    for jid, (f, p, prm) in zip(ids, jobs):
+        st = srv.status(jid)
+        h, cyc = solo_history(f(), p, prm)
+        assert st["state"] == "done", st
+        assert st["cycle"] == cyc >= 2 and st["t"] >= f().tlim, (p, st, cyc)
+        assert np.array_equal(np.array(st["history"]), h), (p, st["history"], h)
+        total += cyc * f().nx1 * f().nx2 * f().nx3
+    assert srv.stats()["zone_updates"] == total
 
 
 def test_jobs_with_diffusion_and_source_terms():
