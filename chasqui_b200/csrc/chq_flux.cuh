@@ -270,7 +270,8 @@ CHQ_D bool mbar_wait(unsigned long long *mb, unsigned parity) {
 }
 // generic-proxy accesses of shared memory before the async-proxy writes that follow
 CHQ_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-// one box of a 4-D tensor map (no multicast) into shared memory, completing on mb
+// one box of a 4-D tensor map over this GPU's own memory into this CTA's shared memory only,
+// completing on mb
 CHQ_D void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, unsigned long long *mb) {
   asm volatile(
       "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(
